@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 rule x scenario evaluator.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): the evaluation of one GP generation -- 1024 rules (the
+initial ramped half-and-half population of a GP run over the 29-terminal
+menu, depth 2-8) on 500 stochastic scenarios of a clustered 100-customer
+synthetic instance (8 Gaussian clusters, H=1000, m=3): 512,000 bit-exact
+(rule, scenario) route simulations.  Synthetic data stands in for the
+benchmark's own instances (the reference ships no generator).
+
+value      : evaluations/s with rules and scenarios resident in HBM, kernel time
+             by CUDA events on the launching stream, L2 flushed between steps.
+e2e        : the same metric through the reference-shaped host call
+             (sidr_evaluate: host rules/scenarios in, host scores out, all
+             copies inside the timed region), wall clock.
+roofline   : the evaluator is bound by the FP64 pipe / issue rate, not HBM or
+             tensor cores; achieved = op-model FP64 operations per launch
+             (counted by the kernel's counting instantiation) / kernel time,
+             peak = the FP64 pipe throughput measured on this GPU.
+cpu_baseline: the reference's CPU simulator (compiled from its own headers,
+             oracle/_ref) or else the C oracle, on all host threads, on a
+             bounded sample of the same workload.
+
+Multi-GPU: pairs are independent, so each rank evaluates its own generation
+(weak scaling, no collective on the data path); the timing is the maximum over
+ranks of the device-timed total.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "solver-informed-dispatching-rules_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "bit-exact rule×scenario evals/s"
+UNIT = "evals/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--P", type=int, default=1024)
+    ap.add_argument("--S", type=int, default=500)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_for(rank: int, P: int, S: int):
+    """Rank 0 evaluates the GP's initial generation; other ranks evaluate the
+    same instance with populations of their own seed (same sizes)."""
+    from sidr import workload as W
+    if rank == 0:
+        return W.gp_generation(P=P, S=S)
+    return W.build("gp_generation", 100, "clustered", 1000.0, 3, 2, P, 2, 8, rank, S, 1)
+
+
+def config_of(P, S, world):
+    return {"workload": f"gp_generation: {P} rules x {S} scenarios, clustered synthetic "
+                        f"instance n=100 (8 clusters), H=1000, m=3, 29-terminal menu, "
+                        f"RHH depth 2-8",
+            "rules": P, "scenarios": S, "customers": 100, "vehicles": 3, "horizon": 1000,
+            "terminals": 29, "parallelism": f"{world} independent generations (one per GPU)",
+            "l2": "flushed between timed steps (256 MiB device write outside the events)"}
+
+
+# --------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
+
+
+def gpu_uuid(dev: int) -> str:
+    import torch
+    u = str(torch.cuda.get_device_properties(dev).uuid)
+    return u if u.startswith("GPU-") else "GPU-" + u
+
+
+# ---------------------------------------------------------- CPU baseline
+
+def cpu_sample(P, S, stride_rules=16, chunk=8):
+    rule_idx = list(range(0, P, stride_rules))
+    chunks = [(s, min(S, s + chunk)) for s in range(0, S, chunk)]
+    return rule_idx, chunks
+
+
+def cpu_checker():
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    if O.reference_available():
+        return O.Reference(), "reference"
+    return O.Oracle(), "port"
+
+
+def cpu_baseline(w, zp, seconds, gpu_out=None):
+    """The CPU simulator on all host threads over a bounded, strided sample of
+    the workload; returns the baseline record (and the parity of the sample
+    against the GPU's scores when given)."""
+    import numpy as np
+    chk, kind = cpu_checker()
+    threads = os.cpu_count() or 1
+    idx, chunks = cpu_sample(w.rules.P, w.S)
+    sub = w.rules.subset(idx)
+    evals, t_used, cmp, bad = 0, 0.0, 0, 0
+    for s0, s1 in chunks:
+        t0 = time.perf_counter()
+        out = chk.eval_pairs(w.sd, zp, sub, w.sampled[s0:s1], s1 - s0, w.mask, nthreads=threads)
+        t_used += time.perf_counter() - t0
+        evals += out.size
+        if gpu_out is not None:
+            g = gpu_out[idx][:, s0:s1]
+            cmp += g.size
+            bad += int(np.count_nonzero(g.view(np.uint64) != out.view(np.uint64)))
+        if t_used >= seconds:
+            break
+    rec = {"value": evals / t_used, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"every 16th rule ({len(idx)} rules) x first {evals // len(idx)} scenarios "
+                     f"= {evals} evaluations in {t_used:.1f} s"}
+    if gpu_out is not None:
+        rec["parity"] = {"pairs": cmp, "mismatches": bad}
+    return rec
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU simulator on the host cores, each
+    step a bounded sample of the workload."""
+    if rank != 0:
+        return
+    from sidr import workload as W
+    import sidr.rules  # noqa: F401
+    w = W.gp_generation(P=args.P, S=args.S)
+    chk, kind = cpu_checker()
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    zp = chk.zp_of(w.sd) if kind == "reference" else chk.zstats(w.sd)
+    threads = os.cpu_count() or 1
+    idx, _ = cpu_sample(w.rules.P, w.S)
+    sub = w.rules.subset(idx)
+    per = 16
+    nsteps = args.warmup + args.steps
+    times, evals = [], 0
+    for k in range(nsteps):
+        s0 = (k * per) % w.S
+        s1 = min(w.S, s0 + per)
+        t0 = time.perf_counter()
+        out = chk.eval_pairs(w.sd, zp, sub, w.sampled[s0:s1], s1 - s0, w.mask, nthreads=threads)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+            evals += out.size
+    tot = sum(times)
+    value = evals / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(args.P, args.S, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"per step {len(idx)} rules (every 16th) x {per} scenarios"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+
+def profile_traffic():
+    """Per-launch DRAM traffic of the evaluator kernel from the committed ncu
+    summary (profiles/), scaled to this workload; None when absent."""
+    p = os.path.join(REPO, "profiles", "eval_kernel_traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        with open(p) as f:
+            return json.load(f).get("bytes_per_launch")
+    except Exception:
+        return None
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    import sidr
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = workload_for(rank, args.P, args.S)
+    zp = sidr.zstats(w.sd)
+    ctx = sidr.Context(w.sd, zp, device=local)
+    batch = ctx.batch(w.rules, w.sampled, w.S, w.mask)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    # op-model counts (separate, untimed launch of the counting instantiation)
+    batch.set_counting(True)
+    batch.run(sh)
+    torch.cuda.synchronize()
+    counts = batch.counts()
+    batch.set_counting(False)
+
+    peak_ops = ctypes_fp64_peak(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        batch.run(sh)
+    torch.cuda.synchronize()
+    ref_out = batch.read()
+
+    clocks = ClockSampler(gpu_uuid(local))
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = sidr.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        batch.run(sh)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = sidr.kernel_launches() - launches0
+    clk = clocks.stop()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total_ms = allmax(sum(step_ms))
+    evals_per_rank = w.rules.P * w.S
+    value = world * evals_per_rank * args.steps / (total_ms / 1e3)
+    same = bool(np.array_equal(batch.read().view(np.uint64), ref_out.view(np.uint64)))
+
+    # end to end through the reference-shaped host call
+    e2e = None
+    if not args.no_e2e:
+        ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
+        barrier()
+        t_e2e = 0.0
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
+            t_e2e += time.perf_counter() - t0
+        t_e2e = allmax(t_e2e)
+        h2d, d2h = transfer_bytes()
+        same = same and bool(np.array_equal(out.view(np.uint64), ref_out.view(np.uint64)))
+        e2e = {"value": world * evals_per_rank * args.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": 1e3 * t_e2e / args.steps}
+
+    avg_s = (sum(step_ms) / len(step_ms)) / 1e3
+    achieved = counts["fp64_ops"] / avg_s
+    traffic = profile_traffic()
+    roofline = {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_ops / 1e12,
+                "unit": "Tops/s (FP64 pipe, op model)", "frac": achieved / peak_ops,
+                "traffic": traffic,
+                "peak_source": "measured on this GPU by sidr_fp64_peak (DFMA chains over all SMs)",
+                "op_model": "sidr_counts.fp64_ops (include/sidr.h)"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_of(args.P, args.S, world),
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk,
+            "counts": counts, "repeat_runs_identical": same}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, zp, args.cpu_seconds, gpu_out=ref_out)
+    batch.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def ctypes_fp64_peak(dev: int) -> float:
+    import ctypes as C
+    import sidr
+    L = sidr.load()
+    L.sidr_fp64_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    v = C.c_double()
+    st = L.sidr_fp64_peak(dev, 5, C.byref(v))
+    if st != 0:
+        raise RuntimeError(L.sidr_last_error().decode())
+    return v.value
+
+
+def transfer_bytes():
+    import ctypes as C
+    import sidr
+    L = sidr.load()
+    L.sidr_last_transfer_bytes.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    a, b = C.c_int64(), C.c_int64()
+    L.sidr_last_transfer_bytes(C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,178 @@
+/*
+ * sidr.h -- C-ABI of the B200 rule x scenario evaluator.
+ *
+ * Scores postfix-encoded dispatching rules against stochastic route-simulation
+ * scenarios of the stochastic team orienteering problem with time windows,
+ * bit-exact against the reference CPU simulator
+ * (augustompm/solver-informed-dispatching-rules, engine/sim_host.hpp:67-83
+ * sim_batch -> engine/sim_core.hpp sim_one/pick_best).
+ *
+ * Plain pointers and sizes only.  Every function returns a status and never
+ * exits the process (the reference's CUDA_CHECK calls exit(2),
+ * engine/factory.cuh:16-18); sidr_last_error() describes the last failure on
+ * the calling thread.  One context per host thread, or external locking.
+ *
+ * Data formats are the reference's own:
+ *   instance  -- SimData SoA (engine/sim_host.hpp:12-40): customers 0..n-1,
+ *                dist (n+1)x(n+1) row-major with the depot at index 0;
+ *   rules     -- PackedTrees (engine/factory.cuh:20-24): post-order int32
+ *                ops[] (-1 terminal slot, -2 constant in thousandths, 0..5
+ *                + - * / min max, 6 rmod) with two int32 args per node, and
+ *                per-rule offsets[] / lengths[];
+ *   scenarios -- sampled service durations, [G groups][T scenarios][n];
+ *   masks     -- int64 rows of 61 terminal flags (engine/sim_host.hpp:85-94);
+ *   output    -- out[p*T + s], the collected score of rule p on scenario s.
+ */
+#ifndef SIDR_H
+#define SIDR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SIDR_N_TERMS 61   /* engine/vocab.hpp:16 N_TERMS   */
+#define SIDR_MAX_N 512    /* engine/vocab.hpp:17 MAX_N     */
+#define SIDR_MAX_TREE 1024 /* engine/vocab.hpp:18 MAX_TREE */
+#define SIDR_MAX_STACK 32 /* engine/vocab.hpp:19 MAX_STACK */
+
+typedef enum sidr_status {
+    SIDR_OK = 0,
+    SIDR_ERR_INVALID = 1,   /* bad argument, size or pointer            */
+    SIDR_ERR_RULE = 2,      /* malformed rule (opcode, slot, stack)      */
+    SIDR_ERR_TOO_LARGE = 3, /* n > SIDR_MAX_N, rule > SIDR_MAX_TREE ...  */
+    SIDR_ERR_CUDA = 4,      /* a CUDA runtime call failed                */
+    SIDR_ERR_NO_DEVICE = 5, /* no usable CUDA device                     */
+    SIDR_ERR_KERNEL = 6,    /* the kernel reported an internal fault     */
+    SIDR_ERR_NONFINITE = 7  /* NaN or infinity in instance or scenarios  */
+} sidr_status;
+
+typedef struct sidr_ctx sidr_ctx;
+typedef struct sidr_batch sidr_batch;
+
+/* One instance, the reference's SimData (engine/sim_host.hpp:12-40). */
+typedef struct sidr_instance_desc {
+    int32_t n;                    /* customers (depot excluded), 1..SIDR_MAX_N */
+    int32_t m;                    /* vehicles                                  */
+    double tmax;                  /* route deadline (depot due time)           */
+    const double* scores;         /* [n]                                       */
+    const double* durations;      /* [n] expected service times                */
+    const double* open_t;         /* [n]                                       */
+    const double* close_t;        /* [n]                                       */
+    const double* dist;           /* [(n+1)*(n+1)], depot at 0                 */
+    const double* dist_to_depot;  /* [n]                                       */
+} sidr_instance_desc;
+
+/* Rules in the reference's PackedTrees layout (engine/factory.cuh:20-40). */
+typedef struct sidr_rules_desc {
+    const int32_t* ops;      /* [n_nodes]                       */
+    const int32_t* args;     /* [2*n_nodes]                     */
+    const int32_t* offsets;  /* [P] first node of rule p        */
+    const int32_t* lengths;  /* [P] node count of rule p        */
+    int32_t P;               /* rules                           */
+    int64_t n_nodes;         /* length of ops                   */
+} sidr_rules_desc;
+
+const char* sidr_last_error(void);
+const char* sidr_status_string(sidr_status s);
+int sidr_version(void);
+
+/* zp_of (engine/sim_host.hpp:96-105 -> zstats, engine/sim_core.hpp:277-312):
+ * the 5 z-feature means then 5 stds at the initial state, computed on the host
+ * with the same libm as the reference. */
+sidr_status sidr_zstats(const sidr_instance_desc* inst, double zp[10]);
+
+/* FactoryContext(sd, zp) (engine/factory.cuh:129-137): copies the instance to
+ * device `device` once, with the per-instance lookup tables the kernels use. */
+sidr_status sidr_ctx_create(const sidr_instance_desc* inst, const double zp[10], int device,
+                            sidr_ctx** out);
+void sidr_ctx_destroy(sidr_ctx* ctx);
+
+/* FactoryContext::evaluate (engine/factory.cuh:144-164): all P rules on the
+ * same N scenarios (sampled [N][n]) under one mask; out[P*N] host. */
+sidr_status sidr_evaluate(sidr_ctx* ctx, const sidr_rules_desc* rules, const double* sampled,
+                          int32_t N, const int64_t* term_mask, double* out);
+
+/* FactoryContext::evaluate_grouped (engine/factory.cuh:167-189): rule p uses
+ * scenario group p/group_size of grouped_sampled [G][T][n]; out[P*T] host. */
+sidr_status sidr_evaluate_grouped(sidr_ctx* ctx, const sidr_rules_desc* rules,
+                                  const double* grouped_sampled, int32_t G, int32_t T,
+                                  int32_t group_size, const int64_t* term_mask, double* out);
+
+/* FactoryContext::evaluate_grouped_masks (engine/factory.cuh:193-216): as
+ * grouped, with mask row p/mask_group of masks [ceil(P/mask_group)][61].
+ * G (the group count, which the reference infers from the vector size) is
+ * passed explicitly so the scenario buffer can be bounds-checked. */
+sidr_status sidr_evaluate_grouped_masks(sidr_ctx* ctx, const sidr_rules_desc* rules,
+                                        const double* grouped_sampled, int32_t G, int32_t T,
+                                        int32_t group_size, int32_t mask_group,
+                                        const int64_t* masks, double* out);
+
+/* Device-resident batches (no reference counterpart; the reference copies
+ * every input on every call, engine/factory.cuh:144-164).  sidr_batch_create
+ * validates and repacks the rules, uploads rules, scenarios and masks once and
+ * keeps them in HBM; sidr_batch_run launches the evaluator on `stream`
+ * (a cudaStream_t, 0 = legacy default) and returns without waiting;
+ * sidr_batch_read waits for the stream and copies out[P*T] to the host;
+ * sidr_batch_fitness writes the per-rule mean over the T scenarios, summed in
+ * scenario order then divided by T, as the reference drivers do
+ * (engine/gp_engine.cu:76-81). */
+sidr_status sidr_batch_create(sidr_ctx* ctx, const sidr_rules_desc* rules,
+                              const double* grouped_sampled, int32_t G, int32_t T,
+                              int32_t group_size, int32_t mask_group, const int64_t* masks,
+                              sidr_batch** out);
+sidr_status sidr_batch_run(sidr_batch* b, void* stream);
+sidr_status sidr_batch_read(sidr_batch* b, double* out);
+sidr_status sidr_batch_fitness(sidr_batch* b, double* fitness);
+/* Device pointer of the [P*T] result buffer (valid until destroy). */
+const double* sidr_batch_device_out(const sidr_batch* b);
+void sidr_batch_destroy(sidr_batch* b);
+
+/* Work counters of the last run of a batch (filled when the batch was run with
+ * counting enabled by sidr_batch_set_counting; no reference counterpart).
+ * fp64_ops is the op model of the roofline: the floating-point operations the
+ * reference's loops perform for the same decisions -- per neighbour visited
+ * by an enabled terminal family, its feasibility test (6 ops) plus the
+ * family's payload; ATRISK neighbours 40 (two erf counted as 15 each);
+ * candidate setup and the rule's binary operators 1 each. */
+typedef struct sidr_counts {
+    int64_t decisions;   /* pick_best calls                               */
+    int64_t candidates;  /* feasible candidates scored                     */
+    int64_t scan_iters;  /* (candidate, neighbour) pairs of the fused scan */
+    int64_t heavy_iters; /* ATRISK neighbour iterations (two erf each)     */
+    int64_t hop_iters;   /* second-hop and REACH-k step neighbour pairs    */
+    int64_t fp64_ops;    /* op-model total, see above                      */
+} sidr_counts;
+sidr_status sidr_batch_set_counting(sidr_batch* b, int enable);
+sidr_status sidr_batch_counts(sidr_batch* b, sidr_counts* out);
+
+/* Host-only validation of rules under their masks (no device needed): the
+ * checks every evaluate call makes -- opcodes, terminal slots < 61, no stack
+ * underflow, stack depth <= SIDR_MAX_STACK, one value left, length <=
+ * SIDR_MAX_TREE -- plus compilation into the kernel's programs.  *max_rows
+ * (may be NULL) receives the per-lane value rows the largest program needs.
+ * No reference counterpart: the reference interpreter does not validate
+ * (engine/sim_core.hpp:11-41). */
+sidr_status sidr_rules_check(const sidr_rules_desc* rules, const int64_t* masks,
+                             int32_t mask_group, int32_t* max_rows);
+
+/* Number of kernel launches issued by this library since load (evaluator
+ * and per-rule fitness kernels). */
+int64_t sidr_kernel_launches(void);
+
+/* Host<->device bytes moved by the calling thread's last sidr_evaluate*
+ * call (rules, scenarios and masks up; scores down). */
+sidr_status sidr_last_transfer_bytes(int64_t* h2d, int64_t* d2h);
+
+/* Measured FP64 pipe throughput of `device`, in operations per second: a
+ * kernel of independent double-precision add/multiply chains over every SM
+ * (each instruction one operation), best of `reps` timed runs.  The
+ * denominator of the evaluator's roofline; no reference counterpart. */
+sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

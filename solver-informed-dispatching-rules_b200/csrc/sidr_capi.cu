@@ -1,0 +1,672 @@
+// sidr_capi.cu -- the C-ABI of the evaluator (include/sidr.h).
+//
+// Contexts own the device copy of one instance and its lookup tables
+// (FactoryContext's one-time upload, engine/factory.cuh:129-137).  Batches own
+// one set of rules, scenarios and masks in HBM.  The reference-shaped
+// evaluate* calls reuse grow-only device buffers held by the context instead of
+// allocating and freeing per call (engine/factory.cuh:144-164 mallocs and frees
+// seven buffers per call).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sidr.h"
+#include "sidr_host.hpp"
+#include "sidr_kernel.cuh"
+
+using namespace sidr;
+
+namespace {
+
+thread_local std::string g_err;
+thread_local long long g_h2d = 0, g_d2h = 0;
+std::atomic<long long> g_launches{0};
+
+// Op-model cost of one fused-scan neighbour for a rule's need set: the
+// feasibility tests it shares plus each family's payload (counting only).
+int scan_ops_of(uint32_t need) {
+    int c = 0;
+    if (need & (kNeedNSFused | kNeedRegret)) c += kOpsTest;
+    if (need & kNeedNS) c += 2;
+    if (need & kNeedMaxN) c += 2;
+    if (need & kNeedReach2) c += 2;
+    if (need & kNeedNSTW) c += 8;
+    if (need & kNeedRegret) c += 1;
+    if (need & kNeedRob) c += kOpsTest + 1;
+    if (need & kNeedNSRob) c += 2;
+    if (need & kNeedReach2Rob) c += 2;
+    if (need & kNeedAfterC) c += kOpsTest;
+    if (need & (kNeedStruct | kNeedPBust)) c += 6;
+    if (need & kNeedReachK) c += 2;
+    return c;
+}
+
+sidr_status fail(sidr_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+#define SIDR_CUDA(call)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(SIDR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// Rules compiled for one launch.
+struct HostPrograms {
+    std::vector<uint32_t> prog;
+    std::vector<double> consts;
+    std::vector<uint8_t> slots;
+    std::vector<RuleMeta> meta;
+    int rows = 1, prog_cap = 1, const_cap = 1;
+};
+
+}  // namespace
+
+struct sidr_ctx {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    HostInstance h;
+    DevInst inst{};
+    std::vector<void*> owned;  // instance arrays and tables
+    cudaStream_t stream = nullptr;
+    // grow-only scratch of the reference-shaped evaluate* calls
+    DevBuf prog, consts, slots, meta, sampled, out, counter, stats, error;
+};
+
+struct sidr_batch {
+    sidr_ctx* ctx = nullptr;
+    DevBatch b{};
+    int P = 0, T = 0, G = 0, group_size = 1;
+    bool counting = false;
+    int grid = 0, block = 0;
+    size_t smem = 0;
+    DevBuf prog, consts, slots, meta, sampled, out, counter, stats, error, fit;
+    bool ran = false;
+};
+
+namespace {
+
+sidr_status check_rules(const sidr_rules_desc* r) {
+    if (!r) return fail(SIDR_ERR_INVALID, "rules descriptor is null");
+    if (r->P < 0) return fail(SIDR_ERR_INVALID, "P < 0");
+    if (r->P > 0 && (!r->ops || !r->args || !r->offsets || !r->lengths))
+        return fail(SIDR_ERR_INVALID, "null rule array");
+    for (int p = 0; p < r->P; p++) {
+        const long long o = r->offsets[p], L = r->lengths[p];
+        if (o < 0 || L < 1 || o + L > r->n_nodes)
+            return fail(SIDR_ERR_INVALID, "rule " + std::to_string(p) + ": offset/length outside ops");
+    }
+    return SIDR_OK;
+}
+
+// Compile every rule under its mask row.
+sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask_group,
+                        HostPrograms& hp) {
+    hp = HostPrograms();
+    hp.meta.resize(r->P);
+    CompiledRule cr;
+    for (int p = 0; p < r->P; p++) {
+        const int64_t* M = masks + (size_t)(p / mask_group) * kTerms;
+        std::string e = compile_rule(r->ops + r->offsets[p], r->args + 2 * (size_t)r->offsets[p],
+                                     r->lengths[p], M, cr);
+        if (!e.empty()) {
+            const sidr_status s = (e.find("MAX_") != std::string::npos) ? SIDR_ERR_TOO_LARGE
+                                                                        : SIDR_ERR_RULE;
+            return fail(s, "rule " + std::to_string(p) + ": " + e);
+        }
+        RuleMeta& m = hp.meta[p];
+        m.prog_off = (int32_t)hp.prog.size();
+        m.const_off = (int32_t)hp.consts.size();
+        m.slot_off = (int32_t)hp.slots.size();
+        m.n_ins = (int16_t)cr.prog.size();
+        m.n_const = (int16_t)cr.consts.size();
+        m.K = (int16_t)cr.K;
+        m.D = (int16_t)cr.D;
+        m.res = (int16_t)cr.res;
+        m.reach_k = (int8_t)cr.reach_k;
+        m.scan_ops = (uint16_t)scan_ops_of(cr.need);
+        m.need = cr.need;
+        m.explore = cr.explore;
+        hp.prog.insert(hp.prog.end(), cr.prog.begin(), cr.prog.end());
+        hp.consts.insert(hp.consts.end(), cr.consts.begin(), cr.consts.end());
+        hp.slots.insert(hp.slots.end(), cr.slots.begin(), cr.slots.end());
+        hp.rows = std::max(hp.rows, cr.K + cr.D);
+        hp.prog_cap = std::max(hp.prog_cap, (int)cr.prog.size());
+        hp.const_cap = std::max(hp.const_cap, (int)cr.consts.size());
+    }
+    if (hp.prog.empty()) hp.prog.push_back(0);
+    if (hp.consts.empty()) hp.consts.push_back(0.0);
+    if (hp.slots.empty()) hp.slots.push_back(0);
+    return SIDR_OK;
+}
+
+sidr_status check_grouping(const sidr_rules_desc* r, const double* sampled, int G, int T,
+                           int group_size, int mask_group, const int64_t* masks) {
+    if (T < 0 || G < 0) return fail(SIDR_ERR_INVALID, "negative scenario count");
+    if (group_size < 1 || mask_group < 1) return fail(SIDR_ERR_INVALID, "group sizes must be >= 1");
+    if (r->P > 0 && T > 0) {
+        if ((long long)(r->P - 1) / group_size >= G)
+            return fail(SIDR_ERR_INVALID, "rules address scenario groups beyond G");
+        if (!sampled) return fail(SIDR_ERR_INVALID, "scenario buffer is null");
+    }
+    if (r->P > 0 && !masks) return fail(SIDR_ERR_INVALID, "mask buffer is null");
+    return SIDR_OK;
+}
+
+sidr_status check_finite(const double* v, size_t count) {
+    for (size_t k = 0; k < count; k++)
+        if (!std::isfinite(v[k]))
+            return fail(SIDR_ERR_NONFINITE, "non-finite sampled duration at index " + std::to_string(k));
+    return SIDR_OK;
+}
+
+template <class T>
+cudaError_t upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = buf.ensure(v.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// Launch geometry for a program set: warps per block bounded by the shared
+// memory each warp's slice takes; one persistent grid over all SMs.
+sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bool counting,
+                        int& grid, int& block, size_t& smem) {
+    const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
+    if (slice > c->smem_optin)
+        return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
+    int wpb = (int)std::min<size_t>(8, c->smem_optin / slice);
+    if (wpb < 1) wpb = 1;
+    block = 32 * wpb;
+    smem = slice * wpb;
+    const void* fn = counting ? (const void*)eval_kernel<true> : (const void*)eval_kernel<false>;
+    SIDR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SIDR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
+    if (per_sm < 1) per_sm = 1;
+    long long want = (items + wpb - 1) / wpb;
+    grid = (int)std::max<long long>(1, std::min<long long>(want, (long long)c->sm_count * per_sm));
+    return SIDR_OK;
+}
+
+sidr_status launch(sidr_ctx* c, const DevBatch& b, bool counting, int grid, int block, size_t smem,
+                   cudaStream_t st) {
+    SIDR_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), st));
+    if (counting && b.stats) SIDR_CUDA(cudaMemsetAsync(b.stats, 0, kStats * sizeof(unsigned long long), st));
+    if ((long long)b.P * b.T == 0) return SIDR_OK;
+    if (counting) eval_kernel<true><<<grid, block, smem, st>>>(c->inst, b);
+    else eval_kernel<false><<<grid, block, smem, st>>>(c->inst, b);
+    SIDR_CUDA(cudaGetLastError());
+    g_launches.fetch_add(1);
+    return SIDR_OK;
+}
+
+// FP64 pipe probe: 8 independent add/multiply chains per thread.
+__global__ void fp64_probe_kernel(double* sink, int iters, double a, double b) {
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = a + threadIdx.x * 1e-9 + k;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = __fma_rn(x[k], b, a);  // one DFMA per chain
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == 1234.5) sink[threadIdx.x] = s;
+}
+
+__global__ void fitness_kernel(const double* out, int P, int T, double* fit) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    double acc = 0.0;
+    for (int s = 0; s < T; s++) acc += out[(size_t)p * T + s];
+    fit[p] = acc / T;
+}
+
+// Shared body of the three reference-shaped evaluate calls.
+sidr_status evaluate_common(sidr_ctx* c, const sidr_rules_desc* r, const double* sampled, int G,
+                            int T, int group_size, int mask_group, const int64_t* masks,
+                            double* out) {
+    if (!c) return fail(SIDR_ERR_INVALID, "context is null");
+    g_h2d = g_d2h = 0;
+    sidr_status s = check_rules(r);
+    if (s) return s;
+    s = check_grouping(r, sampled, G, T, group_size, mask_group, masks);
+    if (s) return s;
+    if (r->P > 0 && T > 0 && !out) return fail(SIDR_ERR_INVALID, "output buffer is null");
+    const int P = r->P;
+    if ((long long)P * T == 0) return SIDR_OK;
+    const int groups_used = (P - 1) / group_size + 1;
+    const size_t n_smp = (size_t)groups_used * T * c->h.n;
+    s = check_finite(sampled, n_smp);
+    if (s) return s;
+    HostPrograms hp;
+    s = compile_all(r, masks, mask_group, hp);
+    if (s) return s;
+    g_h2d = (long long)(hp.prog.size() * 4 + hp.consts.size() * 8 + hp.slots.size() +
+                        hp.meta.size() * sizeof(RuleMeta) + n_smp * 8);
+    g_d2h = (long long)P * T * 8;
+    SIDR_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    SIDR_CUDA(upload(c->prog, hp.prog, st));
+    SIDR_CUDA(upload(c->consts, hp.consts, st));
+    SIDR_CUDA(upload(c->slots, hp.slots, st));
+    SIDR_CUDA(upload(c->meta, hp.meta, st));
+    SIDR_CUDA(c->sampled.ensure(n_smp * sizeof(double)));
+    SIDR_CUDA(cudaMemcpyAsync(c->sampled.p, sampled, n_smp * sizeof(double), cudaMemcpyHostToDevice, st));
+    SIDR_CUDA(c->out.ensure((size_t)P * T * sizeof(double)));
+    SIDR_CUDA(c->counter.ensure(sizeof(unsigned long long)));
+    SIDR_CUDA(c->error.ensure(sizeof(int)));
+    SIDR_CUDA(cudaMemsetAsync(c->error.p, 0, sizeof(int), st));
+    DevBatch b{};
+    b.P = P;
+    b.T = T;
+    b.group_size = group_size;
+    b.n = c->h.n;
+    b.prog = (const uint32_t*)c->prog.p;
+    b.consts = (const double*)c->consts.p;
+    b.slots = (const uint8_t*)c->slots.p;
+    b.meta = (const RuleMeta*)c->meta.p;
+    b.sampled = (const double*)c->sampled.p;
+    b.out = (double*)c->out.p;
+    b.counter = (unsigned long long*)c->counter.p;
+    b.stats = nullptr;
+    b.error = (int*)c->error.p;
+    b.rows = hp.rows;
+    b.prog_cap = hp.prog_cap;
+    b.const_cap = hp.const_cap;
+    int grid, block;
+    size_t smem;
+    s = plan_launch(c, hp, (long long)P * T, false, grid, block, smem);
+    if (s) return s;
+    s = launch(c, b, false, grid, block, smem, st);
+    if (s) return s;
+    SIDR_CUDA(cudaMemcpyAsync(out, c->out.p, (size_t)P * T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SIDR_CUDA(cudaStreamSynchronize(st));
+    return SIDR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sidr_last_error(void) { return g_err.c_str(); }
+
+const char* sidr_status_string(sidr_status s) {
+    switch (s) {
+    case SIDR_OK: return "ok";
+    case SIDR_ERR_INVALID: return "invalid argument";
+    case SIDR_ERR_RULE: return "malformed rule";
+    case SIDR_ERR_TOO_LARGE: return "size limit exceeded";
+    case SIDR_ERR_CUDA: return "CUDA error";
+    case SIDR_ERR_NO_DEVICE: return "no CUDA device";
+    case SIDR_ERR_KERNEL: return "kernel fault";
+    case SIDR_ERR_NONFINITE: return "non-finite input";
+    }
+    return "unknown status";
+}
+
+int sidr_version(void) { return 100; }
+
+int64_t sidr_kernel_launches(void) { return g_launches.load(); }
+
+sidr_status sidr_last_transfer_bytes(int64_t* h2d, int64_t* d2h) {
+    if (h2d) *h2d = g_h2d;
+    if (d2h) *d2h = g_d2h;
+    return SIDR_OK;
+}
+
+sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s) {
+    if (!ops_per_s) return fail(SIDR_ERR_INVALID, "null argument");
+    SIDR_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    SIDR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    double* sink = nullptr;
+    SIDR_CUDA(cudaMalloc(&sink, 1024 * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int iters = 4096, threads = 512, blocks = sms * 4;
+    float best = 1e30f;
+    for (int r = 0; r < (reps < 1 ? 1 : reps) + 1; r++) {
+        cudaEventRecord(e0);
+        fp64_probe_kernel<<<blocks, threads>>>(sink, iters, 1.0000001, 0.9999999);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0 && ms < best) best = ms;  // first run is warm-up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    SIDR_CUDA(cudaGetLastError());
+    // each fused multiply-add is one instruction of the FP64 pipe = one op here
+    const double ops = (double)blocks * threads * iters * 8.0;
+    *ops_per_s = ops / (best * 1e-3);
+    return SIDR_OK;
+}
+
+sidr_status sidr_rules_check(const sidr_rules_desc* r, const int64_t* masks, int32_t mask_group,
+                             int32_t* max_rows) {
+    sidr_status s = check_rules(r);
+    if (s) return s;
+    if (mask_group < 1) return fail(SIDR_ERR_INVALID, "mask_group must be >= 1");
+    if (r->P > 0 && !masks) return fail(SIDR_ERR_INVALID, "mask buffer is null");
+    HostPrograms hp;
+    if (r->P > 0) {
+        s = compile_all(r, masks, mask_group, hp);
+        if (s) return s;
+    }
+    if (max_rows) *max_rows = hp.rows;
+    return SIDR_OK;
+}
+
+sidr_status sidr_zstats(const sidr_instance_desc* d, double zp[10]) {
+    if (!d || !zp) return fail(SIDR_ERR_INVALID, "null argument");
+    HostInstance h;
+    std::string e = build_instance(d->n, d->m, d->tmax, d->scores, d->durations, d->open_t,
+                                   d->close_t, d->dist, d->dist_to_depot, h, false);
+    if (!e.empty()) return fail(e.find("finite") != std::string::npos ? SIDR_ERR_NONFINITE
+                                : (d->n > kMaxN ? SIDR_ERR_TOO_LARGE : SIDR_ERR_INVALID), e);
+    host_zstats(h, zp);
+    return SIDR_OK;
+}
+
+sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], int device,
+                            sidr_ctx** out) {
+    if (!out) return fail(SIDR_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!d || !zp) return fail(SIDR_ERR_INVALID, "null argument");
+    for (int k = 0; k < 10; k++)
+        if (std::isnan(zp[k])) return fail(SIDR_ERR_NONFINITE, "zp holds NaN");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(SIDR_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(SIDR_ERR_INVALID, "device index out of range");
+    sidr_ctx* c = new sidr_ctx();
+    std::string e = build_instance(d->n, d->m, d->tmax, d->scores, d->durations, d->open_t,
+                                   d->close_t, d->dist, d->dist_to_depot, c->h, true);
+    if (!e.empty()) {
+        delete c;
+        return fail(e.find("finite") != std::string::npos ? SIDR_ERR_NONFINITE
+                    : (d->n > kMaxN ? SIDR_ERR_TOO_LARGE : SIDR_ERR_INVALID), e);
+    }
+    c->device = device;
+    auto bail = [&](cudaError_t err, const char* what) {
+        sidr_ctx_destroy(c);
+        return fail(SIDR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+    };
+    cudaError_t err = cudaSetDevice(device);
+    if (err != cudaSuccess) return bail(err, "cudaSetDevice");
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    c->sm_count = v;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    c->smem_optin = (size_t)v;
+    err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) return bail(err, "cudaStreamCreate");
+    auto put = [&](const void* src, size_t bytes, const void** dst) -> cudaError_t {
+        void* p = nullptr;
+        cudaError_t e2 = cudaMalloc(&p, std::max<size_t>(bytes, 8));
+        if (e2 != cudaSuccess) return e2;
+        c->owned.push_back(p);
+        *dst = p;
+        return cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    };
+    const HostInstance& h = c->h;
+    DevInst& I = c->inst;
+    I.n = h.n;
+    I.m = h.m;
+    I.ld = h.n + 1;
+    I.nw = h.nw;
+    I.tmax = h.tmax;
+    struct Item { const void* src; size_t bytes; const void** dst; };
+    const Item items[] = {
+        {h.scores.data(), h.n * 8, (const void**)&I.scores},
+        {h.durations.data(), h.n * 8, (const void**)&I.durations},
+        {h.open_t.data(), h.n * 8, (const void**)&I.open_t},
+        {h.close_t.data(), h.n * 8, (const void**)&I.close_t},
+        {h.d2d.data(), h.n * 8, (const void**)&I.d2d},
+        {h.dist.data(), h.dist.size() * 8, (const void**)&I.dist},
+        {h.F.data(), h.F.size() * 8, (const void**)&I.F},
+        {h.G.data(), h.G.size() * 8, (const void**)&I.G},
+        {h.R.data(), h.R.size() * 8, (const void**)&I.R},
+        {h.P1.data(), h.P1.size() * 8, (const void**)&I.P1},
+        {h.P0.data(), h.P0.size() * 8, (const void**)&I.P0},
+        {h.zlt.data(), h.zlt.size() * 4, (const void**)&I.zlt},
+        {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle},
+        {zp, 80, (const void**)&I.zp},
+    };
+    for (const Item& it : items) {
+        err = put(it.src, it.bytes, it.dst);
+        if (err != cudaSuccess) return bail(err, "instance upload");
+    }
+    *out = c;
+    return SIDR_OK;
+}
+
+void sidr_ctx_destroy(sidr_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    for (void* p : c->owned) cudaFree(p);
+    for (DevBuf* b : {&c->prog, &c->consts, &c->slots, &c->meta, &c->sampled, &c->out, &c->counter,
+                      &c->stats, &c->error})
+        b->release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+sidr_status sidr_evaluate(sidr_ctx* c, const sidr_rules_desc* r, const double* sampled, int32_t N,
+                          const int64_t* term_mask, double* out) {
+    const int P = r ? r->P : 0;
+    return evaluate_common(c, r, sampled, 1, N, P > 0 ? P : 1, P > 0 ? P : 1, term_mask, out);
+}
+
+sidr_status sidr_evaluate_grouped(sidr_ctx* c, const sidr_rules_desc* r,
+                                  const double* grouped_sampled, int32_t G, int32_t T,
+                                  int32_t group_size, const int64_t* term_mask, double* out) {
+    const int P = r ? r->P : 0;
+    return evaluate_common(c, r, grouped_sampled, G, T, group_size, P > 0 ? P : 1, term_mask, out);
+}
+
+sidr_status sidr_evaluate_grouped_masks(sidr_ctx* c, const sidr_rules_desc* r,
+                                        const double* grouped_sampled, int32_t G, int32_t T,
+                                        int32_t group_size, int32_t mask_group,
+                                        const int64_t* masks, double* out) {
+    return evaluate_common(c, r, grouped_sampled, G, T, group_size, mask_group, masks, out);
+}
+
+sidr_status sidr_batch_create(sidr_ctx* c, const sidr_rules_desc* r, const double* sampled,
+                              int32_t G, int32_t T, int32_t group_size, int32_t mask_group,
+                              const int64_t* masks, sidr_batch** out) {
+    if (!out) return fail(SIDR_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!c) return fail(SIDR_ERR_INVALID, "context is null");
+    sidr_status s = check_rules(r);
+    if (s) return s;
+    s = check_grouping(r, sampled, G, T, group_size, mask_group, masks);
+    if (s) return s;
+    const int P = r->P;
+    const int groups_used = P > 0 ? (P - 1) / group_size + 1 : 0;
+    const size_t n_smp = (size_t)groups_used * T * c->h.n;
+    if (P > 0 && T > 0) {
+        s = check_finite(sampled, n_smp);
+        if (s) return s;
+    }
+    HostPrograms hp;
+    if (P > 0) {
+        s = compile_all(r, masks, mask_group, hp);
+        if (s) return s;
+    } else {
+        hp.prog.push_back(0);
+        hp.consts.push_back(0.0);
+        hp.slots.push_back(0);
+    }
+    SIDR_CUDA(cudaSetDevice(c->device));
+    sidr_batch* bt = new sidr_batch();
+    bt->ctx = c;
+    bt->P = P;
+    bt->T = T;
+    bt->G = G;
+    bt->group_size = group_size;
+    auto bail = [&](cudaError_t err, const char* what) {
+        sidr_batch_destroy(bt);
+        return fail(SIDR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+    };
+    cudaStream_t st = c->stream;
+    cudaError_t err;
+    if ((err = upload(bt->prog, hp.prog, st)) != cudaSuccess) return bail(err, "upload programs");
+    if ((err = upload(bt->consts, hp.consts, st)) != cudaSuccess) return bail(err, "upload constants");
+    if ((err = upload(bt->slots, hp.slots, st)) != cudaSuccess) return bail(err, "upload slots");
+    if (!hp.meta.empty() && (err = upload(bt->meta, hp.meta, st)) != cudaSuccess)
+        return bail(err, "upload rule table");
+    if ((err = bt->sampled.ensure(std::max<size_t>(n_smp, 1) * sizeof(double))) != cudaSuccess)
+        return bail(err, "alloc scenarios");
+    if (n_smp && (err = cudaMemcpyAsync(bt->sampled.p, sampled, n_smp * sizeof(double),
+                                        cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return bail(err, "upload scenarios");
+    if ((err = bt->out.ensure(std::max<size_t>((size_t)P * T, 1) * sizeof(double))) != cudaSuccess)
+        return bail(err, "alloc output");
+    if ((err = bt->fit.ensure(std::max<size_t>((size_t)P, 1) * sizeof(double))) != cudaSuccess)
+        return bail(err, "alloc fitness");
+    if ((err = bt->counter.ensure(sizeof(unsigned long long))) != cudaSuccess) return bail(err, "alloc counter");
+    if ((err = bt->stats.ensure(kStats * sizeof(unsigned long long))) != cudaSuccess) return bail(err, "alloc stats");
+    if ((err = bt->error.ensure(sizeof(int))) != cudaSuccess) return bail(err, "alloc error word");
+    if ((err = cudaMemsetAsync(bt->error.p, 0, sizeof(int), st)) != cudaSuccess) return bail(err, "memset");
+    if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return bail(err, "sync");
+    DevBatch& b = bt->b;
+    b.P = P;
+    b.T = T;
+    b.group_size = group_size;
+    b.n = c->h.n;
+    b.prog = (const uint32_t*)bt->prog.p;
+    b.consts = (const double*)bt->consts.p;
+    b.slots = (const uint8_t*)bt->slots.p;
+    b.meta = (const RuleMeta*)bt->meta.p;
+    b.sampled = (const double*)bt->sampled.p;
+    b.out = (double*)bt->out.p;
+    b.counter = (unsigned long long*)bt->counter.p;
+    b.stats = (unsigned long long*)bt->stats.p;
+    b.error = (int*)bt->error.p;
+    b.rows = hp.rows;
+    b.prog_cap = hp.prog_cap;
+    b.const_cap = hp.const_cap;
+    s = plan_launch(c, hp, (long long)P * T, false, bt->grid, bt->block, bt->smem);
+    if (s) {
+        sidr_batch_destroy(bt);
+        return s;
+    }
+    int g2, b2;
+    size_t s2;
+    s = plan_launch(c, hp, (long long)P * T, true, g2, b2, s2);
+    if (s) {
+        sidr_batch_destroy(bt);
+        return s;
+    }
+    *out = bt;
+    return SIDR_OK;
+}
+
+sidr_status sidr_batch_set_counting(sidr_batch* b, int enable) {
+    if (!b) return fail(SIDR_ERR_INVALID, "batch is null");
+    b->counting = enable != 0;
+    return SIDR_OK;
+}
+
+sidr_status sidr_batch_run(sidr_batch* bt, void* stream) {
+    if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
+    SIDR_CUDA(cudaSetDevice(bt->ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : bt->ctx->stream;
+    sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->grid, bt->block, bt->smem, st);
+    if (s) return s;
+    if (bt->P > 0) {
+        fitness_kernel<<<(bt->P + 127) / 128, 128, 0, st>>>(bt->b.out, bt->P, bt->T,
+                                                            (double*)bt->fit.p);
+        SIDR_CUDA(cudaGetLastError());
+        g_launches.fetch_add(1);
+    }
+    bt->ran = true;
+    return SIDR_OK;
+}
+
+sidr_status sidr_batch_read(sidr_batch* bt, double* out) {
+    if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
+    if ((size_t)bt->P * bt->T == 0) return SIDR_OK;
+    if (!out) return fail(SIDR_ERR_INVALID, "output buffer is null");
+    SIDR_CUDA(cudaSetDevice(bt->ctx->device));
+    SIDR_CUDA(cudaDeviceSynchronize());
+    SIDR_CUDA(cudaMemcpy(out, bt->out.p, (size_t)bt->P * bt->T * sizeof(double), cudaMemcpyDeviceToHost));
+    return SIDR_OK;
+}
+
+sidr_status sidr_batch_fitness(sidr_batch* bt, double* fitness) {
+    if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
+    if (bt->P == 0) return SIDR_OK;
+    if (!fitness) return fail(SIDR_ERR_INVALID, "fitness buffer is null");
+    SIDR_CUDA(cudaSetDevice(bt->ctx->device));
+    SIDR_CUDA(cudaDeviceSynchronize());
+    SIDR_CUDA(cudaMemcpy(fitness, bt->fit.p, (size_t)bt->P * sizeof(double), cudaMemcpyDeviceToHost));
+    return SIDR_OK;
+}
+
+const double* sidr_batch_device_out(const sidr_batch* bt) { return bt ? (const double*)bt->out.p : nullptr; }
+
+sidr_status sidr_batch_counts(sidr_batch* bt, sidr_counts* out) {
+    if (!bt || !out) return fail(SIDR_ERR_INVALID, "null argument");
+    unsigned long long v[kStats] = {};
+    SIDR_CUDA(cudaSetDevice(bt->ctx->device));
+    SIDR_CUDA(cudaDeviceSynchronize());
+    SIDR_CUDA(cudaMemcpy(v, bt->stats.p, sizeof v, cudaMemcpyDeviceToHost));
+    out->decisions = (int64_t)v[0];
+    out->candidates = (int64_t)v[1];
+    out->scan_iters = (int64_t)v[2];
+    out->heavy_iters = (int64_t)v[3];
+    out->hop_iters = (int64_t)v[4];
+    out->fp64_ops = (int64_t)v[5];
+    return SIDR_OK;
+}
+
+void sidr_batch_destroy(sidr_batch* bt) {
+    if (!bt) return;
+    cudaSetDevice(bt->ctx->device);
+    cudaDeviceSynchronize();
+    for (DevBuf* b : {&bt->prog, &bt->consts, &bt->slots, &bt->meta, &bt->sampled, &bt->out,
+                      &bt->counter, &bt->stats, &bt->error, &bt->fit})
+        b->release();
+    delete bt;
+}
+
+}  // extern "C"

@@ -1,0 +1,359 @@
+// sidr_host.cpp -- host-side preparation for the evaluator (see sidr_host.hpp).
+// Build with -ffp-contract=off: the tables must reproduce the reference's
+// IEEE operations one by one.
+#include "sidr_host.hpp"
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+namespace sidr {
+
+namespace {
+
+// Monotone map of doubles onto uint64 (total order, -0 just below +0).
+inline uint64_t okey(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+inline double from_okey(uint64_t k) {
+    uint64_t u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    double x;
+    std::memcpy(&x, &u, 8);
+    return x;
+}
+
+// Largest finite double x with pred(x), for a predicate that holds on a
+// down-set; -inf when it holds nowhere.
+template <class Pred>
+double largest_true(Pred pred) {
+    if (!pred(-DBL_MAX)) return -INFINITY;
+    if (pred(DBL_MAX)) return DBL_MAX;
+    uint64_t lo = okey(-DBL_MAX), hi = okey(DBL_MAX);
+    while (hi - lo > 1) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (pred(from_okey(mid))) lo = mid;
+        else hi = mid;
+    }
+    return from_okey(lo);
+}
+
+// The standard and robust neighbour tests of engine/sim_terms.hpp, verbatim in
+// their arithmetic: true when the neighbour can be served after arriving at a.
+struct Tests {
+    const HostInstance& h;
+    bool std_ok(int j, double a) const {
+        if (a > h.close_t[j]) return false;
+        const double st = a > h.open_t[j] ? a : h.open_t[j];
+        return !(st + h.durations[j] + h.d2d[j] > h.tmax);
+    }
+    bool rob_ok(int j, double a) const {
+        if (a > h.close_t[j]) return false;
+        const double st = a > h.open_t[j] ? a : h.open_t[j];
+        return !(st + h.durations[j] * (1.0 + kSigma) + h.d2d[j] > h.tmax);
+    }
+};
+
+inline double D(const HostInstance& h, int a, int b) { return h.dist[(size_t)a * (h.n + 1) + b]; }
+
+// t_reach2 / t_regret / t_eloss_chance at the initial state, for zstats
+// (engine/sim_terms.hpp:95-127, 36-54, 225-257; nothing visited).
+double z_reach2(const HostInstance& h, int i, double fin) {
+    const Tests T{h};
+    double bv = 0.0, fj = 0.0;
+    int bj = -1;
+    for (int j = 0; j < h.n; j++) {
+        if (j == i) continue;
+        const double t = D(h, i + 1, j + 1);
+        if (t < 1e-10) continue;
+        const double a = fin + t;
+        if (!T.std_ok(j, a)) continue;
+        const double v = h.scores[j] / t;
+        if (v > bv) {
+            bv = v;
+            bj = j;
+            const double st = a > h.open_t[j] ? a : h.open_t[j];
+            fj = st + h.durations[j];
+        }
+    }
+    if (bj < 0) return 0.0;
+    double bv2 = 0.0, s2 = 0.0;
+    for (int k = 0; k < h.n; k++) {
+        if (k == i || k == bj) continue;
+        const double t = D(h, bj + 1, k + 1);
+        if (t < 1e-10) continue;
+        if (!T.std_ok(k, fj + t)) continue;
+        const double v = h.scores[k] / t;
+        if (v > bv2) {
+            bv2 = v;
+            s2 = h.scores[k];
+        }
+    }
+    return h.scores[bj] + s2;
+}
+
+double z_regret(const HostInstance& h, int i, double fin) {
+    const Tests T{h};
+    double acc = 0.0;
+    for (int j = 0; j < h.n; j++) {
+        if (j == i) continue;
+        if (!T.std_ok(j, 0.0 + D(h, 0, j + 1))) continue;
+        if (!T.std_ok(j, fin + D(h, i + 1, j + 1))) acc += h.scores[j];
+    }
+    return acc;
+}
+
+double z_atrisk(const HostInstance& h, int c) {
+    const double arr_c = 0.0 + D(h, 0, c + 1);
+    const double st_c = arr_c > h.open_t[c] ? arr_c : h.open_t[c];
+    const double mfin = st_c + h.durations[c];
+    const double sd_c = kSigma * h.durations[c];
+    double acc = 0.0;
+    for (int j = 0; j < h.n; j++) {
+        if (j == c) continue;
+        if (0.0 + D(h, 0, j + 1) > h.close_t[j]) continue;
+        const double marr = mfin + D(h, c + 1, j + 1);
+        double pw;
+        if (sd_c > 1e-9) pw = 0.5 * (1.0 + std::erf(((h.close_t[j] - marr) / sd_c) * 0.7071067811865476));
+        else pw = marr <= h.close_t[j] ? 1.0 : 0.0;
+        double mst, vst;
+        if (marr > h.open_t[j]) {
+            mst = marr;
+            vst = sd_c * sd_c;
+        } else {
+            mst = h.open_t[j];
+            vst = 0.0;
+        }
+        const double sd_j = kSigma * h.durations[j];
+        const double vb = vst + sd_j * sd_j;
+        const double mb = mst + h.durations[j] + h.d2d[j];
+        double pb;
+        if (vb > 1e-18) pb = 0.5 * (1.0 + std::erf(((h.tmax - mb) / std::pow(vb, 0.5)) * 0.7071067811865476));
+        else pb = mb <= h.tmax ? 1.0 : 0.0;
+        acc += h.scores[j] * (1.0 - pw * pb);
+    }
+    return acc;
+}
+
+}  // namespace
+
+std::string build_instance(int n, int m, double tmax, const double* scores,
+                           const double* durations, const double* open_t, const double* close_t,
+                           const double* dist, const double* d2d, HostInstance& h,
+                           bool tables) {
+    if (n < 1 || n > kMaxN) return "n must be in 1..512";
+    if (m < 0 || m > (1 << 20)) return "m must be in 0..2^20";
+    if (!scores || !durations || !open_t || !close_t || !dist || !d2d) return "null instance array";
+    if (!std::isfinite(tmax)) return "tmax is not finite";
+    const int ld = n + 1;
+    h.n = n;
+    h.m = m;
+    h.nw = (n + 31) / 32;
+    h.tmax = tmax;
+    h.scores.assign(scores, scores + n);
+    h.durations.assign(durations, durations + n);
+    h.open_t.assign(open_t, open_t + n);
+    h.close_t.assign(close_t, close_t + n);
+    h.d2d.assign(d2d, d2d + n);
+    h.dist.assign(dist, dist + (size_t)ld * ld);
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(scores[i]) || !std::isfinite(durations[i]) || !std::isfinite(open_t[i]) ||
+            !std::isfinite(close_t[i]) || !std::isfinite(d2d[i]))
+            return "non-finite instance value";
+    for (size_t k = 0; k < h.dist.size(); k++)
+        if (!std::isfinite(h.dist[k])) return "non-finite distance";
+    if (!tables) return "";
+
+    const Tests T{h};
+    const size_t rows = (size_t)ld * n;
+    h.F.assign(rows, 0.0);
+    h.G.assign(rows, 0.0);
+    h.R.assign(rows, 0.0);
+    h.zlt.assign((size_t)ld * h.nw, 0u);
+    h.zle.assign((size_t)ld * h.nw, 0u);
+    for (int o = 0; o < ld; o++) {
+        for (int j = 0; j < n; j++) {
+            const double t = D(h, o, j + 1);
+            h.F[(size_t)o * n + j] = largest_true([&](double f) { return T.std_ok(j, f + t); });
+            h.G[(size_t)o * n + j] = largest_true([&](double f) { return T.rob_ok(j, f + t); });
+            h.R[(size_t)o * n + j] = h.scores[j] / (t > 1e-10 ? t : 1e-10);
+            if (t < 1e-10) h.zlt[(size_t)o * h.nw + (j >> 5)] |= 1u << (j & 31);
+            if (!(t > 1e-10)) h.zle[(size_t)o * h.nw + (j >> 5)] |= 1u << (j & 31);
+        }
+    }
+    h.P1.assign((size_t)n * n, -1.0);
+    h.P0.assign(n, -1.0);
+    for (int j = 0; j < n; j++) {
+        const double sd_j = kSigma * h.durations[j];
+        const double vb0 = 0.0 + sd_j * sd_j;
+        h.P0[j] = vb0 > 1e-18 ? std::pow(vb0, 0.5) : -1.0;
+    }
+    for (int c = 0; c < n; c++) {
+        const double sd_c = kSigma * h.durations[c];
+        const double vs = sd_c * sd_c;
+        for (int j = 0; j < n; j++) {
+            const double sd_j = kSigma * h.durations[j];
+            const double vb = vs + sd_j * sd_j;
+            h.P1[(size_t)c * n + j] = vb > 1e-18 ? std::pow(vb, 0.5) : -1.0;
+        }
+    }
+    return "";
+}
+
+void host_zstats(const HostInstance& h, double zp[10]) {
+    const Tests T{h};
+    double zsum[5] = {0, 0, 0, 0, 0}, zsq[5] = {0, 0, 0, 0, 0};
+    double cnt = 0.0;
+    for (int i = 0; i < h.n; i++) {
+        const double ta = D(h, 0, i + 1);
+        if (!T.std_ok(i, ta)) continue;
+        const double to = h.open_t[i];
+        const double tsv = to > ta ? to : ta;
+        const double fin = tsv + h.durations[i];
+        const double f[5] = {h.close_t[i], z_reach2(h, i, fin), z_regret(h, i, fin), z_atrisk(h, i),
+                             h.d2d[i]};
+        for (int k = 0; k < 5; k++) {
+            zsum[k] += f[k];
+            zsq[k] += f[k] * f[k];
+        }
+        cnt += 1.0;
+    }
+    if (cnt < 1.0) cnt = 1.0;
+    for (int k = 0; k < 5; k++) {
+        const double mean = zsum[k] / cnt;
+        double var = zsq[k] / cnt - mean * mean;
+        if (var < 0.0) var = 0.0;
+        zp[k] = mean;
+        zp[5 + k] = std::sqrt(var) + 1e-9;
+    }
+}
+
+bool slot_active(int s, const int64_t* M) {
+    if (s < 10) return true;
+    if (s == 11) return M[11] || M[33];
+    if (s == 14) return M[14] || M[32];
+    if (s == 30) return M[30] || M[34];
+    return M[s] != 0;
+}
+
+namespace {
+
+// Need bits and deepest REACH-k step for one active slot (the dependencies of
+// terms[] in engine/sim_core.hpp:84-197).
+void slot_needs(int s, uint32_t& need, int& reach_k, uint64_t& explore) {
+    switch (s) {
+    case 10: need |= kNeedNS; break;
+    case 11: case 33: need |= kNeedRegret; break;
+    case 12: need |= kNeedNSRob; break;
+    case 13: need |= kNeedMaxN; break;
+    case 14: case 32: need |= kNeedReach2; break;
+    case 15: need |= kNeedNSTW; break;
+    case 17: case 18: case 19: need |= kNeedStruct; break;
+    case 20: need |= kNeedPBust; break;
+    case 21: need |= kNeedReachK; reach_k = reach_k > 1 ? reach_k : 1; break;
+    case 22: need |= kNeedReachK; reach_k = reach_k > 3 ? reach_k : 3; break;
+    case 23: need |= kNeedReachK; reach_k = 5; break;
+    case 25: case 26: need |= kNeedAgg; break;
+    case 28: case 29: need |= kNeedNS | kNeedStruct; break;
+    case 30: case 34: need |= kNeedAtRisk; break;
+    case 41: need |= kNeedReach2Rob; break;
+    case 43: need |= kNeedReach2Rob | kNeedRegret; break;
+    case 45: need |= kNeedNS | kNeedNSRob; break;
+    case 46: need |= kNeedNSRob; break;
+    case 51: need |= kNeedAgg | kNeedFScore; break;
+    case 52: need |= kNeedAgg | kNeedNFeasRob; break;
+    case 44: case 47: case 48: case 49: case 50: case 53: case 54: case 55: case 56: case 57:
+    case 59: case 60:
+        need |= kNeedExplore;
+        explore |= 1ull << s;
+        break;
+    default: break;
+    }
+}
+
+}  // namespace
+
+std::string compile_rule(const int32_t* ops, const int32_t* args, int len, const int64_t* M,
+                         CompiledRule& out) {
+    out = CompiledRule();
+    if (len < 1) return "empty rule";
+    if (len > kMaxTree) return "rule longer than MAX_TREE (1024)";
+    // Pass 1: stack discipline and the set of active slots read.
+    int sp = 0, maxsp = 0;
+    int slot_row[kTerms];
+    for (int s = 0; s < kTerms; s++) slot_row[s] = -1;
+    for (int k = 0; k < len; k++) {
+        const int o = ops[k];
+        if (o == -1) {
+            const int s = args[2 * k];
+            if (s < 0 || s >= kTerms) return "terminal slot out of range 0..60";
+            if (slot_active(s, M) && !(s >= 36 && s <= 40) && slot_row[s] < 0) {
+                slot_row[s] = out.K++;
+                out.slots.push_back((uint8_t)s);
+            }
+            sp++;
+        } else if (o == -2) {
+            sp++;
+        } else if (o >= 0 && o <= 6) {
+            if (sp < 2) return "operator with fewer than two operands";
+            sp--;
+        } else {
+            return "unknown opcode";
+        }
+        if (sp > maxsp) maxsp = sp;
+        if (sp > kMaxStack) return "stack deeper than MAX_STACK (32)";
+    }
+    if (sp != 1) return "rule leaves more than one value";
+    // Needs of the slots read.
+    for (int s : out.slots) slot_needs(s, out.need, out.reach_k, out.explore);
+    // Pass 2: three-address code.  Operand descriptors: row index, or
+    // kOpConst | constant index.
+    std::map<uint64_t, int> cidx;
+    auto konst = [&](double v) -> uint32_t {
+        uint64_t u;
+        std::memcpy(&u, &v, 8);
+        auto it = cidx.find(u);
+        if (it != cidx.end()) return kOpConst | (uint32_t)it->second;
+        const int c = (int)out.consts.size();
+        cidx[u] = c;
+        out.consts.push_back(v);
+        return kOpConst | (uint32_t)c;
+    };
+    std::vector<uint32_t> st;
+    st.reserve(kMaxStack);
+    int maxtemp = 0;
+    for (int k = 0; k < len; k++) {
+        const int o = ops[k];
+        if (o == -1) {
+            const int s = args[2 * k];
+            if (!slot_active(s, M)) st.push_back(konst(0.0));
+            else if (s >= 36 && s <= 40) {
+                // C1..C5: the literals of terms[36..40] (engine/sim_core.hpp:152-156)
+                static const double kC[5] = {0.1, 0.2, 0.3, 0.4, 0.5};
+                st.push_back(konst(kC[s - 36]));
+            }
+            else st.push_back((uint32_t)slot_row[s]);
+        } else if (o == -2) {
+            st.push_back(konst(args[2 * k] / 1000.0));
+        } else {
+            const uint32_t b = st.back();
+            st.pop_back();
+            const uint32_t a = st.back();
+            st.pop_back();
+            const int pos = (int)st.size();  // result stack position
+            const uint32_t dst = (uint32_t)(out.K + pos);
+            if (pos + 1 > maxtemp) maxtemp = pos + 1;
+            out.prog.push_back((uint32_t)o | (a << 3) | (b << 13) | (dst << 23));
+            st.push_back(dst);
+        }
+    }
+    out.D = maxtemp;
+    out.res = (int)st.back();
+    if (out.consts.size() > 511) return "more than 511 distinct constants";
+    (void)maxsp;
+    return "";
+}
+
+}  // namespace sidr

@@ -1,0 +1,118 @@
+// sidr_internal.hpp -- shared host/device definitions of the evaluator.
+//
+// Device-side layout of one instance (built once per context) and of one
+// batch of rules x scenarios (built per evaluate call or per sidr_batch).
+#pragma once
+#include <cstdint>
+
+namespace sidr {
+
+constexpr int kTerms = 61;     // engine/vocab.hpp:16
+constexpr int kMaxN = 512;     // engine/vocab.hpp:17
+constexpr int kMaxTree = 1024; // engine/vocab.hpp:18
+constexpr int kMaxStack = 32;  // engine/vocab.hpp:19
+constexpr int kMaxWords = kMaxN / 32;
+constexpr double kSigma = 0.2;                // SIM_SIGMA, engine/sim_terms.hpp:15
+constexpr double kSqrt2 = 1.4142135623730951; // SQRT2_C, engine/sim_terms.hpp:16
+
+// ----------------------------------------------------------------- instance
+//
+// Besides the SimData arrays the context keeps lookup tables that turn the
+// reference's per-neighbour feasibility arithmetic into one comparison.  For
+// origin node o (0 = depot, i+1 = customer i) and customer j, with
+// t = dist[o][j+1]:
+//
+//   F[o*n + j] = the largest double f such that the reference's standard test
+//                (arrive = f + t; arrive <= close_j; start = max(arrive, open_j);
+//                 start + dur_j + d2d_j <= tmax) passes, or -inf if none does.
+//                Every operation in that chain is IEEE round-to-nearest and
+//                monotone in f, so the test passes exactly when f <= F.
+//   G[o*n + j] = the same for the robust test (service time * (1 + SIM_SIGMA)).
+//   R[o*n + j] = scores[j] / (t > 1e-10 ? t : 1e-10): the score-per-time ratio
+//                every neighbour scan divides out (same operands, same IEEE
+//                division as the reference).
+//   zlt / zle  = per origin row, bit j set when t < 1e-10 / !(t > 1e-10):
+//                the coincident-location skips of the NS family and of the
+//                structural best-neighbour search.
+//   P1[c*n + j], P0[j] = pow(var, 0.5) of ATRISK's two variance cases
+//                (var = (0.2 d_c)^2 + (0.2 d_j)^2, or 0 + (0.2 d_j)^2),
+//                precomputed on the host with the reference's libm; -1 when
+//                var <= 1e-18 (the reference's deterministic branch).
+struct DevInst {
+    int n, m, ld, nw;
+    double tmax;
+    const double *scores, *durations, *open_t, *close_t, *d2d, *dist;
+    const double *F, *G, *R, *P1, *P0;
+    const uint32_t *zlt, *zle;
+    const double* zp;  // [10]
+};
+
+// ------------------------------------------------------------ rule programs
+//
+// Each postfix rule is compiled on the host into three-address instructions
+// over per-lane value rows held in shared memory: rows [0, K) hold the rule's
+// terminals (only the slots it reads), rows [K, K+D) its stack temporaries.
+// An operand is 10 bits: bit 9 set = constant-pool index, else a row.
+//   word = op | a << 3 | b << 13 | dst << 23
+constexpr uint32_t kOpConst = 512u;
+
+enum NeedBits : uint32_t {
+    kNeedNS = 1u << 0,       // NS value (slots 10, 28, 29)
+    kNeedRegret = 1u << 1,   // 11 (33, 43)
+    kNeedNSRob = 1u << 2,    // 12 (45, 46)
+    kNeedMaxN = 1u << 3,     // 13
+    kNeedReach2 = 1u << 4,   // 14 (32)
+    kNeedNSTW = 1u << 5,     // 15
+    kNeedStruct = 1u << 6,   // 17-19, 28, 29 (FRAGCNT, FRAGSCORE, DOWNSLACK)
+    kNeedPBust = 1u << 7,    // 20
+    kNeedReachK = 1u << 8,   // 21-23 (steps in reach_k)
+    kNeedAtRisk = 1u << 9,   // 30 (34)
+    kNeedReach2Rob = 1u << 10, // 41 (43)
+    kNeedAgg = 1u << 11,     // VFRAC, NFEAS (25, 26)
+    kNeedFScore = 1u << 12,  // FEASCORE (51)
+    kNeedNFeasRob = 1u << 13, // NFEASROB (52)
+    kNeedExplore = 1u << 14, // slots computed by the direct per-lane path
+    kNeedNSFused = kNeedNS | kNeedMaxN | kNeedReach2 | kNeedNSTW,
+    kNeedRob = kNeedNSRob | kNeedReach2Rob,
+    kNeedAfterC = kNeedStruct | kNeedPBust | kNeedReachK,
+};
+
+// Counters of the counting instantiation: decisions, candidates, fused-scan
+// neighbours, ATRISK neighbours, second-hop/REACH-step neighbours, op model.
+constexpr int kStats = 6;
+// Op-model constants (see sidr_counts in include/sidr.h).
+constexpr int kOpsTest = 7;       // one neighbour feasibility test incl. the skip
+constexpr int kOpsAtRisk = 40;    // ATRISK neighbour: 2 div, 2 erf (15 each), 8 more
+constexpr int kOpsHop = 8;        // second-hop / REACH-k step neighbour
+constexpr int kOpsCandidate = 12; // candidate setup (ta .. sd_c)
+
+struct RuleMeta {
+    int32_t prog_off;   // first instruction word
+    int32_t const_off;  // first constant
+    int32_t slot_off;   // first compact-slot byte
+    int16_t n_ins;      // instructions
+    int16_t n_const;    // constants
+    int16_t K;          // terminal rows
+    int16_t D;          // temporary rows
+    int16_t res;        // result operand
+    int8_t reach_k;     // deepest REACH-k step needed (0, 1, 3, 5)
+    uint16_t scan_ops;  // op-model cost of one fused-scan neighbour (counting only)
+    uint32_t need;      // NeedBits
+    uint64_t explore;   // bit s set: exploration slot s is read
+};
+
+struct DevBatch {
+    int P, T, group_size, n;
+    const uint32_t* prog;
+    const double* consts;
+    const uint8_t* slots;
+    const RuleMeta* meta;
+    const double* sampled;  // [G][T][n]
+    double* out;            // [P][T]
+    unsigned long long* counter;  // work-queue head
+    unsigned long long* stats;    // [kStats] counters (may be null)
+    int* error;                   // kernel error word
+    int rows, prog_cap, const_cap;  // per-warp shared-memory sizing
+};
+
+}  // namespace sidr

@@ -1,0 +1,861 @@
+// sidr_kernel.cuh -- the B200 rule x scenario evaluator kernel.
+//
+// Mapping (one persistent launch):
+//   * one warp simulates one (rule, scenario) pair at a time and pulls the
+//     next pair from a global work queue (pairs ordered rule-major, so a warp
+//     usually keeps its rule's program staged in shared memory);
+//   * at each decision point (engine/sim_core.hpp:43-204, pick_best) the warp
+//     builds the feasible-candidate bitmask with one ballot per 32 customers,
+//     compacts it, and spreads the candidates over its lanes, 32 per round;
+//   * each lane computes its candidate's terminals with fused neighbour scans
+//     (every terminal's sum still runs over j in ascending order, so each
+//     accumulator sees the reference's operation sequence), evaluates the rule
+//     program from shared memory, and the warp picks the best candidate with
+//     shuffles (strict >, lowest index on ties, NaN -> -1e300: :199-201);
+//   * the route state (visited bitmask, position, clock, collected score) is
+//     warp-uniform; the rollout order is sim_one's (:207-238).
+//
+// Bit-exactness: compiled with -fmad=false; every floating-point expression
+// keeps the reference's operand order.  The lookup tables of DevInst replace
+// only comparisons whose outcome they reproduce exactly (see sidr_internal.hpp)
+// and divisions with identical operands.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "sidr_internal.hpp"
+
+namespace sidr {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Shared-memory slice of one warp.
+struct WarpSmem {
+    double* rows;      // [rows][32]
+    double* cst;       // [const_cap]
+    uint32_t* prog;    // [prog_cap]
+    int16_t* cand;     // [kMaxN]
+    uint32_t* unv;     // [kMaxWords] unvisited customers
+    uint32_t* feas;    // [kMaxWords] feasible-now & unvisited
+    uint32_t* atr;     // [kMaxWords] ATRISK's arrive-by-close filter
+    uint8_t* slots;    // [64] compact row -> terminal slot
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+__host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int prog_cap) {
+    size_t b = (size_t)rows * 32 * sizeof(double);
+    b += (size_t)const_cap * sizeof(double);
+    b += align_up((size_t)prog_cap * sizeof(uint32_t), 8);
+    b += (size_t)kMaxN * sizeof(int16_t);
+    b += 3 * kMaxWords * sizeof(uint32_t);
+    b += 64;
+    return align_up(b, 16);
+}
+
+__device__ __forceinline__ WarpSmem carve(unsigned char* base, int rows, int const_cap,
+                                          int prog_cap) {
+    WarpSmem s;
+    s.rows = reinterpret_cast<double*>(base);
+    s.cst = s.rows + (size_t)rows * 32;
+    s.prog = reinterpret_cast<uint32_t*>(s.cst + const_cap);
+    s.cand = reinterpret_cast<int16_t*>(
+        reinterpret_cast<unsigned char*>(s.prog) + align_up((size_t)prog_cap * 4, 8));
+    s.unv = reinterpret_cast<uint32_t*>(s.cand + kMaxN);
+    s.feas = s.unv + kMaxWords;
+    s.atr = s.feas + kMaxWords;
+    s.slots = reinterpret_cast<uint8_t*>(s.atr + kMaxWords);
+    return s;
+}
+
+// ------------------------------------------------------------ small helpers
+
+__device__ __forceinline__ double sel_max(double a, double b) { return a > b ? a : b; }
+
+// The reference's standard neighbour test, evaluated directly
+// (engine/sim_terms.hpp loop bodies); used by the exploration terminals.
+__device__ __forceinline__ bool fits_std(const DevInst& I, int j, double arrive) {
+    if (arrive > I.close_t[j]) return false;
+    const double st = arrive > I.open_t[j] ? arrive : I.open_t[j];
+    return !(st + I.durations[j] + I.d2d[j] > I.tmax);
+}
+
+__device__ __forceinline__ bool fits_scaled(const DevInst& I, int j, double arrive, double mul) {
+    if (arrive > I.close_t[j]) return false;
+    const double st = arrive > I.open_t[j] ? arrive : I.open_t[j];
+    return !(st + I.durations[j] * mul + I.d2d[j] > I.tmax);
+}
+
+__device__ __forceinline__ bool is_unvisited(const WarpSmem& S, int j) {
+    return (S.unv[j >> 5] >> (j & 31)) & 1u;
+}
+
+__device__ __forceinline__ uint32_t bit_in_word(int node, int w) {
+    return (node >= 0 && (node >> 5) == w) ? (1u << (node & 31)) : 0u;
+}
+
+// Best neighbour by score/time from origin row o at time tm over unvisited
+// customers outside {x0..x4}: `table` is F (standard) or G (robust).  init 0.0
+// and the coincident skip reproduce REACH2's second loop
+// (engine/sim_terms.hpp:112-126, :175-189); returns the chosen customer's score
+// or 0.0.
+template <bool COUNT>
+__device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const double* table,
+                                   int o, double tm, int x0, int x1, unsigned long long& hops) {
+    const int n = I.n;
+    const double* To = table + (size_t)o * n;
+    const double* Ro = I.R + (size_t)o * n;
+    const uint32_t* zo = I.zlt + (size_t)o * I.nw;
+    double bv = 0.0, bs = 0.0;
+    for (int w = 0; w < I.nw; w++) {
+        uint32_t bits = S.unv[w] & ~(bit_in_word(x0, w) | bit_in_word(x1, w) | zo[w]);
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int j = (w << 5) + b;
+            if (COUNT) hops++;
+            if (tm <= To[j]) {
+                const double v = Ro[j];
+                if (v > bv) {
+                    bv = v;
+                    bs = I.scores[j];
+                }
+            }
+        }
+    }
+    return bs;
+}
+
+// One REACH-k greedy step (engine/sim_terms.hpp:415-431): best unvisited
+// customer outside the path by score/max(t,1e-10) under the standard test, no
+// coincident skip, init -1.0.
+template <bool COUNT>
+__device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm, const int* path,
+                          int np, unsigned long long& hops) {
+    const int n = I.n;
+    const double* Fo = I.F + (size_t)o * n;
+    const double* Ro = I.R + (size_t)o * n;
+    double bv = -1.0;
+    int bq = -1;
+    for (int w = 0; w < I.nw; w++) {
+        uint32_t ex = 0;
+#pragma unroll
+        for (int k = 0; k < 5; k++)
+            if (k < np) ex |= bit_in_word(path[k], w);
+        uint32_t bits = S.unv[w] & ~ex;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int j = (w << 5) + b;
+            if (COUNT) hops++;
+            if (tm <= Fo[j]) {
+                const double v = Ro[j];
+                if (v > bv) {
+                    bv = v;
+                    bq = j;
+                }
+            }
+        }
+    }
+    return bq;
+}
+
+// ------------------------------------------------- exploration terminals
+// Direct restatements for the slots outside the 29-terminal menu
+// (engine/sim_terms.hpp:129-154, 259-401, 443-519).  They read the instance
+// arrays straight, like the reference, and are used only when a mask enables
+// them.
+
+__device__ double x_skiploss(const DevInst& I, const WarpSmem& S, int i, int cur, double ct) {
+    const int ld = I.ld;
+    double bv = 0.0, fq = 0.0;
+    int bq = -1;
+    for (int q = 0; q < I.n; q++) {
+        if (q == i || !is_unvisited(S, q)) continue;
+        const double t = I.dist[(size_t)cur * ld + q + 1];
+        if (t < 1e-10) continue;
+        const double arrive = ct + t;
+        if (arrive > I.close_t[q]) continue;
+        const double st = arrive > I.open_t[q] ? arrive : I.open_t[q];
+        if (st + I.durations[q] + I.d2d[q] > I.tmax) continue;
+        const double v = I.scores[q] / t;
+        if (v > bv) {
+            bv = v;
+            bq = q;
+            fq = st + I.durations[q];
+        }
+    }
+    if (bq < 0) return 0.0;
+    const double ai = fq + I.dist[(size_t)(bq + 1) * ld + i + 1];
+    if (ai > I.close_t[i]) return I.scores[i];
+    const double si = ai > I.open_t[i] ? ai : I.open_t[i];
+    if (si + I.durations[i] + I.d2d[i] > I.tmax) return I.scores[i];
+    return 0.0;
+}
+
+__device__ double x_reach_k_rob(const DevInst& I, const WarpSmem& S, int c, double fin_rob_c,
+                                int K) {
+    const int ld = I.ld;
+    int path[6] = {c, -1, -1, -1, -1, -1};
+    int at = c + 1;
+    double tm = fin_rob_c, tot = 0.0;
+    for (int step = 0; step < K; step++) {
+        int best = -1;
+        double bv = -1.0;
+        for (int q = 0; q < I.n; q++) {
+            if (!is_unvisited(S, q)) continue;
+            bool on = false;
+#pragma unroll
+            for (int k = 0; k < 6; k++) on |= (path[k] == q);
+            if (on) continue;
+            const double ta = I.dist[(size_t)at * ld + q + 1];
+            if (!fits_scaled(I, q, tm + ta, 1.0 + kSigma)) continue;
+            const double tt = ta > 1e-10 ? ta : 1e-10;
+            const double v = I.scores[q] / tt;
+            if (v > bv) {
+                bv = v;
+                best = q;
+            }
+        }
+        if (best < 0) break;
+        const double arrive = tm + I.dist[(size_t)at * ld + best + 1];
+        const double st = arrive > I.open_t[best] ? arrive : I.open_t[best];
+        tm = st + I.durations[best] * (1.0 + kSigma);
+        at = best + 1;
+        tot += I.scores[best];
+        path[step + 1] = best;
+    }
+    return tot;
+}
+
+__device__ double x_ns_family(const DevInst& I, const WarpSmem& S, int i, double fin, int kind) {
+    // kind 0: NSA2 score/t^2, 1: NSA05 score/sqrt(t), 2: NNFWD, 3: NNK3, 4: SCORERANK
+    const int ld = I.ld;
+    double acc = 0.0, d1 = -1.0, d2 = -1.0, d3 = -1.0, below = 0.0, tot = 0.0;
+    for (int j = 0; j < I.n; j++) {
+        if (j == i || !is_unvisited(S, j)) continue;
+        const double t = I.dist[(size_t)(i + 1) * ld + j + 1];
+        if (t < 1e-10) continue;
+        if (!fits_std(I, j, fin + t)) continue;
+        if (kind == 0) acc += I.scores[j] / (t * t);
+        else if (kind == 1) acc += I.scores[j] / sqrt(t);
+        else if (kind == 2) {
+            if (d1 < 0.0 || t < d1) d1 = t;
+        } else if (kind == 3) {
+            if (d1 < 0.0 || t < d1) {
+                d3 = d2;
+                d2 = d1;
+                d1 = t;
+            } else if (d2 < 0.0 || t < d2) {
+                d3 = d2;
+                d2 = t;
+            } else if (d3 < 0.0 || t < d3) {
+                d3 = t;
+            }
+        } else {
+            tot += 1.0;
+            if (I.scores[j] < I.scores[i]) below += 1.0;
+        }
+    }
+    if (kind <= 1) return acc;
+    if (kind == 2) return d1 < 0.0 ? 0.0 : 1.0 / (1.0 + d1);
+    if (kind == 3) {
+        if (d1 < 0.0) return 0.0;
+        double s = d1, k = 1.0;
+        if (d2 >= 0.0) {
+            s += d2;
+            k += 1.0;
+        }
+        if (d3 >= 0.0) {
+            s += d3;
+            k += 1.0;
+        }
+        return 1.0 / (1.0 + s / k);
+    }
+    if (tot == 0.0) return 1.0;
+    return below / tot;
+}
+
+__device__ double x_ns_rob_m(const DevInst& I, const WarpSmem& S, int i, double fin, double m) {
+    const int ld = I.ld;
+    const double ms = m * kSigma;
+    const double frob = fin + I.durations[i] * ms;
+    double acc = 0.0;
+    for (int j = 0; j < I.n; j++) {
+        if (j == i || !is_unvisited(S, j)) continue;
+        const double t = I.dist[(size_t)(i + 1) * ld + j + 1];
+        if (t < 1e-10) continue;
+        if (!fits_scaled(I, j, frob + t, 1.0 + ms)) continue;
+        acc += I.scores[j] / t;
+    }
+    return acc;
+}
+
+__device__ double x_nnchain(const DevInst& I, const WarpSmem& S, int c, double fin_c, int K) {
+    const int ld = I.ld;
+    int path[4] = {c, -1, -1, -1};
+    int at = c + 1, done = 0;
+    double tm = fin_c, tot = 0.0;
+    for (int step = 0; step < K; step++) {
+        int best = -1;
+        double bd = -1.0;
+        for (int q = 0; q < I.n; q++) {
+            if (!is_unvisited(S, q)) continue;
+            bool on = false;
+#pragma unroll
+            for (int k = 0; k < 4; k++) on |= (path[k] == q);
+            if (on) continue;
+            const double ta = I.dist[(size_t)at * ld + q + 1];
+            if (ta < 1e-10) continue;
+            if (!fits_std(I, q, tm + ta)) continue;
+            if (bd < 0.0 || ta < bd) {
+                bd = ta;
+                best = q;
+            }
+        }
+        if (best < 0) break;
+        const double arrive = tm + bd;
+        const double st = arrive > I.open_t[best] ? arrive : I.open_t[best];
+        tm = st + I.durations[best];
+        at = best + 1;
+        tot += bd;
+        done++;
+        if (step + 1 < 4) path[step + 1] = best;
+    }
+    if (done == 0) return 0.0;
+    return 1.0 / (1.0 + tot / done);
+}
+
+__device__ double x_detour(const DevInst& I, const WarpSmem& S, int i, int cur, double fin,
+                           double ta_i) {
+    const int ld = I.ld;
+    double tot = 0.0, cnt = 0.0;
+    for (int j = 0; j < I.n; j++) {
+        if (j == i || !is_unvisited(S, j)) continue;
+        const double t = I.dist[(size_t)(i + 1) * ld + j + 1];
+        if (t < 1e-10) continue;
+        if (!fits_std(I, j, fin + t)) continue;
+        tot += ta_i + t - I.dist[(size_t)cur * ld + j + 1];
+        cnt += 1.0;
+    }
+    if (cnt == 0.0) return 0.0;
+    return tot / cnt;
+}
+
+__device__ __forceinline__ double t_rand_dev(int i) {
+    long long x = (((long long)i + 1) * 1103515245LL + 12345LL) & 0x7FFFFFFFLL;
+    x = (x * 1103515245LL + 12345LL) & 0x7FFFFFFFLL;
+    return (double)(x % 100000LL) / 1000.0;
+}
+
+// -------------------------------------------------------- decision context
+
+struct Decision {
+    int cur, remaining;
+    double ct, sat, vfrac, nfeas, fscore, nfeasrob;
+};
+
+// Counters of one warp (COUNT instantiation only).
+struct WarpCounts {
+    unsigned long long dec, cand, scan, heavy, hop, ops;
+};
+
+// Terminals of candidate i into the lane's value rows, then the rule program.
+// Returns the priority (NaN mapped to -1e300).
+template <bool COUNT>
+__device__ double score_candidate(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
+                                  const Decision& d, int i, WarpCounts& wc) {
+    const int lane = threadIdx.x & 31;
+    const int n = I.n, ld = I.ld;
+    const uint32_t need = rm.need;
+    const double tmax = I.tmax;
+    const double ct = d.ct;
+    const int cur = d.cur;
+
+    const double ta = I.dist[(size_t)cur * ld + i + 1];
+    const double open_i = I.open_t[i], close_i = I.close_t[i];
+    const double dur_i = I.durations[i], sc_i = I.scores[i], d2d_i = I.d2d[i];
+    const double to = open_i - ct;
+    const double tc = close_i - ct;
+    const double tsv = to > ta ? to : ta;
+    const double tfv = tsv + dur_i;
+    const double fin = ct + tfv;                 // finish_i of the NS family
+    const double arr_c = ct + ta;
+    const double st_c = arr_c > open_i ? arr_c : open_i;
+    const double fin_c = st_c + dur_i;           // finish_c of the cascade family
+    const double frob = fin + dur_i * kSigma;    // robust finish
+    const double sd_c = kSigma * dur_i;
+    if (COUNT) wc.ops += kOpsCandidate + rm.n_ins;
+
+    double ns = 0.0, maxn = 0.0, r2v = 0.0, nstw = 0.0, regret = 0.0, nsrob = 0.0, r2rv = 0.0;
+    double fcnt = 0.0, fsc = 0.0, smin = 1e18, sbv = -1.0, k1v = -1.0, eloss = 0.0;
+    int r2j = -1, r2rj = -1, sbq = -1, k1q = -1;
+
+    const uint32_t fused = kNeedNSFused | kNeedRegret | kNeedRob | kNeedAfterC | kNeedAtRisk;
+    if (need & fused) {
+        const double* Fi = I.F + (size_t)(i + 1) * n;
+        const double* Gi = I.G + (size_t)(i + 1) * n;
+        const double* Ri = I.R + (size_t)(i + 1) * n;
+        const double* Di = I.dist + (size_t)(i + 1) * ld + 1;
+        const double* P1i = I.P1 + (size_t)i * n;
+        const uint32_t* zlti = I.zlt + (size_t)(i + 1) * I.nw;
+        const uint32_t* zlei = I.zle + (size_t)(i + 1) * I.nw;
+        unsigned long long scan = 0, heavy = 0;
+        for (int w = 0; w < I.nw; w++) {
+            uint32_t bits = S.unv[w];
+            if (!bits) continue;
+            const uint32_t self = bit_in_word(i, w);
+            const uint32_t zl = zlti[w], ze = zlei[w];
+            const uint32_t nowb = S.feas[w];
+            const uint32_t atb = S.atr[w];
+            do {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                if ((self >> b) & 1u) continue;
+                const int j = (w << 5) + b;
+                if (COUNT) scan++;
+                const double Fj = Fi[j];
+                const double sj = I.scores[j];
+                const bool nz = !((zl >> b) & 1u);
+                const bool fa = fin <= Fj;
+                if (need & kNeedNSFused) {
+                    if (fa && nz) {
+                        const double Rj = Ri[j];
+                        ns += Rj;
+                        if (Rj > maxn) maxn = Rj;
+                        if (Rj > r2v) {
+                            r2v = Rj;
+                            r2j = j;
+                        }
+                        if (need & kNeedNSTW) {
+                            const double arrive = fin + Di[j];
+                            double wait = I.open_t[j] - arrive;
+                            if (wait < 0.0) wait = 0.0;
+                            const double win = I.close_t[j] - I.open_t[j];
+                            double wt = win > 1e-10 ? 1.0 - wait / win : 1.0;
+                            if (wt < 0.0) wt = 0.0;
+                            nstw += Rj * wt;
+                        }
+                    }
+                }
+                if (need & kNeedRegret) {
+                    if (((nowb >> b) & 1u) && !fa) regret += sj;
+                }
+                if (need & kNeedRob) {
+                    if (nz && frob <= Gi[j]) {
+                        const double Rj = Ri[j];
+                        nsrob += Rj;
+                        if (Rj > r2rv) {
+                            r2rv = Rj;
+                            r2rj = j;
+                        }
+                    }
+                }
+                if (need & kNeedAfterC) {
+                    const bool fc = fin_c <= Fj;
+                    if ((need & kNeedStruct) && ((nowb >> b) & 1u) && !fc) {
+                        fcnt += 1.0;
+                        fsc += sj;
+                    }
+                    if (fc) {
+                        if (need & (kNeedStruct | kNeedPBust)) {
+                            const double aq = fin_c + Di[j];
+                            const double slack = I.close_t[j] - aq;
+                            if (slack < smin) smin = slack;
+                            if (!((ze >> b) & 1u)) {
+                                const double v = Ri[j];
+                                if (v > sbv) {
+                                    sbv = v;
+                                    sbq = j;
+                                }
+                            }
+                        }
+                        if (need & kNeedReachK) {
+                            const double v = Ri[j];
+                            if (v > k1v) {
+                                k1v = v;
+                                k1q = j;
+                            }
+                        }
+                    }
+                }
+                if (need & kNeedAtRisk) {
+                    if ((atb >> b) & 1u) {
+                        if (COUNT) heavy++;
+                        const double cj = I.close_t[j], oj = I.open_t[j];
+                        const double marr = fin_c + Di[j];
+                        double pw;
+                        if (sd_c > 1e-9) pw = 0.5 * (1.0 + erf(((cj - marr) / sd_c) * 0.7071067811865476));
+                        else pw = marr <= cj ? 1.0 : 0.0;
+                        double mst, pv;
+                        if (marr > oj) {
+                            mst = marr;
+                            pv = P1i[j];
+                        } else {
+                            mst = oj;
+                            pv = I.P0[j];
+                        }
+                        const double mb = mst + I.durations[j] + I.d2d[j];
+                        double pb;
+                        if (pv >= 0.0) pb = 0.5 * (1.0 + erf(((tmax - mb) / pv) * 0.7071067811865476));
+                        else pb = mb <= tmax ? 1.0 : 0.0;
+                        eloss += sj * (1.0 - pw * pb);
+                    }
+                }
+            } while (bits);
+        }
+        if (COUNT) {
+            wc.scan += scan;
+            wc.heavy += heavy;
+            wc.ops += scan * rm.scan_ops + heavy * kOpsAtRisk;
+        }
+    }
+
+    // REACH2 / REACH2ROB second hops.
+    double reach2 = 0.0, reach2rob = 0.0;
+    if ((need & kNeedReach2) && r2j >= 0) {
+        const double arrive = fin + I.dist[(size_t)(i + 1) * ld + r2j + 1];
+        const double st = arrive > I.open_t[r2j] ? arrive : I.open_t[r2j];
+        const double fj = st + I.durations[r2j];
+        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.F, r2j + 1, fj, i, r2j, wc.hop);
+    }
+    if ((need & kNeedReach2Rob) && r2rj >= 0) {
+        const double arrive = frob + I.dist[(size_t)(i + 1) * ld + r2rj + 1];
+        const double st = arrive > I.open_t[r2rj] ? arrive : I.open_t[r2rj];
+        const double fj = st + I.durations[r2rj] * (1.0 + kSigma);
+        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.G, r2rj + 1, fj, i, r2rj, wc.hop);
+    }
+
+    // REACH-1/3/5 share one greedy path (each is the running total after
+    // 1, 3 or 5 steps of the same walk, engine/sim_terms.hpp:405-441).
+    double rk1 = 0.0, rk3 = 0.0, rk5 = 0.0;
+    if (need & kNeedReachK) {
+        int path[5] = {i, -1, -1, -1, -1};
+        double tot = 0.0, tm = 0.0;
+        int at = 0;
+        bool alive = k1q >= 0;
+        if (alive) {
+            const double arrive = fin_c + I.dist[(size_t)(i + 1) * ld + k1q + 1];
+            const double st = arrive > I.open_t[k1q] ? arrive : I.open_t[k1q];
+            tm = st + I.durations[k1q];
+            at = k1q + 1;
+            tot += I.scores[k1q];
+            path[1] = k1q;
+        }
+        rk1 = tot;
+        for (int step = 2; step <= rm.reach_k; step++) {
+            if (alive) {
+                const int bq = reach_step<COUNT>(I, S, at, tm, path, step, wc.hop);
+                if (bq < 0) {
+                    alive = false;
+                } else {
+                    const double arrive = tm + I.dist[(size_t)at * ld + bq + 1];
+                    const double st = arrive > I.open_t[bq] ? arrive : I.open_t[bq];
+                    tm = st + I.durations[bq];
+                    at = bq + 1;
+                    tot += I.scores[bq];
+                    if (step < 5) path[step] = bq;
+                }
+            }
+            if (step == 3) rk3 = tot;
+            if (step == 5) rk5 = tot;
+        }
+    }
+
+    double pbust = 0.0;
+    if ((need & kNeedPBust) && sbq >= 0) {
+        const double ab = fin_c + I.dist[(size_t)(i + 1) * ld + sbq + 1];
+        const double sd = kSigma * dur_i;
+        if (sd > 1e-12) {
+            const double z = (I.close_t[sbq] - ab) / (sd * kSqrt2);
+            pbust = 0.5 * erfc(z);
+        } else {
+            pbust = ab > I.close_t[sbq] ? 1.0 : 0.0;
+        }
+    }
+    const double downslack = smin > 1e17 ? 0.0 : smin;
+
+    // Terminal rows.
+    for (int k = 0; k < rm.K; k++) {
+        const int slot = S.slots[k];
+        double v;
+        switch (slot) {
+        case 0: v = sc_i; break;
+        case 1: v = dur_i; break;
+        case 2: v = to; break;
+        case 3: v = tc; break;
+        case 4: v = ta; break;
+        case 5: v = d2d_i; break;
+        case 6: v = tsv; break;
+        case 7: v = tfv; break;
+        case 8: v = tc - ta; break;
+        case 9: v = d.remaining * tmax + (tmax - ct); break;
+        case 10: v = ns; break;
+        case 11: v = regret; break;
+        case 12: v = nsrob; break;
+        case 13: v = maxn; break;
+        case 14: v = reach2; break;
+        case 15: v = nstw; break;
+        case 16: v = t_rand_dev(i); break;
+        case 17: v = fcnt; break;
+        case 18: v = fsc; break;
+        case 19: v = downslack; break;
+        case 20: v = pbust; break;
+        case 21: v = rk1; break;
+        case 22: v = rk3; break;
+        case 23: v = rk5; break;
+        case 24: v = d.sat; break;
+        case 25: v = d.vfrac; break;
+        case 26: v = d.nfeas; break;
+        case 27: v = (double)d.remaining; break;
+        case 28: v = fsc / (ns + 1.0); break;
+        case 29: v = fsc - ns; break;
+        case 30: v = eloss; break;
+        case 31: v = (tc - I.zp[0]) / I.zp[5]; break;
+        case 32: v = (reach2 - I.zp[1]) / I.zp[6]; break;
+        case 33: v = (regret - I.zp[2]) / I.zp[7]; break;
+        case 34: v = (eloss - I.zp[3]) / I.zp[8]; break;
+        case 35: v = (d2d_i - I.zp[4]) / I.zp[9]; break;
+        case 36: v = 0.1; break;
+        case 37: v = 0.2; break;
+        case 38: v = 0.3; break;
+        case 39: v = 0.4; break;
+        case 40: v = 0.5; break;
+        case 41: v = reach2rob; break;
+        case 42: {
+            double den = tmax - ct;
+            if (den < 1.0) den = 1.0;
+            v = (ta + dur_i) / den;
+            break;
+        }
+        case 43: v = reach2rob - regret; break;
+        case 44: v = x_skiploss(I, S, i, cur, ct); break;
+        case 45: v = ns - nsrob; break;
+        case 46: {
+            double den = ta + d2d_i;
+            if (den < 1.0) den = 1.0;
+            v = (sc_i + nsrob) / den;
+            break;
+        }
+        case 47: v = x_reach_k_rob(I, S, i, st_c + dur_i * (1.0 + kSigma), 3); break;
+        case 48: v = x_reach_k_rob(I, S, i, st_c + dur_i * (1.0 + kSigma), 5); break;
+        case 49: v = x_ns_family(I, S, i, fin, 0); break;
+        case 50: v = x_ns_family(I, S, i, fin, 1); break;
+        case 51: v = d.fscore; break;
+        case 52: v = d.nfeasrob; break;
+        case 53: v = x_ns_rob_m(I, S, i, fin, 0.5); break;
+        case 54: v = x_ns_rob_m(I, S, i, fin, 2.0); break;
+        case 55: v = x_ns_family(I, S, i, fin, 2); break;
+        case 56: v = x_ns_family(I, S, i, fin, 3); break;
+        case 57: v = x_nnchain(I, S, i, fin_c, 3); break;
+        case 58: v = I.dist[(size_t)cur * ld + 0] + d2d_i - ta; break;
+        case 59: v = x_detour(I, S, i, cur, fin, ta); break;
+        case 60: v = x_ns_family(I, S, i, fin, 4); break;
+        default: v = 0.0; break;
+        }
+        S.rows[k * 32 + lane] = v;
+    }
+
+    // Rule program (engine/sim_core.hpp:11-41 as three-address code).
+    for (int q = 0; q < rm.n_ins; q++) {
+        const uint32_t wd = S.prog[q];
+        const uint32_t op = wd & 7u;
+        const uint32_t oa = (wd >> 3) & 1023u, ob = (wd >> 13) & 1023u, od = wd >> 23;
+        const double a = (oa & kOpConst) ? S.cst[oa & 511u] : S.rows[oa * 32 + lane];
+        const double b = (ob & kOpConst) ? S.cst[ob & 511u] : S.rows[ob * 32 + lane];
+        double r;
+        switch (op) {
+        case 0: r = a + b; break;
+        case 1: r = a - b; break;
+        case 2: r = a * b; break;
+        case 3: r = fabs(b) < 1e-10 ? 1.0 : a / b; break;
+        case 4: r = a < b ? a : b; break;
+        case 5: r = a > b ? a : b; break;
+        default: {
+            const double base = a > 0.0 ? a : 0.0;
+            double e = b;
+            if (e < 0.0) e = 0.0;
+            else if (e > 1.0) e = 1.0;
+            r = pow(base, 1.0 + e);
+        }
+        }
+        S.rows[od * 32 + lane] = r;
+    }
+    const uint32_t res = (uint32_t)rm.res;
+    double pri = (res & kOpConst) ? S.cst[res & 511u] : S.rows[res * 32 + lane];
+    if (pri != pri) pri = -1e300;
+    return pri;
+}
+
+// One decision: returns the chosen customer or -1 (pick_best).
+template <bool COUNT>
+__device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, Decision& d,
+                      WarpCounts& wc) {
+    const int lane = threadIdx.x & 31;
+    const int n = I.n, ld = I.ld, nw = I.nw;
+    const uint32_t need = rm.need;
+    const bool need_atr = (need & kNeedAtRisk) != 0;
+
+    // Feasible-now bitmask (the reference's candidate filter, :75-82) and
+    // ATRISK's arrive-by-close filter, one ballot per 32 customers.
+    const double* Fc = I.F + (size_t)d.cur * n;
+    const double* Dc = I.dist + (size_t)d.cur * ld + 1;
+    for (int w = 0; w < nw; w++) {
+        const int j = (w << 5) + lane;
+        const bool u = (S.unv[w] >> lane) & 1u;
+        const bool f = u && d.ct <= Fc[j];
+        const uint32_t bf = __ballot_sync(kFull, f);
+        uint32_t ba = 0;
+        if (need_atr) {
+            const bool a = u && !(d.ct + Dc[j] > I.close_t[j]);
+            ba = __ballot_sync(kFull, a);
+        }
+        if (lane == 0) {
+            S.feas[w] = bf;
+            S.atr[w] = ba;
+        }
+    }
+    __syncwarp();
+
+    int ncand = 0;
+    for (int w = 0; w < nw; w++) {
+        const uint32_t bits = S.feas[w];
+        if ((bits >> lane) & 1u) S.cand[ncand + __popc(bits & ((1u << lane) - 1u))] = (int16_t)((w << 5) + lane);
+        ncand += __popc(bits);
+    }
+    __syncwarp();
+
+    // Per-decision aggregates (:55-71).
+    d.sat = I.tmax > 0.0 ? d.ct / I.tmax : 0.0;
+    if (need & (kNeedAgg | kNeedFScore | kNeedNFeasRob)) {
+        int unv = 0;
+        for (int w = 0; w < nw; w++) unv += __popc(S.unv[w]);
+        d.vfrac = (double)(n - unv) / n;
+        d.nfeas = (double)ncand;
+        double fs = 0.0, nr = 0.0;
+        if (need & (kNeedFScore | kNeedNFeasRob)) {
+            for (int k = 0; k < ncand; k++) {
+                const int j = S.cand[k];
+                fs += I.scores[j];
+                const double arr = d.ct + Dc[j];
+                const double st = arr > I.open_t[j] ? arr : I.open_t[j];
+                if (st + I.durations[j] * (1.0 + kSigma) + I.d2d[j] <= I.tmax) nr += 1.0;
+            }
+        }
+        d.fscore = fs;
+        d.nfeasrob = nr;
+    } else {
+        d.vfrac = d.nfeas = d.fscore = d.nfeasrob = 0.0;
+    }
+    if (COUNT && lane == 0) {
+        wc.dec++;
+        wc.cand += ncand;
+        wc.ops += 2ull * n;
+    }
+
+    int best = -1;
+    double best_pri = -1e300;
+    for (int base = 0; base < ncand; base += 32) {
+        const int k = base + lane;
+        double pri = -1e300;
+        int idx = 0x7fffffff;
+        if (k < ncand) {
+            idx = S.cand[k];
+            pri = score_candidate<COUNT>(I, S, rm, d, idx, wc);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double op = __shfl_xor_sync(kFull, pri, off);
+            const int oi = __shfl_xor_sync(kFull, idx, off);
+            if (op > pri || (op == pri && oi < idx)) {
+                pri = op;
+                idx = oi;
+            }
+        }
+        if (pri > best_pri) {
+            best_pri = pri;
+            best = idx;
+        }
+    }
+    return best;
+}
+
+// sim_one (engine/sim_core.hpp:207-238) for one pair; every lane returns the
+// same total.
+template <bool COUNT>
+__device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
+                          const double* smp, WarpCounts& wc) {
+    const int lane = threadIdx.x & 31;
+    const int n = I.n, ld = I.ld;
+    for (int w = lane; w < I.nw; w += 32) {
+        const int lo = w << 5;
+        const int cnt = n - lo >= 32 ? 32 : n - lo;
+        S.unv[w] = cnt >= 32 ? kFull : ((1u << cnt) - 1u);
+    }
+    __syncwarp();
+    double total = 0.0;
+    for (int v = 0; v < I.m; v++) {
+        Decision d;
+        d.remaining = I.m - v - 1;
+        d.cur = 0;
+        d.ct = 0.0;
+        for (;;) {
+            const int b = decide<COUNT>(I, S, rm, d, wc);
+            if (b < 0) break;
+            const double arrive = d.ct + I.dist[(size_t)d.cur * ld + b + 1];
+            const double st = arrive > I.open_t[b] ? arrive : I.open_t[b];
+            d.ct = st + smp[b];
+            d.cur = b + 1;
+            total += I.scores[b];
+            if (lane == 0) S.unv[b >> 5] &= ~(1u << (b & 31));
+            __syncwarp();
+        }
+    }
+    return total;
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) eval_kernel(const DevInst I, const DevBatch B) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const size_t slice = warp_slice_bytes(B.rows, B.const_cap, B.prog_cap);
+    const WarpSmem S = carve(smem_raw + (size_t)wib * slice, B.rows, B.const_cap, B.prog_cap);
+
+    const unsigned long long total = (unsigned long long)B.P * (unsigned long long)B.T;
+    int staged = -1;
+    RuleMeta rm;
+    WarpCounts wc = {0, 0, 0, 0, 0, 0};
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(B.counter, 1ull);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= total) break;
+        const int p = (int)(item / (unsigned long long)B.T);
+        const int s = (int)(item % (unsigned long long)B.T);
+        if (p != staged) {
+            rm = B.meta[p];
+            for (int q = lane; q < rm.n_ins; q += 32) S.prog[q] = B.prog[rm.prog_off + q];
+            for (int q = lane; q < rm.n_const; q += 32) S.cst[q] = B.consts[rm.const_off + q];
+            for (int q = lane; q < rm.K; q += 32) S.slots[q] = B.slots[rm.slot_off + q];
+            staged = p;
+            __syncwarp();
+        }
+        const double* smp = B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
+        const double tot = rollout<COUNT>(I, S, rm, smp, wc);
+        if (lane == 0) B.out[(size_t)p * B.T + s] = tot;
+    }
+    if (COUNT) {
+        // dec/cand/per-decision ops live in lane 0; the rest are per lane.
+        unsigned long long v[kStats] = {wc.dec, wc.cand, wc.scan, wc.heavy, wc.hop, wc.ops};
+#pragma unroll
+        for (int k = 2; k < kStats; k++)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(kFull, v[k], off);
+        if (lane == 0 && B.stats) {
+#pragma unroll
+            for (int k = 0; k < kStats; k++) atomicAdd(&B.stats[k], v[k]);
+        }
+    }
+}
+
+}  // namespace sidr

@@ -1,0 +1,274 @@
+"""Python front end of the B200 rule x scenario evaluator (libsidr_b200.so).
+
+A thin ctypes layer over the C-ABI declared in include/sidr.h, shaped like the
+reference's evaluator API (augustompm/solver-informed-dispatching-rules,
+engine/factory.cuh:124-217):
+
+    ctx = Context(simdata, zp, device=0)            # FactoryContext(sd, zp)
+    ctx.evaluate(rules, sampled, N, mask)            # -> [P, N]
+    ctx.evaluate_grouped(rules, grouped, G, T, group_size, mask)
+    ctx.evaluate_grouped_masks(rules, grouped, T, group_size, mask_group, masks)
+
+plus device-resident batches (``ctx.batch(...)``) for repeated launches.
+There is no CPU fallback: if the native library is missing, importing the
+evaluator raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .instance import SimData  # noqa: F401
+from .rules import N_TERMS, PackedRules  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "libsidr_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+class SidrError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"sidr status {status}: {msg}")
+        self.status = status
+
+
+class _Inst(C.Structure):
+    _fields_ = [("n", C.c_int32), ("m", C.c_int32), ("tmax", C.c_double), ("scores", _dp),
+                ("durations", _dp), ("open_t", _dp), ("close_t", _dp), ("dist", _dp),
+                ("dist_to_depot", _dp)]
+
+
+class _Rules(C.Structure):
+    _fields_ = [("ops", _ip), ("args", _ip), ("offsets", _ip), ("lengths", _ip), ("P", C.c_int32),
+                ("n_nodes", C.c_int64)]
+
+
+class _Counts(C.Structure):
+    _fields_ = [("decisions", C.c_int64), ("candidates", C.c_int64), ("scan_iters", C.c_int64),
+                ("heavy_iters", C.c_int64)]
+
+
+EXPORTS = [
+    "sidr_last_error", "sidr_status_string", "sidr_version", "sidr_zstats", "sidr_ctx_create",
+    "sidr_ctx_destroy", "sidr_evaluate", "sidr_evaluate_grouped", "sidr_evaluate_grouped_masks",
+    "sidr_batch_create", "sidr_batch_run", "sidr_batch_read", "sidr_batch_fitness",
+    "sidr_batch_device_out", "sidr_batch_destroy", "sidr_batch_set_counting", "sidr_batch_counts",
+    "sidr_kernel_launches", "sidr_rules_check",
+]
+
+_lib: Optional[C.CDLL] = None
+
+
+def load() -> C.CDLL:
+    """Loads libsidr_b200.so; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run solver-informed-dispatching-rules_b200/"
+                          "build.py (there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    L.sidr_last_error.restype = C.c_char_p
+    L.sidr_status_string.restype = C.c_char_p
+    L.sidr_status_string.argtypes = [C.c_int]
+    L.sidr_zstats.argtypes = [C.POINTER(_Inst), _dp]
+    L.sidr_ctx_create.argtypes = [C.POINTER(_Inst), _dp, C.c_int, C.POINTER(C.c_void_p)]
+    L.sidr_ctx_destroy.argtypes = [C.c_void_p]
+    L.sidr_evaluate.argtypes = [C.c_void_p, C.POINTER(_Rules), _dp, C.c_int32, _lp, _dp]
+    L.sidr_evaluate_grouped.argtypes = [C.c_void_p, C.POINTER(_Rules), _dp, C.c_int32, C.c_int32,
+                                        C.c_int32, _lp, _dp]
+    L.sidr_evaluate_grouped_masks.argtypes = [C.c_void_p, C.POINTER(_Rules), _dp, C.c_int32,
+                                              C.c_int32, C.c_int32, C.c_int32, _lp, _dp]
+    L.sidr_batch_create.argtypes = [C.c_void_p, C.POINTER(_Rules), _dp, C.c_int32, C.c_int32,
+                                    C.c_int32, C.c_int32, _lp, C.POINTER(C.c_void_p)]
+    L.sidr_batch_run.argtypes = [C.c_void_p, C.c_void_p]
+    L.sidr_batch_read.argtypes = [C.c_void_p, _dp]
+    L.sidr_batch_fitness.argtypes = [C.c_void_p, _dp]
+    L.sidr_batch_device_out.argtypes = [C.c_void_p]
+    L.sidr_batch_device_out.restype = C.c_void_p
+    L.sidr_batch_destroy.argtypes = [C.c_void_p]
+    L.sidr_batch_set_counting.argtypes = [C.c_void_p, C.c_int]
+    L.sidr_batch_counts.argtypes = [C.c_void_p, C.POINTER(_Counts)]
+    L.sidr_kernel_launches.restype = C.c_int64
+    L.sidr_rules_check.argtypes = [C.POINTER(_Rules), _lp, C.c_int32, C.POINTER(C.c_int32)]
+    _lib = L
+    return L
+
+
+def _check(st: int) -> None:
+    if st != 0:
+        L = load()
+        raise SidrError(st, L.sidr_last_error().decode())
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+class _Keep:
+    """Holds contiguous copies alive for the duration of a native call."""
+
+    def __init__(self):
+        self.refs = []
+
+    def f64(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.refs.append(a)
+        return a.ctypes.data_as(_dp)
+
+    def i32(self, a):
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        self.refs.append(a)
+        return a.ctypes.data_as(_ip)
+
+    def i64(self, a):
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        self.refs.append(a)
+        return a.ctypes.data_as(_lp)
+
+    def inst(self, sd) -> _Inst:
+        return _Inst(sd.n, sd.m, float(sd.tmax), self.f64(sd.scores), self.f64(sd.durations),
+                     self.f64(sd.open_t), self.f64(sd.close_t), self.f64(sd.dist),
+                     self.f64(sd.dist_to_depot))
+
+    def rules(self, r) -> _Rules:
+        return _Rules(self.i32(r.ops), self.i32(r.args), self.i32(r.offsets), self.i32(r.lengths),
+                      r.P, int(len(r.ops)))
+
+
+def zstats(sd) -> np.ndarray:
+    """zp_of(sd): host computation through the C-ABI."""
+    L = load()
+    k = _Keep()
+    zp = np.zeros(10)
+    inst = k.inst(sd)
+    _check(L.sidr_zstats(C.byref(inst), _d(zp)))
+    return zp
+
+
+def rules_check(rules, masks, mask_group=None) -> int:
+    """Validates and compiles rules on the host; returns the per-lane value
+    rows the largest program needs."""
+    L = load()
+    k = _Keep()
+    masks = np.ascontiguousarray(masks, dtype=np.int64).reshape(-1)
+    r = k.rules(rules)
+    rows = C.c_int32()
+    _check(L.sidr_rules_check(C.byref(r), k.i64(masks), mask_group or max(rules.P, 1),
+                              C.byref(rows)))
+    return rows.value
+
+
+def kernel_launches() -> int:
+    return int(load().sidr_kernel_launches())
+
+
+class Batch:
+    """Rules, scenarios and masks resident in HBM (sidr_batch_*)."""
+
+    def __init__(self, ctx: "Context", handle: int, P: int, T: int):
+        self.ctx, self.h, self.P, self.T = ctx, handle, P, T
+
+    def run(self, stream: int = 0) -> None:
+        _check(load().sidr_batch_run(self.h, C.c_void_p(stream)))
+
+    def read(self) -> np.ndarray:
+        out = np.zeros((self.P, self.T))
+        _check(load().sidr_batch_read(self.h, _d(out)))
+        return out
+
+    def fitness(self) -> np.ndarray:
+        out = np.zeros(self.P)
+        _check(load().sidr_batch_fitness(self.h, _d(out)))
+        return out
+
+    def device_out(self) -> int:
+        return int(load().sidr_batch_device_out(self.h) or 0)
+
+    def set_counting(self, on: bool) -> None:
+        _check(load().sidr_batch_set_counting(self.h, int(on)))
+
+    def counts(self) -> dict:
+        c = _Counts()
+        _check(load().sidr_batch_counts(self.h, C.byref(c)))
+        return {"decisions": c.decisions, "candidates": c.candidates,
+                "scan_iters": c.scan_iters, "heavy_iters": c.heavy_iters}
+
+    def close(self) -> None:
+        if self.h:
+            load().sidr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """FactoryContext(sd, zp) on one device."""
+
+    def __init__(self, sd, zp=None, device: int = 0):
+        L = load()
+        self.sd = sd
+        self.zp = np.ascontiguousarray(zstats(sd) if zp is None else zp, dtype=np.float64)
+        k = _Keep()
+        inst = k.inst(sd)
+        h = C.c_void_p()
+        _check(L.sidr_ctx_create(C.byref(inst), _d(self.zp), device, C.byref(h)))
+        self.h = h.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            load().sidr_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the reference-shaped calls (host buffers, synchronous)
+    def evaluate(self, rules, sampled, N, term_mask) -> np.ndarray:
+        k = _Keep()
+        r = k.rules(rules)
+        out = np.zeros((rules.P, N))
+        _check(load().sidr_evaluate(self.h, C.byref(r), k.f64(sampled), N, k.i64(term_mask),
+                                    _d(out)))
+        return out
+
+    def evaluate_grouped(self, rules, grouped_sampled, G, T, group_size, term_mask):
+        k = _Keep()
+        r = k.rules(rules)
+        out = np.zeros((rules.P, T))
+        _check(load().sidr_evaluate_grouped(self.h, C.byref(r), k.f64(grouped_sampled), G, T,
+                                            group_size, k.i64(term_mask), _d(out)))
+        return out
+
+    def evaluate_grouped_masks(self, rules, grouped_sampled, G, T, group_size, mask_group, masks):
+        k = _Keep()
+        r = k.rules(rules)
+        out = np.zeros((rules.P, T))
+        _check(load().sidr_evaluate_grouped_masks(self.h, C.byref(r), k.f64(grouped_sampled), G,
+                                                  T, group_size, mask_group, k.i64(masks),
+                                                  _d(out)))
+        return out
+
+    def batch(self, rules, grouped_sampled, T, masks, G=1, group_size=None,
+              mask_group=None) -> Batch:
+        k = _Keep()
+        r = k.rules(rules)
+        h = C.c_void_p()
+        _check(load().sidr_batch_create(self.h, C.byref(r), k.f64(grouped_sampled), G, T,
+                                        group_size or max(rules.P, 1),
+                                        mask_group or max(rules.P, 1), k.i64(masks),
+                                        C.byref(h)))
+        return Batch(self, h.value, rules.P, T)

@@ -265,7 +265,8 @@ def run_ours(args, rank, world, local):
     zp = sidr.zstats(w.sd)
     ctx = sidr.Context(w.sd, zp, device=local)
     batch = ctx.batch(w.rules, w.sampled, w.S, w.mask)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # the launching stream: events are recorded on it
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
 
     # op-model counts (separate, untimed launch of the counting instantiation)
@@ -275,7 +276,7 @@ def run_ours(args, rank, world, local):
     counts = batch.counts()
     batch.set_counting(False)
 
-    peak_ops = ctypes_fp64_peak(local)
+    peak_ops = sidr.fp64_peak(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):
@@ -319,7 +320,7 @@ def run_ours(args, rank, world, local):
             out = ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
             t_e2e += time.perf_counter() - t0
         t_e2e = allmax(t_e2e)
-        h2d, d2h = transfer_bytes()
+        h2d, d2h = sidr.last_transfer_bytes()
         same = same and bool(np.array_equal(out.view(np.uint64), ref_out.view(np.uint64)))
         e2e = {"value": world * evals_per_rank * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -348,28 +349,6 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
-
-
-def ctypes_fp64_peak(dev: int) -> float:
-    import ctypes as C
-    import sidr
-    L = sidr.load()
-    L.sidr_fp64_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
-    v = C.c_double()
-    st = L.sidr_fp64_peak(dev, 5, C.byref(v))
-    if st != 0:
-        raise RuntimeError(L.sidr_last_error().decode())
-    return v.value
-
-
-def transfer_bytes():
-    import ctypes as C
-    import sidr
-    L = sidr.load()
-    L.sidr_last_transfer_bytes.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
-    a, b = C.c_int64(), C.c_int64()
-    L.sidr_last_transfer_bytes(C.byref(a), C.byref(b))
-    return a.value, b.value
 
 
 def main():

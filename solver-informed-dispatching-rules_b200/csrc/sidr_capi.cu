@@ -609,7 +609,7 @@ sidr_status sidr_batch_set_counting(sidr_batch* b, int enable) {
 sidr_status sidr_batch_run(sidr_batch* bt, void* stream) {
     if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
-    cudaStream_t st = stream ? (cudaStream_t)stream : bt->ctx->stream;
+    cudaStream_t st = (cudaStream_t)stream;  // 0 = the legacy default stream
     sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->grid, bt->block, bt->smem, st);
     if (s) return s;
     if (bt->P > 0) {

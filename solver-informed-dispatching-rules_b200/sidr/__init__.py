@@ -51,7 +51,11 @@ class _Rules(C.Structure):
 
 class _Counts(C.Structure):
     _fields_ = [("decisions", C.c_int64), ("candidates", C.c_int64), ("scan_iters", C.c_int64),
-                ("heavy_iters", C.c_int64)]
+                ("heavy_iters", C.c_int64), ("hop_iters", C.c_int64), ("fp64_ops", C.c_int64)]
+
+
+# ctypes mirrors of the C structs, checked against include/sidr.h by the tests.
+STRUCTS = {"sidr_instance_desc": _Inst, "sidr_rules_desc": _Rules, "sidr_counts": _Counts}
 
 
 EXPORTS = [
@@ -59,7 +63,7 @@ EXPORTS = [
     "sidr_ctx_destroy", "sidr_evaluate", "sidr_evaluate_grouped", "sidr_evaluate_grouped_masks",
     "sidr_batch_create", "sidr_batch_run", "sidr_batch_read", "sidr_batch_fitness",
     "sidr_batch_device_out", "sidr_batch_destroy", "sidr_batch_set_counting", "sidr_batch_counts",
-    "sidr_kernel_launches", "sidr_rules_check",
+    "sidr_kernel_launches", "sidr_rules_check", "sidr_last_transfer_bytes", "sidr_fp64_peak",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -97,6 +101,8 @@ def load() -> C.CDLL:
     L.sidr_batch_counts.argtypes = [C.c_void_p, C.POINTER(_Counts)]
     L.sidr_kernel_launches.restype = C.c_int64
     L.sidr_rules_check.argtypes = [C.POINTER(_Rules), _lp, C.c_int32, C.POINTER(C.c_int32)]
+    L.sidr_last_transfer_bytes.argtypes = [_lp, _lp]
+    L.sidr_fp64_peak.argtypes = [C.c_int, C.c_int, _dp]
     _lib = L
     return L
 
@@ -169,6 +175,20 @@ def kernel_launches() -> int:
     return int(load().sidr_kernel_launches())
 
 
+def last_transfer_bytes():
+    """(h2d, d2h) bytes of this thread's last evaluate* call."""
+    a, b = C.c_int64(), C.c_int64()
+    _check(load().sidr_last_transfer_bytes(C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def fp64_peak(device: int = 0, reps: int = 5) -> float:
+    """Measured FP64 pipe throughput of the device (operations/s)."""
+    v = C.c_double()
+    _check(load().sidr_fp64_peak(device, reps, C.byref(v)))
+    return v.value
+
+
 class Batch:
     """Rules, scenarios and masks resident in HBM (sidr_batch_*)."""
 
@@ -197,8 +217,7 @@ class Batch:
     def counts(self) -> dict:
         c = _Counts()
         _check(load().sidr_batch_counts(self.h, C.byref(c)))
-        return {"decisions": c.decisions, "candidates": c.candidates,
-                "scan_iters": c.scan_iters, "heavy_iters": c.heavy_iters}
+        return {k: int(getattr(c, k)) for k, _ in _Counts._fields_}
 
     def close(self) -> None:
         if self.h:

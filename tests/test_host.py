@@ -25,7 +25,7 @@ def bits(a):
 
 def header_symbols():
     text = open(os.path.join(REPO, "include", "sidr.h")).read()
-    return sorted(set(re.findall(r"\b(sidr_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(sidr_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -35,6 +35,33 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(L, name), name
     assert set(sidr.EXPORTS) <= set(declared)
+
+
+def test_ctypes_structs_match_header(tmp_path):
+    """Every ctypes mirror has the C struct's size and member offsets (a
+    mismatch lets the library write past a Python-owned buffer)."""
+    import ctypes
+    import subprocess
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "sidr.h"', "int main(void){"]
+    for cname, py in sidr.STRUCTS.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n"):
+        if ln:
+            a, b, c = ln.split()
+            got[(a, b)] = int(c)
+    for cname, py in sidr.STRUCTS.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
 
 
 def test_capi_zstats_matches_golden():

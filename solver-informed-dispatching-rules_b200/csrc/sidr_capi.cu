@@ -204,7 +204,7 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
     const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
     if (slice > c->smem_optin)
         return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
-    int wpb = (int)std::min<size_t>(8, c->smem_optin / slice);
+    int wpb = (int)std::min<size_t>(SIDR_WARPS_PER_BLOCK, c->smem_optin / slice);
     if (wpb < 1) wpb = 1;
     block = 32 * wpb;
     smem = slice * wpb;
@@ -468,6 +468,16 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         {h.P0.data(), h.P0.size() * 8, (const void**)&I.P0},
         {h.zlt.data(), h.zlt.size() * 4, (const void**)&I.zlt},
         {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle},
+        {h.FT.data(), h.FT.size() * 8, (const void**)&I.FT},
+        {h.GT.data(), h.GT.size() * 8, (const void**)&I.GT},
+        {h.RT.data(), h.RT.size() * 8, (const void**)&I.RT},
+        {h.DT.data(), h.DT.size() * 8, (const void**)&I.DT},
+        {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T},
+        {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
+        {h.sR.data(), h.sR.size() * 8, (const void**)&I.sR},
+        {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
+        {h.sFz.data(), h.sFz.size() * 8, (const void**)&I.sFz},
+        {h.sGz.data(), h.sGz.size() * 8, (const void**)&I.sGz},
         {zp, 80, (const void**)&I.zp},
     };
     for (const Item& it : items) {

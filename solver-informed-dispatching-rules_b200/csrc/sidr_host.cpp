@@ -3,6 +3,7 @@
 // IEEE operations one by one.
 #include "sidr_host.hpp"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -197,6 +198,44 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
             const double sd_j = kSigma * h.durations[j];
             const double vb = vs + sd_j * sd_j;
             h.P1[(size_t)c * n + j] = vb > 1e-18 ? std::pow(vb, 0.5) : -1.0;
+        }
+    }
+    // Neighbour-major copies.
+    h.FT.assign(rows, 0.0);
+    h.GT.assign(rows, 0.0);
+    h.RT.assign(rows, 0.0);
+    h.DT.assign(rows, 0.0);
+    h.P1T.assign((size_t)n * n, 0.0);
+    for (int o = 0; o < ld; o++)
+        for (int j = 0; j < n; j++) {
+            const size_t a = (size_t)o * n + j, t = (size_t)j * ld + o;
+            h.FT[t] = h.F[a];
+            h.GT[t] = h.G[a];
+            h.RT[t] = h.R[a];
+            h.DT[t] = D(h, o, j + 1);
+        }
+    for (int c = 0; c < n; c++)
+        for (int j = 0; j < n; j++) h.P1T[(size_t)j * n + c] = h.P1[(size_t)c * n + j];
+    // Per-origin neighbour lists by (R desc, index asc).
+    h.ord.assign(rows, 0);
+    h.sR.assign(rows, 0.0);
+    h.sF.assign(rows, 0.0);
+    h.sFz.assign(rows, 0.0);
+    h.sGz.assign(rows, 0.0);
+    std::vector<int> idx(n);
+    for (int o = 0; o < ld; o++) {
+        const double* Ro = h.R.data() + (size_t)o * n;
+        for (int j = 0; j < n; j++) idx[j] = j;
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return Ro[a] > Ro[b]; });
+        for (int k = 0; k < n; k++) {
+            const int j = idx[k];
+            const size_t a = (size_t)o * n + j, s = (size_t)o * n + k;
+            const bool coincident = (h.zlt[(size_t)o * h.nw + (j >> 5)] >> (j & 31)) & 1u;
+            h.ord[s] = (int16_t)j;
+            h.sR[s] = h.R[a];
+            h.sF[s] = h.F[a];
+            h.sFz[s] = coincident ? -INFINITY : h.F[a];
+            h.sGz[s] = coincident ? -INFINITY : h.G[a];
         }
     }
     return "";

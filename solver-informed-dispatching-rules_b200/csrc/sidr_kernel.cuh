@@ -28,6 +28,15 @@ namespace sidr {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Block shape of the evaluator: warps per block and the minimum resident
+// blocks per SM that bound its registers (__launch_bounds__).
+#ifndef SIDR_WARPS_PER_BLOCK
+#define SIDR_WARPS_PER_BLOCK 8
+#endif
+#ifndef SIDR_MIN_BLOCKS
+#define SIDR_MIN_BLOCKS 1
+#endif
+
 // Shared-memory slice of one warp.
 struct WarpSmem {
     double* rows;      // [rows][32]
@@ -93,70 +102,49 @@ __device__ __forceinline__ uint32_t bit_in_word(int node, int w) {
     return (node >= 0 && (node >> 5) == w) ? (1u << (node & 31)) : 0u;
 }
 
-// Best neighbour by score/time from origin row o at time tm over unvisited
-// customers outside {x0..x4}: `table` is F (standard) or G (robust).  init 0.0
-// and the coincident skip reproduce REACH2's second loop
-// (engine/sim_terms.hpp:112-126, :175-189); returns the chosen customer's score
-// or 0.0.
+// REACH2's second loop (engine/sim_terms.hpp:112-126, robust :175-189): the
+// best unvisited customer outside {x0, x1} by score/time from origin node o at
+// time tm, skipping coincident locations, init 0.0.  `table` is sFz (standard)
+// or sGz (robust).  The argmax with strict > over ascending index is the first
+// feasible entry of o's sorted neighbour list whose ratio exceeds 0.0.
+// Returns the chosen customer's score, or 0.0.
 template <bool COUNT>
 __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const double* table,
                                    int o, double tm, int x0, int x1, unsigned long long& hops) {
     const int n = I.n;
-    const double* To = table + (size_t)o * n;
-    const double* Ro = I.R + (size_t)o * n;
-    const uint32_t* zo = I.zlt + (size_t)o * I.nw;
-    double bv = 0.0, bs = 0.0;
-    for (int w = 0; w < I.nw; w++) {
-        uint32_t bits = S.unv[w] & ~(bit_in_word(x0, w) | bit_in_word(x1, w) | zo[w]);
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const int j = (w << 5) + b;
-            if (COUNT) hops++;
-            if (tm <= To[j]) {
-                const double v = Ro[j];
-                if (v > bv) {
-                    bv = v;
-                    bs = I.scores[j];
-                }
-            }
-        }
+    const int16_t* ord = I.ord + (size_t)o * n;
+    const double* sR = I.sR + (size_t)o * n;
+    const double* sT = table + (size_t)o * n;
+    for (int k = 0; k < n; k++) {
+        if (!(sR[k] > 0.0)) break;
+        const int q = ord[k];
+        if (COUNT) hops++;
+        if (q == x0 || q == x1 || !is_unvisited(S, q)) continue;
+        if (tm <= sT[k]) return I.scores[q];
     }
-    return bs;
+    return 0.0;
 }
 
-// One REACH-k greedy step (engine/sim_terms.hpp:415-431): best unvisited
+// One REACH-k greedy step (engine/sim_terms.hpp:415-431): the best unvisited
 // customer outside the path by score/max(t,1e-10) under the standard test, no
-// coincident skip, init -1.0.
+// coincident skip, init -1.0 -- the first feasible entry of o's sorted list
+// whose ratio exceeds -1.0.
 template <bool COUNT>
-__device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm, const int* path,
-                          int np, unsigned long long& hops) {
+__device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm, int p0, int p1,
+                          int p2, int p3, int p4, unsigned long long& hops) {
+    // p0..p4: the walk so far (candidate first; -1 = unused)
     const int n = I.n;
-    const double* Fo = I.F + (size_t)o * n;
-    const double* Ro = I.R + (size_t)o * n;
-    double bv = -1.0;
-    int bq = -1;
-    for (int w = 0; w < I.nw; w++) {
-        uint32_t ex = 0;
-#pragma unroll
-        for (int k = 0; k < 5; k++)
-            if (k < np) ex |= bit_in_word(path[k], w);
-        uint32_t bits = S.unv[w] & ~ex;
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const int j = (w << 5) + b;
-            if (COUNT) hops++;
-            if (tm <= Fo[j]) {
-                const double v = Ro[j];
-                if (v > bv) {
-                    bv = v;
-                    bq = j;
-                }
-            }
-        }
+    const int16_t* ord = I.ord + (size_t)o * n;
+    const double* sR = I.sR + (size_t)o * n;
+    const double* sF = I.sF + (size_t)o * n;
+    for (int k = 0; k < n; k++) {
+        if (!(sR[k] > -1.0)) break;
+        const int q = ord[k];
+        if (COUNT) hops++;
+        if (!is_unvisited(S, q) || q == p0 || q == p1 || q == p2 || q == p3 || q == p4) continue;
+        if (tm <= sF[k]) return q;
     }
-    return bq;
+    return -1;
 }
 
 // ------------------------------------------------- exploration terminals
@@ -165,7 +153,7 @@ __device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm,
 // arrays straight, like the reference, and are used only when a mask enables
 // them.
 
-__device__ double x_skiploss(const DevInst& I, const WarpSmem& S, int i, int cur, double ct) {
+__device__ __noinline__ double x_skiploss(const DevInst& I, const WarpSmem& S, int i, int cur, double ct) {
     const int ld = I.ld;
     double bv = 0.0, fq = 0.0;
     int bq = -1;
@@ -192,7 +180,7 @@ __device__ double x_skiploss(const DevInst& I, const WarpSmem& S, int i, int cur
     return 0.0;
 }
 
-__device__ double x_reach_k_rob(const DevInst& I, const WarpSmem& S, int c, double fin_rob_c,
+__device__ __noinline__ double x_reach_k_rob(const DevInst& I, const WarpSmem& S, int c, double fin_rob_c,
                                 int K) {
     const int ld = I.ld;
     int path[6] = {c, -1, -1, -1, -1, -1};
@@ -227,7 +215,7 @@ __device__ double x_reach_k_rob(const DevInst& I, const WarpSmem& S, int c, doub
     return tot;
 }
 
-__device__ double x_ns_family(const DevInst& I, const WarpSmem& S, int i, double fin, int kind) {
+__device__ __noinline__ double x_ns_family(const DevInst& I, const WarpSmem& S, int i, double fin, int kind) {
     // kind 0: NSA2 score/t^2, 1: NSA05 score/sqrt(t), 2: NNFWD, 3: NNK3, 4: SCORERANK
     const int ld = I.ld;
     double acc = 0.0, d1 = -1.0, d2 = -1.0, d3 = -1.0, below = 0.0, tot = 0.0;
@@ -275,7 +263,7 @@ __device__ double x_ns_family(const DevInst& I, const WarpSmem& S, int i, double
     return below / tot;
 }
 
-__device__ double x_ns_rob_m(const DevInst& I, const WarpSmem& S, int i, double fin, double m) {
+__device__ __noinline__ double x_ns_rob_m(const DevInst& I, const WarpSmem& S, int i, double fin, double m) {
     const int ld = I.ld;
     const double ms = m * kSigma;
     const double frob = fin + I.durations[i] * ms;
@@ -290,7 +278,7 @@ __device__ double x_ns_rob_m(const DevInst& I, const WarpSmem& S, int i, double 
     return acc;
 }
 
-__device__ double x_nnchain(const DevInst& I, const WarpSmem& S, int c, double fin_c, int K) {
+__device__ __noinline__ double x_nnchain(const DevInst& I, const WarpSmem& S, int c, double fin_c, int K) {
     const int ld = I.ld;
     int path[4] = {c, -1, -1, -1};
     int at = c + 1, done = 0;
@@ -325,7 +313,7 @@ __device__ double x_nnchain(const DevInst& I, const WarpSmem& S, int c, double f
     return 1.0 / (1.0 + tot / done);
 }
 
-__device__ double x_detour(const DevInst& I, const WarpSmem& S, int i, int cur, double fin,
+__device__ __noinline__ double x_detour(const DevInst& I, const WarpSmem& S, int i, int cur, double fin,
                            double ta_i) {
     const int ld = I.ld;
     double tot = 0.0, cnt = 0.0;
@@ -392,11 +380,12 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
 
     const uint32_t fused = kNeedNSFused | kNeedRegret | kNeedRob | kNeedAfterC | kNeedAtRisk;
     if (need & fused) {
-        const double* Fi = I.F + (size_t)(i + 1) * n;
-        const double* Gi = I.G + (size_t)(i + 1) * n;
-        const double* Ri = I.R + (size_t)(i + 1) * n;
-        const double* Di = I.dist + (size_t)(i + 1) * ld + 1;
-        const double* P1i = I.P1 + (size_t)i * n;
+        // neighbour-major tables: entry (origin i+1, neighbour j) at [j*ld + i+1]
+        const double* Fi = I.FT + (i + 1);
+        const double* Gi = I.GT + (i + 1);
+        const double* Ri = I.RT + (i + 1);
+        const double* Di = I.DT + (i + 1);
+        const double* P1i = I.P1T + i;
         const uint32_t* zlti = I.zlt + (size_t)(i + 1) * I.nw;
         const uint32_t* zlei = I.zle + (size_t)(i + 1) * I.nw;
         unsigned long long scan = 0, heavy = 0;
@@ -413,13 +402,13 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                 if ((self >> b) & 1u) continue;
                 const int j = (w << 5) + b;
                 if (COUNT) scan++;
-                const double Fj = Fi[j];
+                const double Fj = Fi[(size_t)j * ld];
                 const double sj = I.scores[j];
                 const bool nz = !((zl >> b) & 1u);
                 const bool fa = fin <= Fj;
                 if (need & kNeedNSFused) {
                     if (fa && nz) {
-                        const double Rj = Ri[j];
+                        const double Rj = Ri[(size_t)j * ld];
                         ns += Rj;
                         if (Rj > maxn) maxn = Rj;
                         if (Rj > r2v) {
@@ -427,7 +416,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                             r2j = j;
                         }
                         if (need & kNeedNSTW) {
-                            const double arrive = fin + Di[j];
+                            const double arrive = fin + Di[(size_t)j * ld];
                             double wait = I.open_t[j] - arrive;
                             if (wait < 0.0) wait = 0.0;
                             const double win = I.close_t[j] - I.open_t[j];
@@ -441,8 +430,8 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     if (((nowb >> b) & 1u) && !fa) regret += sj;
                 }
                 if (need & kNeedRob) {
-                    if (nz && frob <= Gi[j]) {
-                        const double Rj = Ri[j];
+                    if (nz && frob <= Gi[(size_t)j * ld]) {
+                        const double Rj = Ri[(size_t)j * ld];
                         nsrob += Rj;
                         if (Rj > r2rv) {
                             r2rv = Rj;
@@ -458,11 +447,11 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     }
                     if (fc) {
                         if (need & (kNeedStruct | kNeedPBust)) {
-                            const double aq = fin_c + Di[j];
+                            const double aq = fin_c + Di[(size_t)j * ld];
                             const double slack = I.close_t[j] - aq;
                             if (slack < smin) smin = slack;
                             if (!((ze >> b) & 1u)) {
-                                const double v = Ri[j];
+                                const double v = Ri[(size_t)j * ld];
                                 if (v > sbv) {
                                     sbv = v;
                                     sbq = j;
@@ -470,7 +459,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                             }
                         }
                         if (need & kNeedReachK) {
-                            const double v = Ri[j];
+                            const double v = Ri[(size_t)j * ld];
                             if (v > k1v) {
                                 k1v = v;
                                 k1q = j;
@@ -482,23 +471,43 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     if ((atb >> b) & 1u) {
                         if (COUNT) heavy++;
                         const double cj = I.close_t[j], oj = I.open_t[j];
-                        const double marr = fin_c + Di[j];
+                        const double marr = fin_c + Di[(size_t)j * ld];
+                        // norm_cdf(d/s) = 0.5*(1 + erf((d/s)*0.7071067811865476)).  The
+                        // reference's erf (glibc) is exactly +-1 for |x| >= 6, so for
+                        // |d| >= 8.5 s (x >= 6.01 after both roundings) the result is 1
+                        // or 0 with no erf call.
                         double pw;
-                        if (sd_c > 1e-9) pw = 0.5 * (1.0 + erf(((cj - marr) / sd_c) * 0.7071067811865476));
-                        else pw = marr <= cj ? 1.0 : 0.0;
-                        double mst, pv;
-                        if (marr > oj) {
-                            mst = marr;
-                            pv = P1i[j];
+                        const double dw = cj - marr;
+                        if (sd_c > 1e-9) {
+                            if (dw >= 8.5 * sd_c) pw = 1.0;
+                            else if (dw <= -8.5 * sd_c) pw = 0.0;
+                            else pw = 0.5 * (1.0 + erf((dw / sd_c) * 0.7071067811865476));
                         } else {
-                            mst = oj;
-                            pv = I.P0[j];
+                            pw = marr <= cj ? 1.0 : 0.0;
                         }
-                        const double mb = mst + I.durations[j] + I.d2d[j];
-                        double pb;
-                        if (pv >= 0.0) pb = 0.5 * (1.0 + erf(((tmax - mb) / pv) * 0.7071067811865476));
-                        else pb = mb <= tmax ? 1.0 : 0.0;
-                        eloss += sj * (1.0 - pw * pb);
+                        if (pw == 0.0) {
+                            eloss += sj * 1.0;  // sj * (1.0 - 0.0 * p_bud), p_bud finite
+                        } else {
+                            double mst, pv;
+                            if (marr > oj) {
+                                mst = marr;
+                                pv = P1i[(size_t)j * n];
+                            } else {
+                                mst = oj;
+                                pv = I.P0[j];
+                            }
+                            const double mb = mst + I.durations[j] + I.d2d[j];
+                            double pb;
+                            if (pv >= 0.0) {
+                                const double db = tmax - mb;
+                                if (db >= 8.5 * pv) pb = 1.0;
+                                else if (db <= -8.5 * pv) pb = 0.0;
+                                else pb = 0.5 * (1.0 + erf((db / pv) * 0.7071067811865476));
+                            } else {
+                                pb = mb <= tmax ? 1.0 : 0.0;
+                            }
+                            eloss += sj * (1.0 - pw * pb);
+                        }
                     }
                 }
             } while (bits);
@@ -516,20 +525,20 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         const double arrive = fin + I.dist[(size_t)(i + 1) * ld + r2j + 1];
         const double st = arrive > I.open_t[r2j] ? arrive : I.open_t[r2j];
         const double fj = st + I.durations[r2j];
-        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.F, r2j + 1, fj, i, r2j, wc.hop);
+        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.sFz, r2j + 1, fj, i, r2j, wc.hop);
     }
     if ((need & kNeedReach2Rob) && r2rj >= 0) {
         const double arrive = frob + I.dist[(size_t)(i + 1) * ld + r2rj + 1];
         const double st = arrive > I.open_t[r2rj] ? arrive : I.open_t[r2rj];
         const double fj = st + I.durations[r2rj] * (1.0 + kSigma);
-        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.G, r2rj + 1, fj, i, r2rj, wc.hop);
+        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.sGz, r2rj + 1, fj, i, r2rj, wc.hop);
     }
 
     // REACH-1/3/5 share one greedy path (each is the running total after
     // 1, 3 or 5 steps of the same walk, engine/sim_terms.hpp:405-441).
     double rk1 = 0.0, rk3 = 0.0, rk5 = 0.0;
     if (need & kNeedReachK) {
-        int path[5] = {i, -1, -1, -1, -1};
+        int p1 = -1, p2 = -1, p3 = -1, p4 = -1;  // the walk's customers after the candidate
         double tot = 0.0, tm = 0.0;
         int at = 0;
         bool alive = k1q >= 0;
@@ -539,12 +548,12 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
             tm = st + I.durations[k1q];
             at = k1q + 1;
             tot += I.scores[k1q];
-            path[1] = k1q;
+            p1 = k1q;
         }
         rk1 = tot;
         for (int step = 2; step <= rm.reach_k; step++) {
             if (alive) {
-                const int bq = reach_step<COUNT>(I, S, at, tm, path, step, wc.hop);
+                const int bq = reach_step<COUNT>(I, S, at, tm, i, p1, p2, p3, p4, wc.hop);
                 if (bq < 0) {
                     alive = false;
                 } else {
@@ -553,7 +562,9 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     tm = st + I.durations[bq];
                     at = bq + 1;
                     tot += I.scores[bq];
-                    if (step < 5) path[step] = bq;
+                    if (step == 2) p2 = bq;
+                    else if (step == 3) p3 = bq;
+                    else if (step == 4) p4 = bq;
                 }
             }
             if (step == 3) rk3 = tot;
@@ -814,7 +825,8 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) eval_kernel(const DevInst I, const DevBatch B) {
+__global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
+    eval_kernel(const DevInst I, const DevBatch B) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;

@@ -34,7 +34,7 @@ constexpr unsigned kFull = 0xffffffffu;
 #define SIDR_WARPS_PER_BLOCK 8
 #endif
 #ifndef SIDR_MIN_BLOCKS
-#define SIDR_MIN_BLOCKS 1
+#define SIDR_MIN_BLOCKS 2
 #endif
 
 // Shared-memory slice of one warp.

@@ -453,13 +453,14 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
     I.ld = h.n + 1;
     I.nw = h.nw;
     I.tmax = h.tmax;
+    I.ns = h.ns;
     struct Item { const void* src; size_t bytes; const void** dst; };
     const Item items[] = {
-        {h.scores.data(), h.n * 8, (const void**)&I.scores},
-        {h.durations.data(), h.n * 8, (const void**)&I.durations},
-        {h.open_t.data(), h.n * 8, (const void**)&I.open_t},
-        {h.close_t.data(), h.n * 8, (const void**)&I.close_t},
-        {h.d2d.data(), h.n * 8, (const void**)&I.d2d},
+        {h.scores.data(), (size_t)h.n * 8, (const void**)&I.scores},
+        {h.durations.data(), (size_t)h.n * 8, (const void**)&I.durations},
+        {h.open_t.data(), (size_t)h.n * 8, (const void**)&I.open_t},
+        {h.close_t.data(), (size_t)h.n * 8, (const void**)&I.close_t},
+        {h.d2d.data(), (size_t)h.n * 8, (const void**)&I.d2d},
         {h.dist.data(), h.dist.size() * 8, (const void**)&I.dist},
         {h.F.data(), h.F.size() * 8, (const void**)&I.F},
         {h.G.data(), h.G.size() * 8, (const void**)&I.G},
@@ -468,10 +469,8 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         {h.P0.data(), h.P0.size() * 8, (const void**)&I.P0},
         {h.zlt.data(), h.zlt.size() * 4, (const void**)&I.zlt},
         {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle},
-        {h.FT.data(), h.FT.size() * 8, (const void**)&I.FT},
-        {h.GT.data(), h.GT.size() * 8, (const void**)&I.GT},
-        {h.RT.data(), h.RT.size() * 8, (const void**)&I.RT},
-        {h.DT.data(), h.DT.size() * 8, (const void**)&I.DT},
+        {h.FR.data(), h.FR.size() * 8, (const void**)&I.FR},
+        {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
         {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
         {h.sR.data(), h.sR.size() * 8, (const void**)&I.sR},
@@ -680,3 +679,14 @@ void sidr_batch_destroy(sidr_batch* bt) {
 }
 
 }  // extern "C"
+
+#ifdef SIDR_SECTION_CLOCKS
+// Profiling builds only: read (and clear) the per-section cycle totals.
+extern "C" int sidr_section_cycles_take(unsigned long long* out16) {
+    if (cudaMemcpyFromSymbol(out16, sidr::sidr_section_cycles, 16 * sizeof(unsigned long long)) !=
+        cudaSuccess)
+        return 1;
+    static const unsigned long long zero[16] = {};
+    return cudaMemcpyToSymbol(sidr::sidr_section_cycles, zero, sizeof zero) == cudaSuccess ? 0 : 1;
+}
+#endif

@@ -200,28 +200,30 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
             h.P1[(size_t)c * n + j] = vb > 1e-18 ? std::pow(vb, 0.5) : -1.0;
         }
     }
-    // Neighbour-major copies.
-    h.FT.assign(rows, 0.0);
-    h.GT.assign(rows, 0.0);
-    h.RT.assign(rows, 0.0);
-    h.DT.assign(rows, 0.0);
+    // Neighbour-major pair tables: {F, R} and {G, dist} of (origin o,
+    // neighbour j) at pair index j*ld + o.
+    h.FR.assign(2 * rows, 0.0);
+    h.GD.assign(2 * rows, 0.0);
     h.P1T.assign((size_t)n * n, 0.0);
     for (int o = 0; o < ld; o++)
         for (int j = 0; j < n; j++) {
-            const size_t a = (size_t)o * n + j, t = (size_t)j * ld + o;
-            h.FT[t] = h.F[a];
-            h.GT[t] = h.G[a];
-            h.RT[t] = h.R[a];
-            h.DT[t] = D(h, o, j + 1);
+            const size_t a = (size_t)o * n + j, t = 2 * ((size_t)j * ld + o);
+            h.FR[t] = h.F[a];
+            h.FR[t + 1] = h.R[a];
+            h.GD[t] = h.G[a];
+            h.GD[t + 1] = D(h, o, j + 1);
         }
     for (int c = 0; c < n; c++)
         for (int j = 0; j < n; j++) h.P1T[(size_t)j * n + c] = h.P1[(size_t)c * n + j];
-    // Per-origin neighbour lists by (R desc, index asc).
-    h.ord.assign(rows, 0);
-    h.sR.assign(rows, 0.0);
-    h.sF.assign(rows, 0.0);
-    h.sFz.assign(rows, 0.0);
-    h.sGz.assign(rows, 0.0);
+    // Per-origin neighbour lists by (R desc, index asc), rows padded to a
+    // multiple of 4 entries with a ratio of -inf that ends every scan.
+    h.ns = (n + 3) / 4 * 4;
+    const size_t srows = (size_t)ld * h.ns;
+    h.ord.assign(srows, 0);
+    h.sR.assign(srows, -INFINITY);
+    h.sF.assign(srows, -INFINITY);
+    h.sFz.assign(srows, -INFINITY);
+    h.sGz.assign(srows, -INFINITY);
     std::vector<int> idx(n);
     for (int o = 0; o < ld; o++) {
         const double* Ro = h.R.data() + (size_t)o * n;
@@ -229,7 +231,7 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
         std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return Ro[a] > Ro[b]; });
         for (int k = 0; k < n; k++) {
             const int j = idx[k];
-            const size_t a = (size_t)o * n + j, s = (size_t)o * n + k;
+            const size_t a = (size_t)o * n + j, s = (size_t)o * h.ns + k;
             const bool coincident = (h.zlt[(size_t)o * h.nw + (j >> 5)] >> (j & 31)) & 1u;
             h.ord[s] = (int16_t)j;
             h.sR[s] = h.R[a];

@@ -40,21 +40,24 @@ constexpr double kSqrt2 = 1.4142135623730951; // SQRT2_C, engine/sim_terms.hpp:1
 //                var <= 1e-18 (the reference's deterministic branch).
 //
 // Two further layouts of the same values serve the two access patterns:
-//   * neighbour-major copies FT/GT/RT/DT[j*ld + o] (DT = dist[o][j+1]) and
-//     P1T[j*n + c]: in the fused candidate scan all lanes visit the same
-//     neighbour j from different origins, so one warp load stays in one row;
-//   * per-origin neighbour lists ord[o*n + k] sorted by (R desc, index asc),
-//     with sR/sF (R and F in that order) and sFz/sGz (F and G, -inf on
-//     coincident pairs): a greedy "best feasible neighbour by ratio" search --
-//     strict > over ascending index, as in REACH-k and REACH2's second hop --
-//     returns the first feasible entry of the sorted list, so it stops early.
+//   * neighbour-major pair tables FR = {F, R} and GD = {G, dist[o][j+1]} at
+//     pair index j*ld + o, and P1T[j*n + c]: in the fused candidate scan all
+//     lanes visit the same neighbour j from different origins, so one warp's
+//     16-byte loads stay in one row;
+//   * per-origin neighbour lists ord[o*ns + k] sorted by (R desc, index asc),
+//     rows padded to ns = a multiple of 4 with ratio -inf, with sR/sF (R and F
+//     in that order) and sFz/sGz (F and G, -inf on coincident pairs): a greedy
+//     "best feasible neighbour by ratio" search -- strict > over ascending
+//     index, as in REACH-k and REACH2's second hop -- returns the first
+//     feasible entry of the sorted list, so it stops early.
 struct DevInst {
     int n, m, ld, nw;
     double tmax;
     const double *scores, *durations, *open_t, *close_t, *d2d, *dist;
     const double *F, *G, *R, *P1, *P0;
     const uint32_t *zlt, *zle;
-    const double *FT, *GT, *RT, *DT, *P1T;
+    const double *FR, *GD, *P1T;  // FR/GD: interleaved pairs
+    int ns;                        // sorted-list row stride
     const int16_t* ord;
     const double *sR, *sF, *sFz, *sGz;
     const double* zp;  // [10]

@@ -31,10 +31,30 @@ constexpr unsigned kFull = 0xffffffffu;
 // Block shape of the evaluator: warps per block and the minimum resident
 // blocks per SM that bound its registers (__launch_bounds__).
 #ifndef SIDR_WARPS_PER_BLOCK
-#define SIDR_WARPS_PER_BLOCK 8
+#define SIDR_WARPS_PER_BLOCK 4
 #endif
 #ifndef SIDR_MIN_BLOCKS
-#define SIDR_MIN_BLOCKS 2
+#define SIDR_MIN_BLOCKS 3
+#endif
+
+// Section-cycle hooks for profiling builds only (-DSIDR_SECTION_CLOCKS): the
+// first active lane of each warp adds the cycles spent in a section to
+// sidr_section_cycles[].  In normal builds they compile to nothing.
+#ifdef SIDR_SECTION_CLOCKS
+__device__ unsigned long long sidr_section_cycles[16];
+#define SIDR_SEC_MARK(var)      \
+    __syncwarp(__activemask()); \
+    const long long var = clock64();
+#define SIDR_SEC_ADD(idx, var)                                                             \
+    do {                                                                                   \
+        const unsigned am_ = __activemask();                                               \
+        __syncwarp(am_);                                                                   \
+        if ((threadIdx.x & 31) == __ffs(am_) - 1)                                          \
+            atomicAdd(&sidr_section_cycles[idx], (unsigned long long)(clock64() - (var))); \
+    } while (0)
+#else
+#define SIDR_SEC_MARK(var)
+#define SIDR_SEC_ADD(idx, var)
 #endif
 
 // Shared-memory slice of one warp.
@@ -102,6 +122,30 @@ __device__ __forceinline__ uint32_t bit_in_word(int node, int w) {
     return (node >= 0 && (node >> 5) == w) ? (1u << (node & 31)) : 0u;
 }
 
+// The sorted neighbour lists are read four entries at a time: 32-byte ratio
+// and threshold chunks, one 8-byte chunk of four customer indices.
+struct Chunk4 {
+    double r[4], t[4];
+    int q[4];
+};
+
+__device__ __forceinline__ Chunk4 load_chunk(const double* sR, const double* sT,
+                                             const int16_t* ord, int k) {
+    Chunk4 c;
+    const double2 r01 = *reinterpret_cast<const double2*>(sR + k);
+    const double2 r23 = *reinterpret_cast<const double2*>(sR + k + 2);
+    const double2 t01 = *reinterpret_cast<const double2*>(sT + k);
+    const double2 t23 = *reinterpret_cast<const double2*>(sT + k + 2);
+    const uint2 qq = *reinterpret_cast<const uint2*>(ord + k);
+    c.r[0] = r01.x; c.r[1] = r01.y; c.r[2] = r23.x; c.r[3] = r23.y;
+    c.t[0] = t01.x; c.t[1] = t01.y; c.t[2] = t23.x; c.t[3] = t23.y;
+    c.q[0] = (int)(int16_t)(qq.x & 0xffffu);
+    c.q[1] = (int)(int16_t)(qq.x >> 16);
+    c.q[2] = (int)(int16_t)(qq.y & 0xffffu);
+    c.q[3] = (int)(int16_t)(qq.y >> 16);
+    return c;
+}
+
 // REACH2's second loop (engine/sim_terms.hpp:112-126, robust :175-189): the
 // best unvisited customer outside {x0, x1} by score/time from origin node o at
 // time tm, skipping coincident locations, init 0.0.  `table` is sFz (standard)
@@ -111,38 +155,45 @@ __device__ __forceinline__ uint32_t bit_in_word(int node, int w) {
 template <bool COUNT>
 __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const double* table,
                                    int o, double tm, int x0, int x1, unsigned long long& hops) {
-    const int n = I.n;
-    const int16_t* ord = I.ord + (size_t)o * n;
-    const double* sR = I.sR + (size_t)o * n;
-    const double* sT = table + (size_t)o * n;
-    for (int k = 0; k < n; k++) {
-        if (!(sR[k] > 0.0)) break;
-        const int q = ord[k];
-        if (COUNT) hops++;
-        if (q == x0 || q == x1 || !is_unvisited(S, q)) continue;
-        if (tm <= sT[k]) return I.scores[q];
+    const size_t row = (size_t)o * I.ns;
+    const int16_t* ord = I.ord + row;
+    const double* sR = I.sR + row;
+    const double* sT = table + row;
+    for (int k = 0; k < I.ns; k += 4) {
+        const Chunk4 c = load_chunk(sR, sT, ord, k);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            if (!(c.r[e] > 0.0)) return 0.0;
+            if (COUNT) hops++;
+            const int q = c.q[e];
+            if (q != x0 && q != x1 && is_unvisited(S, q) && tm <= c.t[e]) return I.scores[q];
+        }
     }
     return 0.0;
 }
 
 // One REACH-k greedy step (engine/sim_terms.hpp:415-431): the best unvisited
-// customer outside the path by score/max(t,1e-10) under the standard test, no
+// customer outside the walk by score/max(t,1e-10) under the standard test, no
 // coincident skip, init -1.0 -- the first feasible entry of o's sorted list
-// whose ratio exceeds -1.0.
+// whose ratio exceeds -1.0.  p0..p4: the walk so far (-1 = unused).
 template <bool COUNT>
 __device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm, int p0, int p1,
                           int p2, int p3, int p4, unsigned long long& hops) {
-    // p0..p4: the walk so far (candidate first; -1 = unused)
-    const int n = I.n;
-    const int16_t* ord = I.ord + (size_t)o * n;
-    const double* sR = I.sR + (size_t)o * n;
-    const double* sF = I.sF + (size_t)o * n;
-    for (int k = 0; k < n; k++) {
-        if (!(sR[k] > -1.0)) break;
-        const int q = ord[k];
-        if (COUNT) hops++;
-        if (!is_unvisited(S, q) || q == p0 || q == p1 || q == p2 || q == p3 || q == p4) continue;
-        if (tm <= sF[k]) return q;
+    const size_t row = (size_t)o * I.ns;
+    const int16_t* ord = I.ord + row;
+    const double* sR = I.sR + row;
+    const double* sF = I.sF + row;
+    for (int k = 0; k < I.ns; k += 4) {
+        const Chunk4 c = load_chunk(sR, sF, ord, k);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            if (!(c.r[e] > -1.0)) return -1;
+            if (COUNT) hops++;
+            const int q = c.q[e];
+            if (q != p0 && q != p1 && q != p2 && q != p3 && q != p4 && is_unvisited(S, q) &&
+                tm <= c.t[e])
+                return q;
+        }
     }
     return -1;
 }
@@ -359,6 +410,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
     const double ct = d.ct;
     const int cur = d.cur;
 
+    SIDR_SEC_MARK(t_setup)
     const double ta = I.dist[(size_t)cur * ld + i + 1];
     const double open_i = I.open_t[i], close_i = I.close_t[i];
     const double dur_i = I.durations[i], sc_i = I.scores[i], d2d_i = I.d2d[i];
@@ -378,139 +430,151 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
     double fcnt = 0.0, fsc = 0.0, smin = 1e18, sbv = -1.0, k1v = -1.0, eloss = 0.0;
     int r2j = -1, r2rj = -1, sbq = -1, k1q = -1;
 
+    SIDR_SEC_ADD(2, t_setup);
+    SIDR_SEC_MARK(t_fused)
     const uint32_t fused = kNeedNSFused | kNeedRegret | kNeedRob | kNeedAfterC | kNeedAtRisk;
     if (need & fused) {
-        // neighbour-major tables: entry (origin i+1, neighbour j) at [j*ld + i+1]
-        const double* Fi = I.FT + (i + 1);
-        const double* Gi = I.GT + (i + 1);
-        const double* Ri = I.RT + (i + 1);
-        const double* Di = I.DT + (i + 1);
+        // neighbour-major pairs of origin i+1: {F, R} and {G, dist} at j*ld + i+1
+        const double2* FRi = reinterpret_cast<const double2*>(I.FR) + (i + 1);
+        const double2* GDi = reinterpret_cast<const double2*>(I.GD) + (i + 1);
+        const bool need_gd =
+            (need & (kNeedRob | kNeedNSTW | kNeedStruct | kNeedPBust | kNeedAtRisk)) != 0;
         const double* P1i = I.P1T + i;
         const uint32_t* zlti = I.zlt + (size_t)(i + 1) * I.nw;
         const uint32_t* zlei = I.zle + (size_t)(i + 1) * I.nw;
         unsigned long long scan = 0, heavy = 0;
+
+        // One neighbour j (bit b of its word): every accumulator is updated in
+        // ascending j, as each reference loop runs.
+        auto visit = [&](int j, int b, double2 fr, double2 gd, uint32_t zl, uint32_t ze,
+                         uint32_t nowb, uint32_t atb) {
+            if (COUNT) scan++;
+            const double Fj = fr.x, Rj = fr.y;
+            const double sj = I.scores[j];
+            const bool nz = !((zl >> b) & 1u);
+            const bool fa = fin <= Fj;
+            if (need & kNeedNSFused) {
+                if (fa && nz) {
+                    ns += Rj;
+                    if (Rj > maxn) maxn = Rj;
+                    if (Rj > r2v) {
+                        r2v = Rj;
+                        r2j = j;
+                    }
+                    if (need & kNeedNSTW) {
+                        const double arrive = fin + gd.y;
+                        double wait = I.open_t[j] - arrive;
+                        if (wait < 0.0) wait = 0.0;
+                        const double win = I.close_t[j] - I.open_t[j];
+                        double wt = win > 1e-10 ? 1.0 - wait / win : 1.0;
+                        if (wt < 0.0) wt = 0.0;
+                        nstw += Rj * wt;
+                    }
+                }
+            }
+            if (need & kNeedRegret) {
+                if (((nowb >> b) & 1u) && !fa) regret += sj;
+            }
+            if (need & kNeedRob) {
+                if (nz && frob <= gd.x) {
+                    nsrob += Rj;
+                    if (Rj > r2rv) {
+                        r2rv = Rj;
+                        r2rj = j;
+                    }
+                }
+            }
+            if (need & kNeedAfterC) {
+                const bool fc = fin_c <= Fj;
+                if ((need & kNeedStruct) && ((nowb >> b) & 1u) && !fc) {
+                    fcnt += 1.0;
+                    fsc += sj;
+                }
+                if (fc) {
+                    if (need & (kNeedStruct | kNeedPBust)) {
+                        const double aq = fin_c + gd.y;
+                        const double slack = I.close_t[j] - aq;
+                        if (slack < smin) smin = slack;
+                        if (!((ze >> b) & 1u) && Rj > sbv) {
+                            sbv = Rj;
+                            sbq = j;
+                        }
+                    }
+                    if ((need & kNeedReachK) && Rj > k1v) {
+                        k1v = Rj;
+                        k1q = j;
+                    }
+                }
+            }
+            if (need & kNeedAtRisk) {
+                if ((atb >> b) & 1u) {
+                    if (COUNT) heavy++;
+                    const double cj = I.close_t[j], oj = I.open_t[j];
+                    const double marr = fin_c + gd.y;
+                    // norm_cdf(d/s) = 0.5*(1 + erf((d/s)*0.7071067811865476)).  The
+                    // reference's erf (glibc) is exactly +-1 for |x| >= 6, so for
+                    // |d| >= 8.5 s (x >= 6.01 after both roundings) the result is 1
+                    // or 0 with no erf call.
+                    double pw;
+                    const double dw = cj - marr;
+                    if (sd_c > 1e-9) {
+                        if (dw >= 8.5 * sd_c) pw = 1.0;
+                        else if (dw <= -8.5 * sd_c) pw = 0.0;
+                        else pw = 0.5 * (1.0 + erf((dw / sd_c) * 0.7071067811865476));
+                    } else {
+                        pw = marr <= cj ? 1.0 : 0.0;
+                    }
+                    if (pw == 0.0) {
+                        eloss += sj * 1.0;  // sj * (1.0 - 0.0 * p_bud), p_bud finite
+                    } else {
+                        double mst, pv;
+                        if (marr > oj) {
+                            mst = marr;
+                            pv = P1i[(size_t)j * n];
+                        } else {
+                            mst = oj;
+                            pv = I.P0[j];
+                        }
+                        const double mb = mst + I.durations[j] + I.d2d[j];
+                        double pb;
+                        if (pv >= 0.0) {
+                            const double db = tmax - mb;
+                            if (db >= 8.5 * pv) pb = 1.0;
+                            else if (db <= -8.5 * pv) pb = 0.0;
+                            else pb = 0.5 * (1.0 + erf((db / pv) * 0.7071067811865476));
+                        } else {
+                            pb = mb <= tmax ? 1.0 : 0.0;
+                        }
+                        eloss += sj * (1.0 - pw * pb);
+                    }
+                }
+            }
+        };
+
         for (int w = 0; w < I.nw; w++) {
-            uint32_t bits = S.unv[w];
+            uint32_t bits = S.unv[w] & ~bit_in_word(i, w);
             if (!bits) continue;
-            const uint32_t self = bit_in_word(i, w);
             const uint32_t zl = zlti[w], ze = zlei[w];
             const uint32_t nowb = S.feas[w];
             const uint32_t atb = S.atr[w];
-            do {
-                const int b = __ffs(bits) - 1;
+            // two neighbours per iteration, both loads issued before either visit
+            while (bits) {
+                const int b0 = __ffs(bits) - 1;
                 bits &= bits - 1;
-                if ((self >> b) & 1u) continue;
-                const int j = (w << 5) + b;
-                if (COUNT) scan++;
-                const double Fj = Fi[(size_t)j * ld];
-                const double sj = I.scores[j];
-                const bool nz = !((zl >> b) & 1u);
-                const bool fa = fin <= Fj;
-                if (need & kNeedNSFused) {
-                    if (fa && nz) {
-                        const double Rj = Ri[(size_t)j * ld];
-                        ns += Rj;
-                        if (Rj > maxn) maxn = Rj;
-                        if (Rj > r2v) {
-                            r2v = Rj;
-                            r2j = j;
-                        }
-                        if (need & kNeedNSTW) {
-                            const double arrive = fin + Di[(size_t)j * ld];
-                            double wait = I.open_t[j] - arrive;
-                            if (wait < 0.0) wait = 0.0;
-                            const double win = I.close_t[j] - I.open_t[j];
-                            double wt = win > 1e-10 ? 1.0 - wait / win : 1.0;
-                            if (wt < 0.0) wt = 0.0;
-                            nstw += Rj * wt;
-                        }
-                    }
+                const bool has1 = bits != 0;
+                const int b1 = has1 ? __ffs(bits) - 1 : b0;
+                bits &= bits - 1;
+                const int j0 = (w << 5) + b0, j1 = (w << 5) + b1;
+                const double2 fr0 = FRi[(size_t)j0 * ld];
+                const double2 fr1 = FRi[(size_t)j1 * ld];
+                double2 gd0 = make_double2(0.0, 0.0), gd1 = gd0;
+                if (need_gd) {
+                    gd0 = GDi[(size_t)j0 * ld];
+                    gd1 = GDi[(size_t)j1 * ld];
                 }
-                if (need & kNeedRegret) {
-                    if (((nowb >> b) & 1u) && !fa) regret += sj;
-                }
-                if (need & kNeedRob) {
-                    if (nz && frob <= Gi[(size_t)j * ld]) {
-                        const double Rj = Ri[(size_t)j * ld];
-                        nsrob += Rj;
-                        if (Rj > r2rv) {
-                            r2rv = Rj;
-                            r2rj = j;
-                        }
-                    }
-                }
-                if (need & kNeedAfterC) {
-                    const bool fc = fin_c <= Fj;
-                    if ((need & kNeedStruct) && ((nowb >> b) & 1u) && !fc) {
-                        fcnt += 1.0;
-                        fsc += sj;
-                    }
-                    if (fc) {
-                        if (need & (kNeedStruct | kNeedPBust)) {
-                            const double aq = fin_c + Di[(size_t)j * ld];
-                            const double slack = I.close_t[j] - aq;
-                            if (slack < smin) smin = slack;
-                            if (!((ze >> b) & 1u)) {
-                                const double v = Ri[(size_t)j * ld];
-                                if (v > sbv) {
-                                    sbv = v;
-                                    sbq = j;
-                                }
-                            }
-                        }
-                        if (need & kNeedReachK) {
-                            const double v = Ri[(size_t)j * ld];
-                            if (v > k1v) {
-                                k1v = v;
-                                k1q = j;
-                            }
-                        }
-                    }
-                }
-                if (need & kNeedAtRisk) {
-                    if ((atb >> b) & 1u) {
-                        if (COUNT) heavy++;
-                        const double cj = I.close_t[j], oj = I.open_t[j];
-                        const double marr = fin_c + Di[(size_t)j * ld];
-                        // norm_cdf(d/s) = 0.5*(1 + erf((d/s)*0.7071067811865476)).  The
-                        // reference's erf (glibc) is exactly +-1 for |x| >= 6, so for
-                        // |d| >= 8.5 s (x >= 6.01 after both roundings) the result is 1
-                        // or 0 with no erf call.
-                        double pw;
-                        const double dw = cj - marr;
-                        if (sd_c > 1e-9) {
-                            if (dw >= 8.5 * sd_c) pw = 1.0;
-                            else if (dw <= -8.5 * sd_c) pw = 0.0;
-                            else pw = 0.5 * (1.0 + erf((dw / sd_c) * 0.7071067811865476));
-                        } else {
-                            pw = marr <= cj ? 1.0 : 0.0;
-                        }
-                        if (pw == 0.0) {
-                            eloss += sj * 1.0;  // sj * (1.0 - 0.0 * p_bud), p_bud finite
-                        } else {
-                            double mst, pv;
-                            if (marr > oj) {
-                                mst = marr;
-                                pv = P1i[(size_t)j * n];
-                            } else {
-                                mst = oj;
-                                pv = I.P0[j];
-                            }
-                            const double mb = mst + I.durations[j] + I.d2d[j];
-                            double pb;
-                            if (pv >= 0.0) {
-                                const double db = tmax - mb;
-                                if (db >= 8.5 * pv) pb = 1.0;
-                                else if (db <= -8.5 * pv) pb = 0.0;
-                                else pb = 0.5 * (1.0 + erf((db / pv) * 0.7071067811865476));
-                            } else {
-                                pb = mb <= tmax ? 1.0 : 0.0;
-                            }
-                            eloss += sj * (1.0 - pw * pb);
-                        }
-                    }
-                }
-            } while (bits);
+                visit(j0, b0, fr0, gd0, zl, ze, nowb, atb);
+                if (has1) visit(j1, b1, fr1, gd1, zl, ze, nowb, atb);
+            }
         }
         if (COUNT) {
             wc.scan += scan;
@@ -519,6 +583,8 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         }
     }
 
+    SIDR_SEC_ADD(3, t_fused);
+    SIDR_SEC_MARK(t_hops)
     // REACH2 / REACH2ROB second hops.
     double reach2 = 0.0, reach2rob = 0.0;
     if ((need & kNeedReach2) && r2j >= 0) {
@@ -572,6 +638,8 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         }
     }
 
+    SIDR_SEC_ADD(4, t_hops);
+    SIDR_SEC_MARK(t_pbust)
     double pbust = 0.0;
     if ((need & kNeedPBust) && sbq >= 0) {
         const double ab = fin_c + I.dist[(size_t)(i + 1) * ld + sbq + 1];
@@ -585,6 +653,8 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
     }
     const double downslack = smin > 1e17 ? 0.0 : smin;
 
+    SIDR_SEC_ADD(5, t_pbust);
+    SIDR_SEC_MARK(t_rows)
     // Terminal rows.
     for (int k = 0; k < rm.K; k++) {
         const int slot = S.slots[k];
@@ -666,6 +736,8 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         S.rows[k * 32 + lane] = v;
     }
 
+    SIDR_SEC_ADD(6, t_rows);
+    SIDR_SEC_MARK(t_prog)
     // Rule program (engine/sim_core.hpp:11-41 as three-address code).
     for (int q = 0; q < rm.n_ins; q++) {
         const uint32_t wd = S.prog[q];
@@ -691,6 +763,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         }
         S.rows[od * 32 + lane] = r;
     }
+    SIDR_SEC_ADD(7, t_prog);
     const uint32_t res = (uint32_t)rm.res;
     double pri = (res & kOpConst) ? S.cst[res & 511u] : S.rows[res * 32 + lane];
     if (pri != pri) pri = -1e300;
@@ -706,6 +779,7 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
     const uint32_t need = rm.need;
     const bool need_atr = (need & kNeedAtRisk) != 0;
 
+    SIDR_SEC_MARK(t_prep)
     // Feasible-now bitmask (the reference's candidate filter, :75-82) and
     // ATRISK's arrive-by-close filter, one ballot per 32 customers.
     const double* Fc = I.F + (size_t)d.cur * n;
@@ -727,6 +801,8 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
     }
     __syncwarp();
 
+    SIDR_SEC_ADD(0, t_prep);
+    SIDR_SEC_MARK(t_compact)
     int ncand = 0;
     for (int w = 0; w < nw; w++) {
         const uint32_t bits = S.feas[w];
@@ -763,6 +839,7 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         wc.ops += 2ull * n;
     }
 
+    SIDR_SEC_ADD(1, t_compact);
     int best = -1;
     double best_pri = -1e300;
     for (int base = 0; base < ncand; base += 32) {
@@ -773,6 +850,7 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
             idx = S.cand[k];
             pri = score_candidate<COUNT>(I, S, rm, d, idx, wc);
         }
+        SIDR_SEC_MARK(t_argmax)
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             const double op = __shfl_xor_sync(kFull, pri, off);
@@ -786,6 +864,7 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
             best_pri = pri;
             best = idx;
         }
+        SIDR_SEC_ADD(8, t_argmax);
     }
     return best;
 }
@@ -812,6 +891,7 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
         for (;;) {
             const int b = decide<COUNT>(I, S, rm, d, wc);
             if (b < 0) break;
+            SIDR_SEC_MARK(t_upd)
             const double arrive = d.ct + I.dist[(size_t)d.cur * ld + b + 1];
             const double st = arrive > I.open_t[b] ? arrive : I.open_t[b];
             d.ct = st + smp[b];
@@ -819,6 +899,7 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
             total += I.scores[b];
             if (lane == 0) S.unv[b >> 5] &= ~(1u << (b & 31));
             __syncwarp();
+            SIDR_SEC_ADD(9, t_upd);
         }
     }
     return total;

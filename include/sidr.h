@@ -158,6 +158,32 @@ sidr_status sidr_batch_counts(sidr_batch* b, sidr_counts* out);
 sidr_status sidr_rules_check(const sidr_rules_desc* rules, const int64_t* masks,
                              int32_t mask_group, int32_t* max_rows);
 
+/* Evaluation that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: code whose device
+ * memory belongs to another allocator (a framework's caching pool that must
+ * not be bypassed), or that must not pay cudaMalloc/cudaFree's implicit
+ * device synchronisation on every call.  Same meaning as
+ * sidr_evaluate_grouped_masks, but without a context: the instance, zp,
+ * rules, scenarios, masks and out are all HOST buffers, and everything the
+ * evaluator keeps on the device -- the instance's lookup tables, the compiled
+ * rules, the scenarios, the work-queue counter and the scores before they are
+ * copied back -- is placed in one file-scope static device array of
+ * SIDR_STATIC_SCRATCH_BYTES, which every GPU that loads the library holds
+ * until the process exits.  Limits: n <= SIDR_STATIC_MAX_N, and all of the
+ * above must fit the array; larger calls return SIDR_ERR_TOO_LARGE with the
+ * sizes in sidr_last_error().  The first call on a device looks up the
+ * array's device address there.  All calls in a process share the one array,
+ * which keeps the last call's contents; each call clears what must start at
+ * zero.  Calls that overlapped on the GPU would race on the array, so each
+ * call holds a process-wide lock from its first copy to its last and returns
+ * only after the scores are in `out`. */
+#define SIDR_STATIC_SCRATCH_BYTES (16u << 20)
+#define SIDR_STATIC_MAX_N 128
+sidr_status sidr_evaluate_static(const sidr_instance_desc* inst, const double zp[10],
+                                 const sidr_rules_desc* rules, const double* grouped_sampled,
+                                 int32_t G, int32_t T, int32_t group_size, int32_t mask_group,
+                                 const int64_t* masks, int32_t device, double* out);
+
 /* Number of kernel launches issued by this library since load (evaluator
  * and per-rule fitness kernels). */
 int64_t sidr_kernel_launches(void);

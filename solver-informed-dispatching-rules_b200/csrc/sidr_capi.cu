@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -690,3 +691,172 @@ extern "C" int sidr_section_cycles_take(unsigned long long* out16) {
     return cudaMemcpyToSymbol(sidr::sidr_section_cycles, zero, sizeof zero) == cudaSuccess ? 0 : 1;
 }
 #endif
+
+// ----------------------------------------------------------------------------
+// Evaluation without device allocation (sidr_evaluate_static).
+//
+// For callers that cannot call cudaMalloc -- their device memory belongs to
+// another allocator, or they must not pay cudaMalloc/cudaFree's implicit device
+// synchronisation per call.  Everything the evaluator keeps on the device for
+// one call lives in this file-scope array, which every GPU that loads the
+// library holds until the process exits.  In host code the name
+// sidr_static_scratch is only a host-side stand-in, not a device address: the
+// address comes from cudaGetSymbolAddress, looked up once per device with that
+// device current, and is passed to the kernel inside DevInst/DevBatch.
+
+namespace {
+
+static __device__ __align__(256) unsigned char sidr_static_scratch[SIDR_STATIC_SCRATCH_BYTES];
+
+std::mutex g_static_lock;                 // serialises every use of the array
+unsigned char* g_static_ptr[256] = {};    // device address per device index
+
+// Byte layout of one call inside the array.
+struct StaticLayout {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        const size_t at = off;
+        off = align_up(off + (bytes ? bytes : 1), 256);
+        return at;
+    }
+};
+
+}  // namespace
+
+extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const double zp[10],
+                                            const sidr_rules_desc* r, const double* sampled,
+                                            int32_t G, int32_t T, int32_t group_size,
+                                            int32_t mask_group, const int64_t* masks,
+                                            int32_t device, double* out) {
+    g_h2d = g_d2h = 0;
+    if (!d || !zp) return fail(SIDR_ERR_INVALID, "null argument");
+    if (d->n > SIDR_STATIC_MAX_N)
+        return fail(SIDR_ERR_TOO_LARGE, "sidr_evaluate_static: n = " + std::to_string(d->n) +
+                                            " exceeds SIDR_STATIC_MAX_N = " +
+                                            std::to_string(SIDR_STATIC_MAX_N));
+    sidr_status s = check_rules(r);
+    if (s) return s;
+    s = check_grouping(r, sampled, G, T, group_size, mask_group, masks);
+    if (s) return s;
+    if (r->P > 0 && T > 0 && !out) return fail(SIDR_ERR_INVALID, "output buffer is null");
+    for (int k = 0; k < 10; k++)
+        if (std::isnan(zp[k])) return fail(SIDR_ERR_NONFINITE, "zp holds NaN");
+    const int P = r->P;
+    if ((long long)P * T == 0) return SIDR_OK;
+    HostInstance h;
+    std::string e = build_instance(d->n, d->m, d->tmax, d->scores, d->durations, d->open_t,
+                                   d->close_t, d->dist, d->dist_to_depot, h, true);
+    if (!e.empty())
+        return fail(e.find("finite") != std::string::npos ? SIDR_ERR_NONFINITE : SIDR_ERR_INVALID, e);
+    const size_t n_smp = (size_t)((P - 1) / group_size + 1) * T * h.n;
+    s = check_finite(sampled, n_smp);
+    if (s) return s;
+    HostPrograms hp;
+    s = compile_all(r, masks, mask_group, hp);
+    if (s) return s;
+
+    // Place every device-side array of this call in the scratch.
+    struct Piece { const void* src; size_t bytes; const void** dst; size_t at; };
+    DevInst I{};
+    DevBatch b{};
+    std::vector<Piece> up = {
+        {h.scores.data(), (size_t)h.n * 8, (const void**)&I.scores, 0},
+        {h.durations.data(), (size_t)h.n * 8, (const void**)&I.durations, 0},
+        {h.open_t.data(), (size_t)h.n * 8, (const void**)&I.open_t, 0},
+        {h.close_t.data(), (size_t)h.n * 8, (const void**)&I.close_t, 0},
+        {h.d2d.data(), (size_t)h.n * 8, (const void**)&I.d2d, 0},
+        {h.dist.data(), h.dist.size() * 8, (const void**)&I.dist, 0},
+        {h.F.data(), h.F.size() * 8, (const void**)&I.F, 0},
+        {h.G.data(), h.G.size() * 8, (const void**)&I.G, 0},
+        {h.R.data(), h.R.size() * 8, (const void**)&I.R, 0},
+        {h.P1.data(), h.P1.size() * 8, (const void**)&I.P1, 0},
+        {h.P0.data(), h.P0.size() * 8, (const void**)&I.P0, 0},
+        {h.zlt.data(), h.zlt.size() * 4, (const void**)&I.zlt, 0},
+        {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle, 0},
+        {h.FR.data(), h.FR.size() * 8, (const void**)&I.FR, 0},
+        {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD, 0},
+        {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T, 0},
+        {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord, 0},
+        {h.sR.data(), h.sR.size() * 8, (const void**)&I.sR, 0},
+        {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF, 0},
+        {h.sFz.data(), h.sFz.size() * 8, (const void**)&I.sFz, 0},
+        {h.sGz.data(), h.sGz.size() * 8, (const void**)&I.sGz, 0},
+        {zp, 80, (const void**)&I.zp, 0},
+        {hp.prog.data(), hp.prog.size() * 4, (const void**)&b.prog, 0},
+        {hp.consts.data(), hp.consts.size() * 8, (const void**)&b.consts, 0},
+        {hp.slots.data(), hp.slots.size(), (const void**)&b.slots, 0},
+        {hp.meta.data(), hp.meta.size() * sizeof(RuleMeta), (const void**)&b.meta, 0},
+        {sampled, n_smp * 8, (const void**)&b.sampled, 0},
+    };
+    StaticLayout L;
+    for (Piece& p : up) p.at = L.take(p.bytes);
+    const size_t at_out = L.take((size_t)P * T * 8);
+    const size_t at_counter = L.take(sizeof(unsigned long long));
+    const size_t at_error = L.take(sizeof(int));
+    if (L.off > (size_t)SIDR_STATIC_SCRATCH_BYTES)
+        return fail(SIDR_ERR_TOO_LARGE, "sidr_evaluate_static: this call needs " +
+                                            std::to_string(L.off) + " bytes of device scratch, "
+                                            "more than SIDR_STATIC_SCRATCH_BYTES = " +
+                                            std::to_string((size_t)SIDR_STATIC_SCRATCH_BYTES));
+
+    std::lock_guard<std::mutex> guard(g_static_lock);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(SIDR_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev || device >= 256)
+        return fail(SIDR_ERR_INVALID, "device index out of range");
+    SIDR_CUDA(cudaSetDevice(device));
+    if (!g_static_ptr[device]) {  // once per device, with that device current
+        void* ptr = nullptr;
+        SIDR_CUDA(cudaGetSymbolAddress(&ptr, sidr_static_scratch));
+        g_static_ptr[device] = static_cast<unsigned char*>(ptr);
+    }
+    unsigned char* base = g_static_ptr[device];
+    cudaStream_t st = 0;  // legacy default stream
+    for (const Piece& p : up) {
+        *p.dst = base + p.at;
+        SIDR_CUDA(cudaMemcpyAsync(base + p.at, p.src, p.bytes, cudaMemcpyHostToDevice, st));
+    }
+    I.n = h.n;
+    I.m = h.m;
+    I.ld = h.n + 1;
+    I.nw = h.nw;
+    I.tmax = h.tmax;
+    I.ns = h.ns;
+    b.P = P;
+    b.T = T;
+    b.group_size = group_size;
+    b.n = h.n;
+    b.out = reinterpret_cast<double*>(base + at_out);
+    b.counter = reinterpret_cast<unsigned long long*>(base + at_counter);
+    b.stats = nullptr;
+    b.error = reinterpret_cast<int*>(base + at_error);
+    b.rows = hp.rows;
+    b.prog_cap = hp.prog_cap;
+    b.const_cap = hp.const_cap;
+    SIDR_CUDA(cudaMemsetAsync(base + at_error, 0, sizeof(int), st));  // launch() clears the counter
+
+    // Launch geometry from the device's own attributes (no context here).
+    sidr_ctx geo;
+    geo.device = device;
+    int v = 0;
+    SIDR_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
+    geo.sm_count = v;
+    SIDR_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    geo.smem_optin = (size_t)v;
+    geo.inst = I;
+    int grid, block;
+    size_t smem;
+    s = plan_launch(&geo, hp, (long long)P * T, false, grid, block, smem);
+    if (s) return s;
+    s = launch(&geo, b, false, grid, block, smem, st);
+    if (s) return s;
+    SIDR_CUDA(cudaMemcpyAsync(out, base + at_out, (size_t)P * T * 8, cudaMemcpyDeviceToHost, st));
+    SIDR_CUDA(cudaStreamSynchronize(st));
+    g_h2d = 0;
+    for (const Piece& p : up) g_h2d += (long long)p.bytes;
+    g_d2h = (long long)P * T * 8;
+    return SIDR_OK;
+}

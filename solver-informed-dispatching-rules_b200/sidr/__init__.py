@@ -64,6 +64,7 @@ EXPORTS = [
     "sidr_batch_create", "sidr_batch_run", "sidr_batch_read", "sidr_batch_fitness",
     "sidr_batch_device_out", "sidr_batch_destroy", "sidr_batch_set_counting", "sidr_batch_counts",
     "sidr_kernel_launches", "sidr_rules_check", "sidr_last_transfer_bytes", "sidr_fp64_peak",
+    "sidr_evaluate_static",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -103,6 +104,8 @@ def load() -> C.CDLL:
     L.sidr_rules_check.argtypes = [C.POINTER(_Rules), _lp, C.c_int32, C.POINTER(C.c_int32)]
     L.sidr_last_transfer_bytes.argtypes = [_lp, _lp]
     L.sidr_fp64_peak.argtypes = [C.c_int, C.c_int, _dp]
+    L.sidr_evaluate_static.argtypes = [C.POINTER(_Inst), _dp, C.POINTER(_Rules), _dp, C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_int32, _lp, C.c_int32, _dp]
     _lib = L
     return L
 
@@ -187,6 +190,25 @@ def fp64_peak(device: int = 0, reps: int = 5) -> float:
     v = C.c_double()
     _check(load().sidr_fp64_peak(device, reps, C.byref(v)))
     return v.value
+
+
+STATIC_SCRATCH_BYTES = 16 << 20  # SIDR_STATIC_SCRATCH_BYTES
+STATIC_MAX_N = 128               # SIDR_STATIC_MAX_N
+
+
+def evaluate_static(sd, zp, rules, grouped_sampled, G, T, group_size, mask_group, masks,
+                    device: int = 0) -> np.ndarray:
+    """sidr_evaluate_static: the grouped, multi-mask evaluation with no device
+    allocation (all device data in the library's fixed static array); every
+    argument is a host array.  Returns [P, T] scores."""
+    k = _Keep()
+    inst = k.inst(sd)
+    r = k.rules(rules)
+    out = np.zeros((rules.P, T))
+    _check(load().sidr_evaluate_static(C.byref(inst), k.f64(zp), C.byref(r),
+                                       k.f64(grouped_sampled), G, T, group_size, mask_group,
+                                       k.i64(masks), device, _d(out)))
+    return out
 
 
 class Batch:

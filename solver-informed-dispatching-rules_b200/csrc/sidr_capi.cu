@@ -474,10 +474,10 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
         {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
-        {h.sR.data(), h.sR.size() * 8, (const void**)&I.sR},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
-        {h.sFz.data(), h.sFz.size() * 8, (const void**)&I.sFz},
-        {h.sGz.data(), h.sGz.size() * 8, (const void**)&I.sGz},
+        {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},
+        {h.cnt_pos.data(), h.cnt_pos.size() * 4, (const void**)&I.cnt_pos},
+        {h.cnt_gm1.data(), h.cnt_gm1.size() * 4, (const void**)&I.cnt_gm1},
         {zp, 80, (const void**)&I.zp},
     };
     for (const Item& it : items) {
@@ -777,10 +777,10 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
         {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD, 0},
         {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T, 0},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord, 0},
-        {h.sR.data(), h.sR.size() * 8, (const void**)&I.sR, 0},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF, 0},
-        {h.sFz.data(), h.sFz.size() * 8, (const void**)&I.sFz, 0},
-        {h.sGz.data(), h.sGz.size() * 8, (const void**)&I.sGz, 0},
+        {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG, 0},
+        {h.cnt_pos.data(), h.cnt_pos.size() * 4, (const void**)&I.cnt_pos, 0},
+        {h.cnt_gm1.data(), h.cnt_gm1.size() * 4, (const void**)&I.cnt_gm1, 0},
         {zp, 80, (const void**)&I.zp, 0},
         {hp.prog.data(), hp.prog.size() * 4, (const void**)&b.prog, 0},
         {hp.consts.data(), hp.consts.size() * 8, (const void**)&b.consts, 0},

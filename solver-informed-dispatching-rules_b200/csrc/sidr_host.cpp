@@ -216,14 +216,15 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
     for (int c = 0; c < n; c++)
         for (int j = 0; j < n; j++) h.P1T[(size_t)j * n + c] = h.P1[(size_t)c * n + j];
     // Per-origin neighbour lists by (R desc, index asc), rows padded to a
-    // multiple of 4 entries with a ratio of -inf that ends every scan.
+    // multiple of 4 entries; bit 14 of an index marks a coincident location.
+    // cnt_pos / cnt_gm1 = how many leading entries have a ratio > 0 / > -1.
     h.ns = (n + 3) / 4 * 4;
     const size_t srows = (size_t)ld * h.ns;
     h.ord.assign(srows, 0);
-    h.sR.assign(srows, -INFINITY);
     h.sF.assign(srows, -INFINITY);
-    h.sFz.assign(srows, -INFINITY);
-    h.sGz.assign(srows, -INFINITY);
+    h.sG.assign(srows, -INFINITY);
+    h.cnt_pos.assign(ld, 0);
+    h.cnt_gm1.assign(ld, 0);
     std::vector<int> idx(n);
     for (int o = 0; o < ld; o++) {
         const double* Ro = h.R.data() + (size_t)o * n;
@@ -233,11 +234,11 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
             const int j = idx[k];
             const size_t a = (size_t)o * n + j, s = (size_t)o * h.ns + k;
             const bool coincident = (h.zlt[(size_t)o * h.nw + (j >> 5)] >> (j & 31)) & 1u;
-            h.ord[s] = (int16_t)j;
-            h.sR[s] = h.R[a];
+            h.ord[s] = (int16_t)(j | (coincident ? kOrdCoincident : 0));
             h.sF[s] = h.F[a];
-            h.sFz[s] = coincident ? -INFINITY : h.F[a];
-            h.sGz[s] = coincident ? -INFINITY : h.G[a];
+            h.sG[s] = h.G[a];
+            if (Ro[j] > 0.0) h.cnt_pos[o] = k + 1;
+            if (Ro[j] > -1.0) h.cnt_gm1[o] = k + 1;
         }
     }
     return "";

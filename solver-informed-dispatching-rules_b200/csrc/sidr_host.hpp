@@ -18,7 +18,8 @@ struct HostInstance {
     std::vector<double> FR, GD, P1T;                                     // neighbour-major
     int ns = 0;                                                          // sorted row stride
     std::vector<int16_t> ord;                                            // sorted lists
-    std::vector<double> sR, sF, sFz, sGz;
+    std::vector<double> sF, sG;
+    std::vector<int32_t> cnt_pos, cnt_gm1;
 };
 
 // Validates the SimData arrays (finite, n in range) and builds the tables

@@ -14,6 +14,7 @@ constexpr int kMaxStack = 32;  // engine/vocab.hpp:19
 constexpr int kMaxWords = kMaxN / 32;
 constexpr double kSigma = 0.2;                // SIM_SIGMA, engine/sim_terms.hpp:15
 constexpr double kSqrt2 = 1.4142135623730951; // SQRT2_C, engine/sim_terms.hpp:16
+constexpr int kOrdCoincident = 1 << 14;       // flag bit of the sorted neighbour lists
 
 // ----------------------------------------------------------------- instance
 //
@@ -45,11 +46,13 @@ constexpr double kSqrt2 = 1.4142135623730951; // SQRT2_C, engine/sim_terms.hpp:1
 //     lanes visit the same neighbour j from different origins, so one warp's
 //     16-byte loads stay in one row;
 //   * per-origin neighbour lists ord[o*ns + k] sorted by (R desc, index asc),
-//     rows padded to ns = a multiple of 4 with ratio -inf, with sR/sF (R and F
-//     in that order) and sFz/sGz (F and G, -inf on coincident pairs): a greedy
+//     rows padded to ns = a multiple of 4, with sF/sG (F and G in that order),
+//     bit 14 of ord marking coincident locations, and cnt_pos[o] / cnt_gm1[o]
+//     = the number of leading entries whose ratio exceeds 0 / -1: a greedy
 //     "best feasible neighbour by ratio" search -- strict > over ascending
-//     index, as in REACH-k and REACH2's second hop -- returns the first
-//     feasible entry of the sorted list, so it stops early.
+//     index from an initial best of 0 or -1, as in REACH2's second hop and
+//     REACH-k -- returns the first feasible entry among those, so it stops
+//     early.
 struct DevInst {
     int n, m, ld, nw;
     double tmax;
@@ -59,7 +62,8 @@ struct DevInst {
     const double *FR, *GD, *P1T;  // FR/GD: interleaved pairs
     int ns;                        // sorted-list row stride
     const int16_t* ord;
-    const double *sR, *sF, *sFz, *sGz;
+    const double *sF, *sG;
+    const int32_t *cnt_pos, *cnt_gm1;
     const double* zp;  // [10]
 };
 

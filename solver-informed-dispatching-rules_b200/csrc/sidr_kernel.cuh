@@ -122,51 +122,48 @@ __device__ __forceinline__ uint32_t bit_in_word(int node, int w) {
     return (node >= 0 && (node >> 5) == w) ? (1u << (node & 31)) : 0u;
 }
 
-// The sorted neighbour lists are read four entries at a time: 32-byte ratio
-// and threshold chunks, one 8-byte chunk of four customer indices.
+// The sorted neighbour lists are read four entries at a time: a 32-byte
+// chunk of thresholds and an 8-byte chunk of four indices.
 struct Chunk4 {
-    double r[4], t[4];
+    double t[4];
     int q[4];
 };
 
-__device__ __forceinline__ Chunk4 load_chunk(const double* sR, const double* sT,
-                                             const int16_t* ord, int k) {
+__device__ __forceinline__ Chunk4 load_chunk(const double* sT, const int16_t* ord, int k) {
     Chunk4 c;
-    const double2 r01 = *reinterpret_cast<const double2*>(sR + k);
-    const double2 r23 = *reinterpret_cast<const double2*>(sR + k + 2);
     const double2 t01 = *reinterpret_cast<const double2*>(sT + k);
     const double2 t23 = *reinterpret_cast<const double2*>(sT + k + 2);
     const uint2 qq = *reinterpret_cast<const uint2*>(ord + k);
-    c.r[0] = r01.x; c.r[1] = r01.y; c.r[2] = r23.x; c.r[3] = r23.y;
     c.t[0] = t01.x; c.t[1] = t01.y; c.t[2] = t23.x; c.t[3] = t23.y;
-    c.q[0] = (int)(int16_t)(qq.x & 0xffffu);
-    c.q[1] = (int)(int16_t)(qq.x >> 16);
-    c.q[2] = (int)(int16_t)(qq.y & 0xffffu);
-    c.q[3] = (int)(int16_t)(qq.y >> 16);
+    c.q[0] = (int)(qq.x & 0xffffu);
+    c.q[1] = (int)(qq.x >> 16);
+    c.q[2] = (int)(qq.y & 0xffffu);
+    c.q[3] = (int)(qq.y >> 16);
     return c;
 }
 
 // REACH2's second loop (engine/sim_terms.hpp:112-126, robust :175-189): the
 // best unvisited customer outside {x0, x1} by score/time from origin node o at
-// time tm, skipping coincident locations, init 0.0.  `table` is sFz (standard)
-// or sGz (robust).  The argmax with strict > over ascending index is the first
-// feasible entry of o's sorted neighbour list whose ratio exceeds 0.0.
-// Returns the chosen customer's score, or 0.0.
+// time tm, skipping coincident locations, init 0.0.  `table` is sF (standard)
+// or sG (robust).  The argmax with strict > over ascending index is the first
+// feasible entry among the cnt_pos[o] leading entries of o's sorted list (those
+// whose ratio exceeds 0.0).  Returns the chosen customer's score, or 0.0.
 template <bool COUNT>
 __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const double* table,
                                    int o, double tm, int x0, int x1, unsigned long long& hops) {
     const size_t row = (size_t)o * I.ns;
     const int16_t* ord = I.ord + row;
-    const double* sR = I.sR + row;
     const double* sT = table + row;
-    for (int k = 0; k < I.ns; k += 4) {
-        const Chunk4 c = load_chunk(sR, sT, ord, k);
+    const int cnt = I.cnt_pos[o];
+    for (int k = 0; k < cnt; k += 4) {
+        const Chunk4 c = load_chunk(sT, ord, k);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            if (!(c.r[e] > 0.0)) return 0.0;
+            if (k + e >= cnt) return 0.0;
             if (COUNT) hops++;
-            const int q = c.q[e];
-            if (q != x0 && q != x1 && is_unvisited(S, q) && tm <= c.t[e]) return I.scores[q];
+            const int q = c.q[e];  // coincident entries keep bit 14 and never match
+            if (q < kOrdCoincident && q != x0 && q != x1 && is_unvisited(S, q) && tm <= c.t[e])
+                return I.scores[q];
         }
     }
     return 0.0;
@@ -174,22 +171,22 @@ __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const do
 
 // One REACH-k greedy step (engine/sim_terms.hpp:415-431): the best unvisited
 // customer outside the walk by score/max(t,1e-10) under the standard test, no
-// coincident skip, init -1.0 -- the first feasible entry of o's sorted list
-// whose ratio exceeds -1.0.  p0..p4: the walk so far (-1 = unused).
+// coincident skip, init -1.0 -- the first feasible entry among the cnt_gm1[o]
+// leading entries of o's sorted list.  p0..p4: the walk so far (-1 = unused).
 template <bool COUNT>
 __device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm, int p0, int p1,
                           int p2, int p3, int p4, unsigned long long& hops) {
     const size_t row = (size_t)o * I.ns;
     const int16_t* ord = I.ord + row;
-    const double* sR = I.sR + row;
     const double* sF = I.sF + row;
-    for (int k = 0; k < I.ns; k += 4) {
-        const Chunk4 c = load_chunk(sR, sF, ord, k);
+    const int cnt = I.cnt_gm1[o];
+    for (int k = 0; k < cnt; k += 4) {
+        const Chunk4 c = load_chunk(sF, ord, k);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            if (!(c.r[e] > -1.0)) return -1;
+            if (k + e >= cnt) return -1;
             if (COUNT) hops++;
-            const int q = c.q[e];
+            const int q = c.q[e] & (kOrdCoincident - 1);
             if (q != p0 && q != p1 && q != p2 && q != p3 && q != p4 && is_unvisited(S, q) &&
                 tm <= c.t[e])
                 return q;
@@ -591,13 +588,13 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         const double arrive = fin + I.dist[(size_t)(i + 1) * ld + r2j + 1];
         const double st = arrive > I.open_t[r2j] ? arrive : I.open_t[r2j];
         const double fj = st + I.durations[r2j];
-        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.sFz, r2j + 1, fj, i, r2j, wc.hop);
+        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.sF, r2j + 1, fj, i, r2j, wc.hop);
     }
     if ((need & kNeedReach2Rob) && r2rj >= 0) {
         const double arrive = frob + I.dist[(size_t)(i + 1) * ld + r2rj + 1];
         const double st = arrive > I.open_t[r2rj] ? arrive : I.open_t[r2rj];
         const double fj = st + I.durations[r2rj] * (1.0 + kSigma);
-        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.sGz, r2rj + 1, fj, i, r2rj, wc.hop);
+        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.sG, r2rj + 1, fj, i, r2rj, wc.hop);
     }
 
     // REACH-1/3/5 share one greedy path (each is the running total after

@@ -1,0 +1,91 @@
+/*
+ * sidr_gp.h -- C-ABI of the host GP loop that drives the evaluator.
+ *
+ * The reference's GP (augustompm/solver-informed-dispatching-rules,
+ * engine/gp.hpp:13-194) and its seed-batched driver (engine/gp_engine.cu:
+ * 131-203), rebuilt on flat prefix-order rule arrays: ramped half-and-half
+ * initialisation, Koza 90/10 point selection, subtree crossover and mutation
+ * under the depth limit, size-7 tournaments, elitism and gp_step's rates, all
+ * driven by a Python-compatible MT19937 so that the same seed gives the same
+ * populations as the reference.  Fitness comes from the B200 evaluator.
+ */
+#ifndef SIDR_GP_H
+#define SIDR_GP_H
+
+#include <stdint.h>
+
+#include "sidr.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* EvolutionConfig and TreeConfig (engine/gp.hpp:13-34). */
+typedef struct sidr_gp_config {
+    int32_t population;        /* 1024 */
+    int32_t generations;       /* 51   */
+    int32_t max_depth;         /* 8    */
+    int32_t min_depth;         /* 2    */
+    int32_t tournament;        /* 7    */
+    int32_t elitism;           /* 10   */
+    double crossover_rate;     /* 0.80 */
+    double mutation_rate;      /* 0.15 */
+    double reproduction_rate;  /* 0.05 */
+    int32_t train_samples;     /* 1    */
+    int32_t test_samples;      /* 500  */
+    int32_t with_rmod;         /* 0: FUNCTIONS, 1: FUNCS_RMOD (engine/tree.hpp:33-34) */
+} sidr_gp_config;
+
+/* The reference defaults (engine/gp.hpp:20-34). */
+void sidr_gp_default_config(sidr_gp_config* cfg);
+
+/* One GP population of one seed (engine/gp_engine.cu:69-84's state).
+ * terminals_csv: the terminal set, comma separated ("ERC" = random constant,
+ * label "%.3f"); the generator is Mt19937(seed). */
+typedef struct sidr_gp_session sidr_gp_session;
+sidr_status sidr_gp_create(const sidr_gp_config* cfg, const char* terminals_csv, uint64_t seed,
+                           sidr_gp_session** out);
+void sidr_gp_destroy(sidr_gp_session* s);
+
+/* The population as prefix text (engine/tree.hpp:62-69), '\n' separated;
+ * returns the bytes needed (call with cap 0 to size the buffer). */
+int64_t sidr_gp_population_text(const sidr_gp_session* s, char* buf, int64_t cap);
+
+/* The population compiled to the evaluator's PackedTrees layout
+ * (engine/factory.cuh:26-40): sizes first (pass NULL arrays), then fill. */
+sidr_status sidr_gp_population_packed(const sidr_gp_session* s, int32_t* ops, int32_t* args,
+                                      int32_t* offsets, int32_t* lengths, int64_t* n_nodes);
+
+/* gp_step (engine/gp.hpp:170-194) with the given per-rule fitness. */
+sidr_status sidr_gp_step(sidr_gp_session* s, const double* fitness);
+
+/* The seed-batched GP run of engine/gp_engine.cu:131-203 (exhaust_batched):
+ * n_seeds populations (seeds first_seed .. first_seed+n_seeds-1) evolve
+ * together, each generation evaluated in one grouped call on the evaluator with
+ * train_samples scenarios of base seed seed*10000+gen per population; after the
+ * last generation the best rule of each population (on one more train block) is
+ * scored on test_samples scenarios from test_seed.
+ *   best_test[n_seeds]      mean held-out score of each population's best rule
+ *   best_train[gens*n_seeds] best train fitness per generation and population
+ *   best_rules              the best rules' prefix text, '\n' separated
+ *   eval_seconds / host_seconds  time in evaluator calls / in the host GP
+ */
+typedef struct sidr_gp_result {
+    double eval_seconds;
+    double host_seconds;
+    int64_t evaluations;
+} sidr_gp_result;
+sidr_status sidr_gp_run_batched(sidr_ctx* ctx, const sidr_instance_desc* inst,
+                                const sidr_gp_config* cfg, const char* terminals_csv,
+                                const int64_t* term_mask, int32_t n_seeds, int64_t first_seed,
+                                int64_t test_seed, double* best_test, double* best_train,
+                                char* best_rules, int64_t rules_cap, sidr_gp_result* result);
+
+/* gen_durations (engine/sim_host.hpp:43-58) on the host: [S][n]. */
+sidr_status sidr_gen_durations(int32_t n, const double* durations, double sigma, int32_t S,
+                               int64_t base_seed, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -231,3 +231,30 @@ class Reference:
         out = np.zeros(count)
         self.lib.ref_mt_draws(seed, kind, arg, count, _d(out))
         return out
+
+
+def _ref_gp_replay(self, terminals, with_rmod, seed, pop, fits):
+    """The reference's RHH + gp_step over len(fits) generations; returns the
+    populations (prefix text) of generations 0..len(fits)."""
+    L = self.lib
+    L.ref_gp_replay.argtypes = [C.c_char_p, C.c_int, C.c_ulonglong, C.c_int, C.c_int, _dp,
+                                C.c_char_p, C.c_long]
+    L.ref_gp_replay.restype = C.c_long
+    fits = np.ascontiguousarray(fits, dtype=np.float64)
+    cap = 1 << 27
+    buf = C.create_string_buffer(cap)
+    n = L.ref_gp_replay(",".join(terminals).encode(), int(with_rmod), seed, pop, len(fits),
+                        fits.ctypes.data_as(_dp), buf, cap)
+    if n < 0:
+        raise RuntimeError("replay buffer too small")
+    out, cur = [], []
+    for line in buf.value.decode().splitlines():
+        if line == "#":
+            out.append(cur)
+            cur = []
+        else:
+            cur.append(line)
+    return out
+
+
+Reference.gp_replay = _ref_gp_replay

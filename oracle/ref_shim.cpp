@@ -200,3 +200,37 @@ void ref_mt_draws(unsigned long long seed, int kind, long long arg, int count, d
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// The reference's GP over `gens` steps with given fitness arrays
+// (fits[g*pop + p]): ramped_half_and_half with Mt19937(seed), then gp_step
+// (engine/gp.hpp:67-194) after each generation's fitness.  Writes the gens+1
+// populations as prefix text, one rule per line, generations separated by a
+// line "#".  Returns bytes used or -1.
+long ref_gp_replay(const char* terminals_csv, int with_rmod, unsigned long long seed, int pop,
+                   int gens, const double* fits, char* buf, long cap) {
+    TreeConfig tc;
+    tc.terminals = split_csv(terminals_csv);
+    tc.functions = with_rmod ? FUNCS_RMOD : FUNCTIONS;
+    EvolutionConfig cfg;
+    cfg.population_size = pop;
+    Mt19937 rng((uint64_t)seed);
+    std::vector<NodeP> p = ramped_half_and_half(tc, rng, pop);
+    std::string all;
+    for (int g = 0; g <= gens; g++) {
+        for (auto& t : p) {
+            all += to_prefix(t);
+            all += '\n';
+        }
+        all += "#\n";
+        if (g == gens) break;
+        std::vector<double> f(fits + (size_t)g * pop, fits + (size_t)(g + 1) * pop);
+        p = gp_step(p, f, rng, tc, cfg);
+    }
+    if ((long)all.size() + 1 > cap) return -1;
+    std::memcpy(buf, all.c_str(), all.size() + 1);
+    return (long)all.size();
+}
+
+}  // extern "C"

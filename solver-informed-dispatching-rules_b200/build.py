@@ -29,8 +29,9 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall"]
 
 CU_SOURCES = ["sidr_capi.cu"]
-CPP_SOURCES = ["sidr_host.cpp"]
+CPP_SOURCES = ["sidr_host.cpp", "sidr_gp.cpp"]
 HEADERS = ["sidr_internal.hpp", "sidr_kernel.cuh", "sidr_host.hpp"]
+PUBLIC_HEADERS = ["sidr.h", "sidr_gp.h"]
 
 
 def _newer(target: str, deps) -> bool:
@@ -52,7 +53,7 @@ def _run(cmd, log=None):
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    deps_common = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "sidr.h")]
+    deps_common = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, h) for h in PUBLIC_HEADERS]
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)

@@ -1,0 +1,142 @@
+"""Python front end of the host GP loop (include/sidr_gp.h): the reference's
+GP (engine/gp.hpp) on flat prefix-order rules in C++, evaluated by the B200
+evaluator."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Sequence
+
+import numpy as np
+
+from . import _Keep, _check, load
+from .rules import PackedRules
+
+
+class _Cfg(C.Structure):
+    _fields_ = [("population", C.c_int32), ("generations", C.c_int32), ("max_depth", C.c_int32),
+                ("min_depth", C.c_int32), ("tournament", C.c_int32), ("elitism", C.c_int32),
+                ("crossover_rate", C.c_double), ("mutation_rate", C.c_double),
+                ("reproduction_rate", C.c_double), ("train_samples", C.c_int32),
+                ("test_samples", C.c_int32), ("with_rmod", C.c_int32)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("eval_seconds", C.c_double), ("host_seconds", C.c_double),
+                ("evaluations", C.c_int64)]
+
+
+def _lib():
+    L = load()
+    if not getattr(L, "_gp_ready", False):
+        L.sidr_gp_default_config.argtypes = [C.POINTER(_Cfg)]
+        L.sidr_gp_create.argtypes = [C.POINTER(_Cfg), C.c_char_p, C.c_uint64, C.POINTER(C.c_void_p)]
+        L.sidr_gp_destroy.argtypes = [C.c_void_p]
+        L.sidr_gp_population_text.argtypes = [C.c_void_p, C.c_char_p, C.c_int64]
+        L.sidr_gp_population_text.restype = C.c_int64
+        ip = C.POINTER(C.c_int32)
+        L.sidr_gp_population_packed.argtypes = [C.c_void_p, ip, ip, ip, ip, C.POINTER(C.c_int64)]
+        L.sidr_gp_step.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        dp = C.POINTER(C.c_double)
+        L.sidr_gen_durations.argtypes = [C.c_int32, dp, C.c_double, C.c_int32, C.c_int64, dp]
+        from . import _Inst
+        L.sidr_gp_run_batched.argtypes = [C.c_void_p, C.POINTER(_Inst), C.POINTER(_Cfg), C.c_char_p,
+                                          C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
+                                          dp, dp, C.c_char_p, C.c_int64, C.POINTER(_Result)]
+        L._gp_ready = True
+    return L
+
+
+def config(**kw) -> _Cfg:
+    """EvolutionConfig defaults (engine/gp.hpp:20-34) with overrides."""
+    c = _Cfg()
+    _lib().sidr_gp_default_config(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class Session:
+    """One seed's population (ramped half-and-half with Mt19937(seed))."""
+
+    def __init__(self, terminals: Sequence[str], seed: int, **cfg):
+        self.cfg = config(**cfg)
+        h = C.c_void_p()
+        _check(_lib().sidr_gp_create(C.byref(self.cfg), ",".join(terminals).encode(), seed,
+                                     C.byref(h)))
+        self.h = h.value
+
+    def text(self) -> List[str]:
+        L = _lib()
+        n = L.sidr_gp_population_text(self.h, None, 0)
+        buf = C.create_string_buffer(int(n))
+        L.sidr_gp_population_text(self.h, buf, n)
+        return buf.value.decode().splitlines()
+
+    def packed(self) -> PackedRules:
+        L = _lib()
+        nn = C.c_int64()
+        _check(L.sidr_gp_population_packed(self.h, None, None, None, None, C.byref(nn)))
+        P = self.cfg.population
+        ops = np.zeros(nn.value, np.int32)
+        args = np.zeros(2 * nn.value, np.int32)
+        off = np.zeros(P, np.int32)
+        ln = np.zeros(P, np.int32)
+        ip = C.POINTER(C.c_int32)
+        _check(L.sidr_gp_population_packed(self.h, ops.ctypes.data_as(ip), args.ctypes.data_as(ip),
+                                           off.ctypes.data_as(ip), ln.ctypes.data_as(ip),
+                                           C.byref(nn)))
+        return PackedRules(ops, args, off, ln)
+
+    def step(self, fitness) -> None:
+        f = np.ascontiguousarray(fitness, dtype=np.float64)
+        _check(_lib().sidr_gp_step(self.h, f.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().sidr_gp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_durations(durations, sigma: float, S: int, base_seed: int) -> np.ndarray:
+    d = np.ascontiguousarray(durations, dtype=np.float64)
+    out = np.zeros((S, len(d)))
+    dp = C.POINTER(C.c_double)
+    _check(_lib().sidr_gen_durations(len(d), d.ctypes.data_as(dp), sigma, S, base_seed,
+                                     out.ctypes.data_as(dp)))
+    return out
+
+
+@dataclass
+class RunResult:
+    best_test: np.ndarray
+    best_train: np.ndarray  # [generations, n_seeds]
+    best_rules: List[str]
+    eval_seconds: float
+    host_seconds: float
+    evaluations: int
+
+
+def run_batched(ctx, terminals: Sequence[str], mask, n_seeds: int, first_seed: int = 0,
+                test_seed: int = 1000000, **cfg) -> RunResult:
+    """exhaust_batched (engine/gp_engine.cu:131-203) on the B200 evaluator."""
+    c = config(**cfg)
+    k = _Keep()
+    inst = k.inst(ctx.sd)
+    bt = np.zeros(n_seeds)
+    btr = np.zeros((c.generations, n_seeds))
+    buf = C.create_string_buffer(1 << 22)
+    res = _Result()
+    dp = C.POINTER(C.c_double)
+    _check(_lib().sidr_gp_run_batched(ctx.h, C.byref(inst), C.byref(c),
+                                      ",".join(terminals).encode(), k.i64(mask), n_seeds,
+                                      first_seed, test_seed, bt.ctypes.data_as(dp),
+                                      btr.ctypes.data_as(dp), buf, 1 << 22, C.byref(res)))
+    return RunResult(bt, btr, buf.value.decode().splitlines(), res.eval_seconds,
+                     res.host_seconds, res.evaluations)

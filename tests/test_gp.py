@@ -1,0 +1,63 @@
+"""The host GP loop (include/sidr_gp.h) against the reference: the golden
+populations and fitnesses of verify/golden/gp.txt, and the reference's own
+gp_step replayed over many generations."""
+import numpy as np
+import pytest
+
+from sidr import gp
+from sidr import rules as R
+from sidr import workload
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.uint64)
+
+
+def test_gp_reproduces_golden_generations():
+    """c101 golden GP (seed 0): populations of generations 0-2 step by step,
+    driven by the golden fitness of each generation."""
+    from test_oracle import load_gp_blocks
+    blocks = {b: (rules, exp) for b, sd, rules, mask, sampled, exp in load_gp_blocks()}
+    for case, terms, rmod in (("ns11", R.NS_TERMINALS, 0), ("ext29rmod", R.NS_TERMINALS + R.EXTRA, 1)):
+        s = gp.Session(terms, 0, with_rmod=rmod)
+        for g in range(3):
+            want, fits = blocks[f"{case}_g{g}"]
+            got = s.packed()
+            assert np.array_equal(got.ops, want.ops) and np.array_equal(got.args, want.args), (case, g)
+            assert np.array_equal(got.offsets, want.offsets), (case, g)
+            s.step(fits)
+        s.close()
+
+
+@pytest.mark.parametrize("terms,rmod,seed", [(workload.MENU29, 0, 3),
+                                             (R.NS_TERMINALS + ["ERC"], 1, 11)])
+def test_gp_matches_reference_over_generations(reference, terms, rmod, seed):
+    """Random fitness with many ties (stable sort, tournament ties): six
+    generations of 256 rules equal the reference's gp_step text."""
+    rng = np.random.default_rng(seed)
+    fits = rng.integers(0, 40, size=(6, 256)).astype(np.float64)
+    want = reference.gp_replay(terms, rmod, seed, 256, fits)
+    s = gp.Session(terms, seed, population=256, with_rmod=rmod)
+    for g in range(7):
+        assert s.text() == want[g], g
+        if g < 6:
+            s.step(fits[g])
+    s.close()
+
+
+def test_gen_durations_capi_matches_golden():
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "durations.npz"))
+    for b in z["blocks"]:
+        exp = z[f"{b}/expected"]
+        got = gp.gen_durations(z[f"{b}/durations"], 0.2, exp.shape[0], int(z[f"{b}/base_seed"][0]))
+        assert np.array_equal(bits(got), bits(exp)), b
+
+
+def test_gp_rejects_bad_config():
+    import sidr
+    with pytest.raises(sidr.SidrError):
+        gp.Session(["SCORE", "NOPE"], 0)
+    with pytest.raises(sidr.SidrError):
+        gp.Session(["SCORE"], 0, max_depth=9)

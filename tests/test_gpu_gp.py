@@ -1,0 +1,57 @@
+"""The seed-batched GP driver (sidr_gp_run_batched, the reference's
+exhaust_batched) on the B200 evaluator, against a CPU replica: the same GP
+sessions stepped with the oracle's fitness."""
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+
+import sidr
+from sidr import gp
+from sidr import rules as R
+from sidr import workload
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.uint64)
+
+
+def test_run_batched_matches_cpu_replica(oracle):
+    w = workload.plain_eval(P=2, S=1)
+    zp = sidr.zstats(w.sd)
+    terms = workload.MENU29
+    n_seeds, first_seed, T, gens, pop, test_n = 3, 5, 2, 3, 48, 16
+    cfg = dict(population=pop, generations=gens, train_samples=T, test_samples=test_n)
+    ctx = sidr.Context(w.sd, zp)
+    res = gp.run_batched(ctx, terms, w.mask, n_seeds, first_seed=first_seed, test_seed=777, **cfg)
+    ctx.close()
+
+    sessions = [gp.Session(terms, first_seed + s, **cfg) for s in range(n_seeds)]
+
+    def fit_all(gen):
+        out = []
+        for s, sess in enumerate(sessions):
+            smp = gp.gen_durations(w.sd.durations, 0.2, T, (first_seed + s) * 10000 + gen)
+            r = oracle.eval_pairs(w.sd, zp, sess.packed(), smp, T, w.mask)
+            out.append(np.array([sum(float(v) for v in row) / T for row in r]))
+        return out
+
+    for g in range(gens):
+        fits = fit_all(g)
+        for s in range(n_seeds):
+            assert res.best_train[g, s] == fits[s].max(), (g, s)
+        if g < gens - 1:
+            for s in range(n_seeds):
+                sessions[s].step(fits[s])
+    fits = fit_all(gens)
+    test = gp.gen_durations(w.sd.durations, 0.2, test_n, 777)
+    for s in range(n_seeds):
+        bi = int(np.argmax(fits[s]))  # first maximum, as the reference's strict >
+        rule = sessions[s].packed().subset([bi])
+        assert res.best_rules[s] == sessions[s].text()[bi]
+        held = oracle.eval_pairs(w.sd, zp, rule, test, test_n, w.mask)[0]
+        assert bits(res.best_test[s]) == bits(sum(float(v) for v in held) / test_n)
+    assert res.evaluations == gens * n_seeds * pop * T + n_seeds * pop * T + n_seeds * test_n

@@ -58,6 +58,10 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--gp", action="store_true",
+                    help="also run the GP loop of the workload (50 generations of 1024 rules x "
+                         "500 scenarios + held-out evaluation) and report its wall time")
+    ap.add_argument("--gp-generations", type=int, default=50)
     return ap.parse_args()
 
 
@@ -343,12 +347,35 @@ def run_ours(args, rank, world, local):
             "counts": counts, "repeat_runs_identical": same}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, zp, args.cpu_seconds, gpu_out=ref_out)
+    if args.gp and rank == 0:
+        line["gp"] = gp_leg(ctx, w, args)
     batch.close()
     ctx.close()
     if dist:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def gp_leg(ctx, w, args):
+    """The GP run behind the workload: the reference's GP (engine/gp.hpp) with
+    the benchmark's settings -- population 1024, 500 training scenarios per
+    generation (base seed seed*10000+gen), 50 generations, the best rule scored
+    on 500 held-out scenarios (base seed 1000000) -- evaluated by the B200
+    evaluator; host GP in C++."""
+    from sidr import gp
+    from sidr.workload import MENU29
+    t0 = time.perf_counter()
+    res = gp.run_batched(ctx, MENU29, w.mask, 1, first_seed=0, test_seed=1000000,
+                         population=args.P, generations=args.gp_generations,
+                         train_samples=args.S, test_samples=500)
+    wall = time.perf_counter() - t0
+    return {"population": args.P, "train_scenarios": args.S, "generations": args.gp_generations,
+            "wall_seconds": wall, "eval_seconds": res.eval_seconds,
+            "host_seconds": res.host_seconds, "evaluations": res.evaluations,
+            "held_out_mean_score": float(res.best_test[0]),
+            "best_train_first": float(res.best_train[0, 0]),
+            "best_train_last": float(res.best_train[-1, 0]), "best_rule": res.best_rules[0]}
 
 
 def main():

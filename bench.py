@@ -62,6 +62,11 @@ def parse_args():
                     help="also run the GP loop of the workload (50 generations of 1024 rules x "
                          "500 scenarios + held-out evaluation) and report its wall time")
     ap.add_argument("--gp-generations", type=int, default=50)
+    ap.add_argument("--multi", action="store_true",
+                    help="also time the uneven multi-instance batch (40 instances of 25-288 "
+                         "customers) in one autotuned, graph-captured launch")
+    ap.add_argument("--multi-rules", type=int, default=100)
+    ap.add_argument("--multi-S", type=int, default=100)
     return ap.parse_args()
 
 
@@ -349,12 +354,46 @@ def run_ours(args, rank, world, local):
         line["cpu_baseline"] = cpu_baseline(w, zp, args.cpu_seconds, gpu_out=ref_out)
     if args.gp and rank == 0:
         line["gp"] = gp_leg(ctx, w, args)
+    if args.multi and rank == 0:
+        line["multi"] = multi_leg(args, stream)
     batch.close()
     ctx.close()
     if dist:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def multi_leg(args, stream):
+    """The uneven batch (40 instances: 25/50/100/288 customers, three layouts,
+    m 2-4, H 230/1000, rules of log-uniform length 3-255) in one persistent
+    launch: autotuned block shape, CUDA-graph replay, device-timed."""
+    import torch
+    import sidr
+    from sidr import workload
+    t0 = time.perf_counter()
+    mw = workload.batched_uneven(K=40, rules_per_instance=args.multi_rules, S=args.multi_S)
+    zps = [sidr.zstats(sd) for sd in mw.sds]
+    m = sidr.Multi(mw.sds, zps, mw.rules, mw.sampled, mw.S, mw.masks)
+    prep = time.perf_counter() - t0
+    chosen, ms = m.autotune(reps=1)
+    m.capture()
+    m.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(3)]
+    for e0, e1 in ev:
+        e0.record(stream)
+        m.run(stream.cuda_stream)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    t = min(e0.elapsed_time(e1) for e0, e1 in ev) / 1e3
+    P = sum(r.P for r in mw.rules)
+    m.close()
+    return {"workload": f"40 instances x {args.multi_rules} rules x {args.multi_S} scenarios",
+            "evaluations": P * mw.S, "seconds": t, "evals_per_s": P * mw.S / t,
+            "shapes_ms": ms, "chosen_shape": list(sidr.Multi.SHAPES[chosen]),
+            "host_prep_seconds": prep}
 
 
 def gp_leg(ctx, w, args):

@@ -148,6 +148,34 @@ typedef struct sidr_counts {
 sidr_status sidr_batch_set_counting(sidr_batch* b, int enable);
 sidr_status sidr_batch_counts(sidr_batch* b, sidr_counts* out);
 
+/* Multi-instance batches (no reference counterpart; the reference evaluates
+ * one instance per FactoryContext).  K instances of uneven size, each with its
+ * own rules, scenarios and mask, evaluated together in ONE persistent launch:
+ * rule p belongs to instance rule_instance[p], reads the [T][n_k] scenario
+ * block at sampled + sampled_offsets[k] (in doubles; the flat host buffer
+ * holds n_sampled doubles) and mask row k of masks [K][61]; out[p*T + s].
+ * Work is handed out longest-estimated-rule first.  Several block shapes of
+ * the kernel are compiled in; sidr_multi_autotune times each on this batch
+ * (reps runs, best time), keeps the fastest and remembers the choice for
+ * batches of the same shape (instances' sizes, rule and scenario counts,
+ * program sizes, SM count) in this process; ms[] (may be NULL) receives
+ * each shape's time, *chosen its index.  sidr_multi_capture records the
+ * launch (counter reset + kernel) as a CUDA graph that sidr_multi_run then
+ * replays. */
+typedef struct sidr_multi sidr_multi;
+#define SIDR_MULTI_SHAPES 3
+sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                              const sidr_rules_desc* rules, const int32_t* rule_instance,
+                              const double* sampled, int64_t n_sampled,
+                              const int64_t* sampled_offsets, int32_t T, const int64_t* masks,
+                              int32_t device, sidr_multi** out);
+sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, float* ms);
+sidr_status sidr_multi_set_shape(sidr_multi* m, int32_t shape);
+sidr_status sidr_multi_capture(sidr_multi* m);
+sidr_status sidr_multi_run(sidr_multi* m, void* stream);
+sidr_status sidr_multi_read(sidr_multi* m, double* out);
+void sidr_multi_destroy(sidr_multi* m);
+
 /* Host-only validation of rules under their masks (no device needed): the
  * checks every evaluate call makes -- opcodes, terminal slots < 61, no stack
  * underflow, stack depth <= SIDR_MAX_STACK, one value left, length <=

@@ -130,14 +130,16 @@ sidr_status check_rules(const sidr_rules_desc* r) {
     return SIDR_OK;
 }
 
-// Compile every rule under its mask row.
+// Compile every rule under its mask row: row p/mask_group, or row_of[p] when
+// given (multi-instance batches, where it is also the rule's instance).
 sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask_group,
-                        HostPrograms& hp) {
+                        HostPrograms& hp, const int32_t* row_of = nullptr) {
     hp = HostPrograms();
     hp.meta.resize(r->P);
     CompiledRule cr;
     for (int p = 0; p < r->P; p++) {
-        const int64_t* M = masks + (size_t)(p / mask_group) * kTerms;
+        const int row = row_of ? row_of[p] : p / mask_group;
+        const int64_t* M = masks + (size_t)row * kTerms;
         std::string e = compile_rule(r->ops + r->offsets[p], r->args + 2 * (size_t)r->offsets[p],
                                      r->lengths[p], M, cr);
         if (!e.empty()) {
@@ -156,6 +158,7 @@ sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask
         m.res = (int16_t)cr.res;
         m.reach_k = (int8_t)cr.reach_k;
         m.scan_ops = (uint16_t)scan_ops_of(cr.need);
+        m.inst = (int16_t)(row_of ? row_of[p] : 0);
         m.need = cr.need;
         m.explore = cr.explore;
         hp.prog.insert(hp.prog.end(), cr.prog.begin(), cr.prog.end());
@@ -860,3 +863,337 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
     g_d2h = (long long)P * T * 8;
     return SIDR_OK;
 }
+
+// ----------------------------------------------------------------------------
+// Multi-instance batches (sidr_multi_*).
+
+#include <map>
+
+namespace {
+
+// The compiled block shapes of eval_multi_kernel: {warps per block, min blocks}.
+constexpr int kShapes[SIDR_MULTI_SHAPES][2] = {{4, 3}, {8, 2}, {2, 6}};
+const void* multi_kernel(int shape) {
+    switch (shape) {
+    case 0: return (const void*)eval_multi_kernel<4, 3>;
+    case 1: return (const void*)eval_multi_kernel<8, 2>;
+    default: return (const void*)eval_multi_kernel<2, 6>;
+    }
+}
+
+std::mutex g_tune_lock;
+std::map<std::string, int> g_tune_cache;  // batch shape -> chosen block shape
+
+}  // namespace
+
+struct sidr_multi {
+    int device = 0, K = 0, P = 0, T = 0, sm_count = 0;
+    size_t smem_optin = 0;
+    std::vector<void*> owned;
+    DevBatch b{};
+    int shape = 0;
+    int grid[SIDR_MULTI_SHAPES] = {}, block[SIDR_MULTI_SHAPES] = {};
+    size_t smem[SIDR_MULTI_SHAPES] = {};
+    std::string key;
+    cudaStream_t gstream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+};
+
+namespace {
+
+void multi_free(sidr_multi* m) {
+    if (!m) return;
+    cudaSetDevice(m->device);
+    cudaDeviceSynchronize();
+    if (m->gexec) cudaGraphExecDestroy(m->gexec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    if (m->gstream) cudaStreamDestroy(m->gstream);
+    for (void* p : m->owned) cudaFree(p);
+    delete m;
+}
+
+cudaError_t put_dev(sidr_multi* m, const void* src, size_t bytes, const void** dst) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 8);
+    if (e != cudaSuccess) return e;
+    m->owned.push_back(p);
+    *dst = p;
+    return bytes ? cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+}
+
+sidr_status multi_launch(sidr_multi* m, int shape, cudaStream_t st) {
+    SIDR_CUDA(cudaMemsetAsync(m->b.counter, 0, sizeof(unsigned long long), st));
+    void* args[] = {&m->b};
+    SIDR_CUDA(cudaLaunchKernel(multi_kernel(shape), dim3(m->grid[shape]), dim3(m->block[shape]),
+                               args, m->smem[shape], st));
+    g_launches.fetch_add(1);
+    return SIDR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                              const sidr_rules_desc* r, const int32_t* rule_instance,
+                              const double* sampled, int64_t n_sampled,
+                              const int64_t* sampled_offsets, int32_t T, const int64_t* masks,
+                              int32_t device, sidr_multi** out) {
+    if (!out) return fail(SIDR_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!insts || !zps || K < 1 || K > 32767 || !rule_instance || !sampled_offsets || !masks)
+        return fail(SIDR_ERR_INVALID, "null argument or K out of 1..32767");
+    sidr_status s = check_rules(r);
+    if (s) return s;
+    if (T < 0) return fail(SIDR_ERR_INVALID, "T < 0");
+    for (int p = 0; p < r->P; p++)
+        if (rule_instance[p] < 0 || rule_instance[p] >= K)
+            return fail(SIDR_ERR_INVALID, "rule " + std::to_string(p) + ": instance out of range");
+    std::vector<HostInstance> hs(K);
+    for (int k = 0; k < K; k++) {
+        const sidr_instance_desc& d = insts[k];
+        std::string e = build_instance(d.n, d.m, d.tmax, d.scores, d.durations, d.open_t,
+                                       d.close_t, d.dist, d.dist_to_depot, hs[k], true);
+        if (!e.empty())
+            return fail(e.find("finite") != std::string::npos ? SIDR_ERR_NONFINITE
+                        : (d.n > kMaxN ? SIDR_ERR_TOO_LARGE : SIDR_ERR_INVALID),
+                        "instance " + std::to_string(k) + ": " + e);
+        const int64_t need = sampled_offsets[k] + (int64_t)T * d.n;
+        if (sampled_offsets[k] < 0 || need > n_sampled)
+            return fail(SIDR_ERR_INVALID, "instance " + std::to_string(k) + ": scenario block outside the buffer");
+        s = check_finite(sampled + sampled_offsets[k], (size_t)T * d.n);
+        if (s) return s;
+    }
+    HostPrograms hp;
+    if (r->P > 0) {
+        s = compile_all(r, masks, 1, hp, rule_instance);
+        if (s) return s;
+    } else {
+        hp.prog.push_back(0);
+        hp.consts.push_back(0.0);
+        hp.slots.push_back(0);
+    }
+    // Longest-estimated-first order: n^2 x the neighbour work of the rule's
+    // families, plus the program.
+    std::vector<int32_t> order(r->P);
+    std::vector<double> est(r->P);
+    for (int p = 0; p < r->P; p++) {
+        const RuleMeta& mm = hp.meta[p];
+        const double nk = hs[mm.inst].n;
+        const double fam = 8.0 + scan_ops_of(mm.need) + ((mm.need & kNeedAtRisk) ? kOpsAtRisk : 0) +
+                           8.0 * mm.reach_k;
+        est[p] = nk * nk * fam + nk * mm.n_ins;
+        order[p] = p;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return est[a] > est[b]; });
+
+    SIDR_CUDA(cudaSetDevice(device));
+    sidr_multi* m = new sidr_multi();
+    m->device = device;
+    m->K = K;
+    m->P = r->P;
+    m->T = T;
+    auto bail = [&](cudaError_t err, const char* what) {
+        multi_free(m);
+        return fail(SIDR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+    };
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    m->sm_count = v;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    m->smem_optin = (size_t)v;
+    std::vector<DevInst> dinst(K);
+    for (int k = 0; k < K; k++) {
+        const HostInstance& h = hs[k];
+        DevInst& I = dinst[k];
+        I.n = h.n;
+        I.m = h.m;
+        I.ld = h.n + 1;
+        I.nw = h.nw;
+        I.tmax = h.tmax;
+        I.ns = h.ns;
+        struct Item { const void* src; size_t bytes; const void** dst; };
+        const Item items[] = {
+            {h.scores.data(), (size_t)h.n * 8, (const void**)&I.scores},
+            {h.durations.data(), (size_t)h.n * 8, (const void**)&I.durations},
+            {h.open_t.data(), (size_t)h.n * 8, (const void**)&I.open_t},
+            {h.close_t.data(), (size_t)h.n * 8, (const void**)&I.close_t},
+            {h.d2d.data(), (size_t)h.n * 8, (const void**)&I.d2d},
+            {h.dist.data(), h.dist.size() * 8, (const void**)&I.dist},
+            {h.F.data(), h.F.size() * 8, (const void**)&I.F},
+            {h.G.data(), h.G.size() * 8, (const void**)&I.G},
+            {h.R.data(), h.R.size() * 8, (const void**)&I.R},
+            {h.P1.data(), h.P1.size() * 8, (const void**)&I.P1},
+            {h.P0.data(), h.P0.size() * 8, (const void**)&I.P0},
+            {h.zlt.data(), h.zlt.size() * 4, (const void**)&I.zlt},
+            {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle},
+            {h.FR.data(), h.FR.size() * 8, (const void**)&I.FR},
+            {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
+            {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T},
+            {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
+            {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
+            {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},
+            {h.cnt_pos.data(), h.cnt_pos.size() * 4, (const void**)&I.cnt_pos},
+            {h.cnt_gm1.data(), h.cnt_gm1.size() * 4, (const void**)&I.cnt_gm1},
+            {zps + 10 * (size_t)k, 80, (const void**)&I.zp},
+        };
+        for (const Item& it : items) {
+            cudaError_t e = put_dev(m, it.src, it.bytes, it.dst);
+            if (e != cudaSuccess) return bail(e, "instance upload");
+        }
+    }
+    DevBatch& b = m->b;
+    const size_t out_n = std::max<size_t>((size_t)r->P * T, 1);
+    cudaError_t e;
+    if ((e = put_dev(m, dinst.data(), dinst.size() * sizeof(DevInst), (const void**)&b.insts)) ||
+        (e = put_dev(m, hp.prog.data(), hp.prog.size() * 4, (const void**)&b.prog)) ||
+        (e = put_dev(m, hp.consts.data(), hp.consts.size() * 8, (const void**)&b.consts)) ||
+        (e = put_dev(m, hp.slots.data(), hp.slots.size(), (const void**)&b.slots)) ||
+        (e = put_dev(m, hp.meta.data(), hp.meta.size() * sizeof(RuleMeta), (const void**)&b.meta)) ||
+        (e = put_dev(m, sampled, (size_t)n_sampled * 8, (const void**)&b.sampled)) ||
+        (e = put_dev(m, sampled_offsets, (size_t)K * 8, (const void**)&b.smp_off)) ||
+        (e = put_dev(m, order.data(), order.size() * 4, (const void**)&b.order)) ||
+        (e = put_dev(m, nullptr, out_n * 8, (const void**)&b.out)) ||
+        (e = put_dev(m, nullptr, 8, (const void**)&b.counter)) ||
+        (e = put_dev(m, nullptr, 8, (const void**)&b.error)))
+        return bail(e, "batch upload");
+    b.P = r->P;
+    b.T = T;
+    b.group_size = r->P > 0 ? r->P : 1;
+    b.n = 0;
+    b.stats = nullptr;
+    b.rows = hp.rows;
+    b.prog_cap = hp.prog_cap;
+    b.const_cap = hp.const_cap;
+    const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
+    int nmax = 0;
+    for (int k = 0; k < K; k++) nmax = std::max(nmax, hs[k].n);
+    char kb[256];
+    std::snprintf(kb, sizeof kb, "K%d P%d T%d rows%d prog%d sm%d nmax%d|", K, r->P, T, hp.rows,
+                  hp.prog_cap, m->sm_count, nmax);
+    m->key = kb;
+    for (int k = 0; k < K; k++) m->key += std::to_string(hs[k].n) + ",";
+    for (int sh = 0; sh < SIDR_MULTI_SHAPES; sh++) {
+        const int wpb = kShapes[sh][0];
+        m->block[sh] = 32 * wpb;
+        m->smem[sh] = slice * wpb;
+        if (m->smem[sh] > m->smem_optin) {
+            multi_free(m);
+            return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
+        }
+        if ((e = cudaFuncSetAttribute(multi_kernel(sh), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)m->smem[sh])) != cudaSuccess)
+            return bail(e, "cudaFuncSetAttribute");
+        int per_sm = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_kernel(sh), m->block[sh],
+                                                               m->smem[sh])) != cudaSuccess)
+            return bail(e, "occupancy");
+        const long long items = (long long)r->P * T;
+        m->grid[sh] = (int)std::max<long long>(
+            1, std::min<long long>((items + wpb - 1) / wpb, (long long)m->sm_count * std::max(per_sm, 1)));
+    }
+    {
+        std::lock_guard<std::mutex> g(g_tune_lock);
+        auto it = g_tune_cache.find(m->key);
+        if (it != g_tune_cache.end()) m->shape = it->second;
+    }
+    *out = m;
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_set_shape(sidr_multi* m, int32_t shape) {
+    if (!m || shape < 0 || shape >= SIDR_MULTI_SHAPES) return fail(SIDR_ERR_INVALID, "bad shape");
+    if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
+    m->shape = shape;
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, float* ms) {
+    if (!m) return fail(SIDR_ERR_INVALID, "null batch");
+    if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
+    SIDR_CUDA(cudaSetDevice(m->device));
+    if ((long long)m->P * m->T == 0) {
+        if (chosen) *chosen = m->shape;
+        return SIDR_OK;
+    }
+    cudaEvent_t e0, e1;
+    SIDR_CUDA(cudaEventCreate(&e0));
+    SIDR_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_sh = 0;
+    for (int sh = 0; sh < SIDR_MULTI_SHAPES; sh++) {
+        float t_best = 1e30f;
+        for (int k = 0; k < (reps < 1 ? 1 : reps) + 1; k++) {  // first run warms up
+            SIDR_CUDA(cudaEventRecord(e0, 0));
+            sidr_status s = multi_launch(m, sh, 0);
+            if (s) return s;
+            SIDR_CUDA(cudaEventRecord(e1, 0));
+            SIDR_CUDA(cudaEventSynchronize(e1));
+            float t = 0.f;
+            SIDR_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            if (k > 0 && t < t_best) t_best = t;
+        }
+        if (ms) ms[sh] = t_best;
+        if (t_best < best) {
+            best = t_best;
+            best_sh = sh;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    m->shape = best_sh;
+    {
+        std::lock_guard<std::mutex> g(g_tune_lock);
+        g_tune_cache[m->key] = best_sh;
+    }
+    if (chosen) *chosen = best_sh;
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_capture(sidr_multi* m) {
+    if (!m) return fail(SIDR_ERR_INVALID, "null batch");
+    if (m->gexec) return SIDR_OK;
+    SIDR_CUDA(cudaSetDevice(m->device));
+    if (!m->gstream) SIDR_CUDA(cudaStreamCreateWithFlags(&m->gstream, cudaStreamNonBlocking));
+    SIDR_CUDA(cudaStreamBeginCapture(m->gstream, cudaStreamCaptureModeThreadLocal));
+    sidr_status s = SIDR_OK;
+    if ((long long)m->P * m->T > 0) s = multi_launch(m, m->shape, m->gstream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(m->gstream, &g);
+    if (s) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) return fail(SIDR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    m->graph = g;
+    SIDR_CUDA(cudaGraphInstantiate(&m->gexec, m->graph, 0));
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_run(sidr_multi* m, void* stream) {
+    if (!m) return fail(SIDR_ERR_INVALID, "null batch");
+    SIDR_CUDA(cudaSetDevice(m->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (m->gexec) {
+        SIDR_CUDA(cudaGraphLaunch(m->gexec, st));
+        if ((long long)m->P * m->T > 0) g_launches.fetch_add(1);
+        return SIDR_OK;
+    }
+    if ((long long)m->P * m->T == 0) return SIDR_OK;
+    return multi_launch(m, m->shape, st);
+}
+
+sidr_status sidr_multi_read(sidr_multi* m, double* out) {
+    if (!m) return fail(SIDR_ERR_INVALID, "null batch");
+    if ((long long)m->P * m->T == 0) return SIDR_OK;
+    if (!out) return fail(SIDR_ERR_INVALID, "output buffer is null");
+    SIDR_CUDA(cudaSetDevice(m->device));
+    SIDR_CUDA(cudaDeviceSynchronize());
+    SIDR_CUDA(cudaMemcpy(out, m->b.out, (size_t)m->P * m->T * 8, cudaMemcpyDeviceToHost));
+    return SIDR_OK;
+}
+
+void sidr_multi_destroy(sidr_multi* m) { multi_free(m); }
+
+}  // extern "C"

@@ -117,6 +117,7 @@ struct RuleMeta {
     int16_t res;        // result operand
     int8_t reach_k;     // deepest REACH-k step needed (0, 1, 3, 5)
     uint16_t scan_ops;  // op-model cost of one fused-scan neighbour (counting only)
+    int16_t inst;       // instance of a multi-instance batch (0 otherwise)
     uint32_t need;      // NeedBits
     uint64_t explore;   // bit s set: exploration slot s is read
 };
@@ -133,6 +134,12 @@ struct DevBatch {
     unsigned long long* stats;    // [kStats] counters (may be null)
     int* error;                   // kernel error word
     int rows, prog_cap, const_cap;  // per-warp shared-memory sizing
+    // Multi-instance batches: per-instance descriptors, scenario block offsets
+    // (doubles; instance k's [T][n_k] block starts at sampled + smp_off[k]), and
+    // the order in which rules are handed out (null = index order).
+    const DevInst* insts;
+    const int64_t* smp_off;
+    const int32_t* order;
 };
 
 }  // namespace sidr

@@ -59,6 +59,7 @@ __device__ unsigned long long sidr_section_cycles[16];
 
 // Shared-memory slice of one warp.
 struct WarpSmem {
+    DevInst* inst;     // the rule's instance (multi-instance batches)
     double* rows;      // [rows][32]
     double* cst;       // [const_cap]
     uint32_t* prog;    // [prog_cap]
@@ -71,8 +72,13 @@ struct WarpSmem {
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// A copy of the current rule's instance descriptor (multi-instance batches)
+// closes every warp's slice.
+constexpr size_t kInstBytes = (sizeof(DevInst) + 15) / 16 * 16;
+
 __host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int prog_cap) {
-    size_t b = (size_t)rows * 32 * sizeof(double);
+    size_t b = kInstBytes;
+    b += (size_t)rows * 32 * sizeof(double);
     b += (size_t)const_cap * sizeof(double);
     b += align_up((size_t)prog_cap * sizeof(uint32_t), 8);
     b += (size_t)kMaxN * sizeof(int16_t);
@@ -84,6 +90,8 @@ __host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int 
 __device__ __forceinline__ WarpSmem carve(unsigned char* base, int rows, int const_cap,
                                           int prog_cap) {
     WarpSmem s;
+    s.inst = reinterpret_cast<DevInst*>(base);
+    base += kInstBytes;
     s.rows = reinterpret_cast<double*>(base);
     s.cst = s.rows + (size_t)rows * 32;
     s.prog = reinterpret_cast<uint32_t*>(s.cst + const_cap);
@@ -902,9 +910,10 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
     return total;
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
-    eval_kernel(const DevInst I, const DevBatch B) {
+// The persistent work loop.  MULTI: every rule carries its instance; the
+// warp stages the instance descriptor with the rule's program.
+template <bool COUNT, bool MULTI>
+__device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -920,17 +929,27 @@ __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
         if (lane == 0) item = atomicAdd(B.counter, 1ull);
         item = __shfl_sync(kFull, item, 0);
         if (item >= total) break;
-        const int p = (int)(item / (unsigned long long)B.T);
+        const int r = (int)(item / (unsigned long long)B.T);
         const int s = (int)(item % (unsigned long long)B.T);
+        const int p = B.order ? B.order[r] : r;
         if (p != staged) {
             rm = B.meta[p];
             for (int q = lane; q < rm.n_ins; q += 32) S.prog[q] = B.prog[rm.prog_off + q];
             for (int q = lane; q < rm.n_const; q += 32) S.cst[q] = B.consts[rm.const_off + q];
             for (int q = lane; q < rm.K; q += 32) S.slots[q] = B.slots[rm.slot_off + q];
+            if (MULTI) {
+                const unsigned long long* src =
+                    reinterpret_cast<const unsigned long long*>(B.insts + rm.inst);
+                unsigned long long* dst = reinterpret_cast<unsigned long long*>(S.inst);
+                for (int q = lane; q < (int)(sizeof(DevInst) / 8); q += 32) dst[q] = src[q];
+            }
             staged = p;
             __syncwarp();
         }
-        const double* smp = B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
+        const DevInst& I = MULTI ? *S.inst : I0;
+        const double* smp =
+            MULTI ? B.sampled + B.smp_off[rm.inst] + (size_t)s * I.n
+                  : B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
         const double tot = rollout<COUNT>(I, S, rm, smp, wc);
         if (lane == 0) B.out[(size_t)p * B.T + s] = tot;
     }
@@ -946,6 +965,20 @@ __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
             for (int k = 0; k < kStats; k++) atomicAdd(&B.stats[k], v[k]);
         }
     }
+}
+
+// Single-instance evaluator (the instance travels as a kernel parameter).
+template <bool COUNT>
+__global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
+    eval_kernel(const DevInst I, const DevBatch B) {
+    eval_body<COUNT, false>(I, B);
+}
+
+// Multi-instance evaluator, one instantiation per block shape (warps per
+// block x minimum resident blocks); the autotuner picks among them.
+template <int WPB, int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) eval_multi_kernel(const DevBatch B) {
+    eval_body<false, true>(DevInst{}, B);
 }
 
 }  // namespace sidr

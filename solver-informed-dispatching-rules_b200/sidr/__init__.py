@@ -64,7 +64,8 @@ EXPORTS = [
     "sidr_batch_create", "sidr_batch_run", "sidr_batch_read", "sidr_batch_fitness",
     "sidr_batch_device_out", "sidr_batch_destroy", "sidr_batch_set_counting", "sidr_batch_counts",
     "sidr_kernel_launches", "sidr_rules_check", "sidr_last_transfer_bytes", "sidr_fp64_peak",
-    "sidr_evaluate_static",
+    "sidr_evaluate_static", "sidr_multi_create", "sidr_multi_autotune", "sidr_multi_set_shape",
+    "sidr_multi_capture", "sidr_multi_run", "sidr_multi_read", "sidr_multi_destroy",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -313,3 +314,90 @@ class Context:
                                         mask_group or max(rules.P, 1), k.i64(masks),
                                         C.byref(h)))
         return Batch(self, h.value, rules.P, T)
+
+
+class Multi:
+    """A multi-instance batch (sidr_multi_*): several instances of uneven size,
+    each with its own rules, scenarios and mask, in one persistent launch."""
+
+    SHAPES = ((4, 3), (8, 2), (2, 6))  # warps per block, min blocks per SM
+
+    def __init__(self, sds, zps, rules_per_instance, sampled_per_instance, T, masks,
+                 device: int = 0):
+        L = load()
+        if not getattr(L, "_multi_ready", False):
+            vp = C.c_void_p
+            L.sidr_multi_create.argtypes = [C.POINTER(_Inst), _dp, C.c_int32, C.POINTER(_Rules),
+                                            _ip, _dp, C.c_int64, _lp, C.c_int32, _lp, C.c_int32,
+                                            C.POINTER(vp)]
+            L.sidr_multi_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32),
+                                              C.POINTER(C.c_float)]
+            L.sidr_multi_set_shape.argtypes = [vp, C.c_int32]
+            L.sidr_multi_capture.argtypes = [vp]
+            L.sidr_multi_run.argtypes = [vp, vp]
+            L.sidr_multi_read.argtypes = [vp, _dp]
+            L.sidr_multi_destroy.argtypes = [vp]
+            L._multi_ready = True
+        from .rules import pack_compiled
+        K = len(sds)
+        k = _Keep()
+        insts = (_Inst * K)(*[k.inst(sd) for sd in sds])
+        zp = np.ascontiguousarray(np.stack([np.asarray(z, dtype=np.float64) for z in zps]))
+        compiled, owner = [], []
+        for i, r in enumerate(rules_per_instance):
+            for p in range(r.P):
+                compiled.append(r.rule(p))
+                owner.append(i)
+        allr = pack_compiled(compiled)
+        self.P, self.T, self.counts = allr.P, T, [r.P for r in rules_per_instance]
+        offs, blocks, at = [], [], 0
+        for sd, smp in zip(sds, sampled_per_instance):
+            a = np.ascontiguousarray(smp, dtype=np.float64).reshape(-1)[:T * sd.n]
+            offs.append(at)
+            blocks.append(a)
+            at += a.size
+        flat = np.concatenate(blocks) if blocks else np.zeros(1)
+        m = np.ascontiguousarray(np.stack([np.asarray(x, dtype=np.int64) for x in masks]))
+        rr = k.rules(allr)
+        h = C.c_void_p()
+        _check(L.sidr_multi_create(insts, zp.ctypes.data_as(_dp), K, C.byref(rr),
+                                   k.i32(np.asarray(owner, dtype=np.int32)), k.f64(flat),
+                                   int(flat.size), k.i64(np.asarray(offs, dtype=np.int64)), T,
+                                   m.ctypes.data_as(_lp), device, C.byref(h)))
+        self.h = h.value
+
+    def autotune(self, reps: int = 1):
+        ch = C.c_int32()
+        ms = (C.c_float * len(self.SHAPES))()
+        _check(load().sidr_multi_autotune(self.h, reps, C.byref(ch), ms))
+        return ch.value, [float(x) for x in ms]
+
+    def set_shape(self, shape: int):
+        _check(load().sidr_multi_set_shape(self.h, shape))
+
+    def capture(self):
+        _check(load().sidr_multi_capture(self.h))
+
+    def run(self, stream: int = 0):
+        _check(load().sidr_multi_run(self.h, C.c_void_p(stream)))
+
+    def read(self):
+        """Scores split per instance: a list of [P_k, T] arrays."""
+        out = np.zeros((self.P, self.T))
+        _check(load().sidr_multi_read(self.h, _d(out)))
+        res, at = [], 0
+        for c in self.counts:
+            res.append(out[at:at + c])
+            at += c
+        return res
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().sidr_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

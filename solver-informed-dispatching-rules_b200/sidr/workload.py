@@ -13,6 +13,10 @@ evaluation sizes the benchmark names, with the reference's own rule generator
                     H=1000, m=3; the 1024-rule initial population of a GP run
                     (depth 2-8, 29-terminal menu, the GP's own RHH settings,
                     engine/gp.hpp:13-18); 500 scenarios from base seed 1.
+  batched_uneven    40 instances of 25/50/100/288 customers, uniform/clustered/
+                    mixed layouts, m in {2,3,4}, H in {230,1000}, each with 1000
+                    rules of log-uniform length 3-255 and 500 scenarios, for the
+                    multi-instance launch.
 """
 from __future__ import annotations
 
@@ -21,8 +25,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from .instance import SimData, generate_instance, parse_solomon_text
-from .rules import (EXTRA, FUNCTIONS, NS_TERMINALS, PackedRules, gen_durations, pack,
-                    ramped_half_and_half, term_mask_from)
+from .rules import (EXTRA, FUNCTIONS, NS_TERMINALS, PackedRules, compile_rule, gen_durations,
+                    pack, ramped_half_and_half, term_mask_from)
 
 MENU29 = NS_TERMINALS + EXTRA
 
@@ -60,6 +64,59 @@ def plain_eval(P: int = 256, S: int = 500) -> Workload:
 
 def gp_generation(P: int = 1024, S: int = 500) -> Workload:
     return build("gp_generation", 100, "clustered", 1000.0, 3, 2, P, 2, 8, 0, S, 1)
+
+
+def _rules_of_lengths(seed: int, count: int, lo: int = 3, hi: int = 255):
+    """`count` rules over the 29-terminal menu whose post-order lengths follow a
+    log-uniform distribution on [lo, hi]: a pool of ramped half-and-half rules
+    of depths 1-7 is drawn with Mt19937(seed), then for each log-uniform target
+    length the pool rule of the nearest length is taken."""
+    import math
+    import random as _random
+    pool = ramped_half_and_half(MENU29, FUNCTIONS, 1, 7, seed, 2048)
+    by_len = {}
+    for t in pool:
+        by_len.setdefault(len(compile_rule(t)[0]), []).append(t)
+    lengths = sorted(by_len)
+    rng = _random.Random(seed + 1)
+    out = []
+    for _ in range(count):
+        target = math.exp(math.log(lo) + rng.random() * (math.log(hi) - math.log(lo)))
+        L = min(lengths, key=lambda x: (abs(x - target), x))
+        bucket = by_len[L]
+        out.append(bucket[rng.randrange(len(bucket))])
+    return out
+
+
+@dataclass
+class MultiWorkload:
+    name: str
+    sds: list
+    rules: list       # PackedRules per instance
+    sampled: list     # [S, n_k] per instance
+    masks: list
+    S: int
+
+
+def batched_uneven(K: int = 40, rules_per_instance: int = 1000, S: int = 500) -> MultiWorkload:
+    """The uneven batch: K instances cycling through 25/50/100/288 customers,
+    uniform/clustered/mixed layouts, m in {2,3,4}, H in {230,1000}; each with
+    its own rules (log-uniform lengths 3-255) and S scenarios (base seed
+    1 + 1000k)."""
+    sizes, layouts = (25, 50, 100, 288), ("uniform", "clustered", "mixed")
+    sds, rules, sampled, masks = [], [], [], []
+    for k in range(K):
+        n = sizes[k % 4]
+        layout = layouts[k % 3]
+        m = 2 + k % 3
+        H = (230.0, 1000.0)[(k // 4) % 2]
+        text = generate_instance(n, layout, H, 100 + k, n_clusters=8)
+        sd = SimData.from_instance(parse_solomon_text(text), m=m)
+        sds.append(sd)
+        rules.append(pack(_rules_of_lengths(1000 + k, rules_per_instance)))
+        sampled.append(gen_durations(sd.durations, sd.sigma, S, 1 + 1000 * k))
+        masks.append(term_mask_from(MENU29))
+    return MultiWorkload("batched_uneven", sds, rules, sampled, masks, S)
 
 
 WORKLOADS = {"plain_eval": plain_eval, "gp_generation": gp_generation}

@@ -919,7 +919,8 @@ cudaError_t put_dev(sidr_multi* m, const void* src, size_t bytes, const void** d
     if (e != cudaSuccess) return e;
     m->owned.push_back(p);
     *dst = p;
-    return bytes ? cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+    if (!src || !bytes) return cudaSuccess;  // allocation only
+    return cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
 }
 
 sidr_status multi_launch(sidr_multi* m, int shape, cudaStream_t st) {

@@ -468,12 +468,16 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     }
                     if (need & kNeedNSTW) {
                         const double arrive = fin + gd.y;
-                        double wait = I.open_t[j] - arrive;
-                        if (wait < 0.0) wait = 0.0;
-                        const double win = I.close_t[j] - I.open_t[j];
-                        double wt = win > 1e-10 ? 1.0 - wait / win : 1.0;
-                        if (wt < 0.0) wt = 0.0;
-                        nstw += Rj * wt;
+                        const double oj = I.open_t[j];
+                        if (arrive >= oj) {
+                            nstw += Rj;  // wait 0: weight 1 - 0/win = 1 (or 1 when win <= 1e-10)
+                        } else {
+                            const double wait = oj - arrive;
+                            const double win = I.close_t[j] - oj;
+                            double wt = win > 1e-10 ? 1.0 - wait / win : 1.0;
+                            if (wt < 0.0) wt = 0.0;
+                            nstw += Rj * wt;
+                        }
                     }
                 }
             }

@@ -163,18 +163,26 @@ __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const do
     const int16_t* ord = I.ord + row;
     const double* sT = table + row;
     const int cnt = I.cnt_pos[o];
+    double res = 0.0;
+    // The scan leaves both loops by flags rather than returning from inside
+    // the unrolled body, which keeps the warp's exit point single.
     for (int k = 0; k < cnt; k += 4) {
         const Chunk4 c = load_chunk(sT, ord, k);
+        bool hit = false;
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            if (k + e >= cnt) return 0.0;
+            if (k + e >= cnt) break;
             if (COUNT) hops++;
             const int q = c.q[e];  // coincident entries keep bit 14 and never match
-            if (q < kOrdCoincident && q != x0 && q != x1 && is_unvisited(S, q) && tm <= c.t[e])
-                return I.scores[q];
+            if (q < kOrdCoincident && q != x0 && q != x1 && is_unvisited(S, q) && tm <= c.t[e]) {
+                res = I.scores[q];
+                hit = true;
+                break;
+            }
         }
+        if (hit) break;
     }
-    return 0.0;
+    return res;
 }
 
 // One REACH-k greedy step (engine/sim_terms.hpp:415-431): the best unvisited
@@ -188,19 +196,23 @@ __device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm,
     const int16_t* ord = I.ord + row;
     const double* sF = I.sF + row;
     const int cnt = I.cnt_gm1[o];
+    int res = -1;
     for (int k = 0; k < cnt; k += 4) {
         const Chunk4 c = load_chunk(sF, ord, k);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            if (k + e >= cnt) return -1;
+            if (k + e >= cnt) break;
             if (COUNT) hops++;
             const int q = c.q[e] & (kOrdCoincident - 1);
             if (q != p0 && q != p1 && q != p2 && q != p3 && q != p4 && is_unvisited(S, q) &&
-                tm <= c.t[e])
-                return q;
+                tm <= c.t[e]) {
+                res = q;
+                break;
+            }
         }
+        if (res >= 0) break;
     }
-    return -1;
+    return res;
 }
 
 // ------------------------------------------------- exploration terminals

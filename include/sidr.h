@@ -226,6 +226,12 @@ sidr_status sidr_last_transfer_bytes(int64_t* h2d, int64_t* d2h);
  * denominator of the evaluator's roofline; no reference counterpart. */
 sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s);
 
+/* The device erf (fn 0), erfc (1) and exp (2) that the evaluator uses for
+ * ATRISK's normal CDF and PBUST (engine/sim_terms.hpp:221-223, :571) in place
+ * of CUDA's, on host arrays x[n] -> out[n] (diagnostic; no reference
+ * counterpart).  They reproduce glibc 2.39's results bit for bit. */
+sidr_status sidr_libm_eval(int32_t fn, const double* x, int64_t n, int device, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -30,7 +30,7 @@ CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall"]
 
 CU_SOURCES = ["sidr_capi.cu"]
 CPP_SOURCES = ["sidr_host.cpp", "sidr_gp.cpp"]
-HEADERS = ["sidr_internal.hpp", "sidr_kernel.cuh", "sidr_host.hpp"]
+HEADERS = ["sidr_internal.hpp", "sidr_kernel.cuh", "sidr_host.hpp", "sidr_libm.cuh", "sidr_exp_table.h"]
 PUBLIC_HEADERS = ["sidr.h", "sidr_gp.h"]
 
 

@@ -381,6 +381,33 @@ sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s) {
     return SIDR_OK;
 }
 
+__global__ void libm_kernel(int fn, const double* x, long long n, double* out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        out[i] = fn == 0 ? libm::erf_(v) : fn == 1 ? libm::erfc_(v) : libm::exp_(v);
+    }
+}
+
+sidr_status sidr_libm_eval(int32_t fn, const double* x, int64_t n, int device, double* out) {
+    if (fn < 0 || fn > 2 || n < 0 || (n > 0 && (!x || !out))) return fail(SIDR_ERR_INVALID, "bad argument");
+    if (n == 0) return SIDR_OK;
+    SIDR_CUDA(cudaSetDevice(device));
+    double *dx = nullptr, *dout = nullptr;
+    SIDR_CUDA(cudaMalloc(&dx, (size_t)n * sizeof(double)));
+    cudaError_t e = cudaMalloc(&dout, (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        libm_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256>>>(fn, dx, n, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(SIDR_ERR_CUDA, std::string("libm eval: ") + cudaGetErrorString(e));
+    return SIDR_OK;
+}
+
 sidr_status sidr_rules_check(const sidr_rules_desc* r, const int64_t* masks, int32_t mask_group,
                              int32_t* max_rows) {
     sidr_status s = check_rules(r);

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "sidr_internal.hpp"
+#include "sidr_libm.cuh"
 
 namespace sidr {
 
@@ -541,7 +542,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     if (sd_c > 1e-9) {
                         if (dw >= 8.5 * sd_c) pw = 1.0;
                         else if (dw <= -8.5 * sd_c) pw = 0.0;
-                        else pw = 0.5 * (1.0 + erf((dw / sd_c) * 0.7071067811865476));
+                        else pw = 0.5 * (1.0 + libm::erf_((dw / sd_c) * 0.7071067811865476));
                     } else {
                         pw = marr <= cj ? 1.0 : 0.0;
                     }
@@ -562,7 +563,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                             const double db = tmax - mb;
                             if (db >= 8.5 * pv) pb = 1.0;
                             else if (db <= -8.5 * pv) pb = 0.0;
-                            else pb = 0.5 * (1.0 + erf((db / pv) * 0.7071067811865476));
+                            else pb = 0.5 * (1.0 + libm::erf_((db / pv) * 0.7071067811865476));
                         } else {
                             pb = mb <= tmax ? 1.0 : 0.0;
                         }
@@ -667,7 +668,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         const double sd = kSigma * dur_i;
         if (sd > 1e-12) {
             const double z = (I.close_t[sbq] - ab) / (sd * kSqrt2);
-            pbust = 0.5 * erfc(z);
+            pbust = 0.5 * libm::erfc_(z);
         } else {
             pbust = ab > I.close_t[sbq] ? 1.0 : 0.0;
         }

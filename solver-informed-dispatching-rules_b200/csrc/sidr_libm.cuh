@@ -1,0 +1,282 @@
+// sidr_libm.cuh -- erf, erfc and exp with the results of the C library the
+// reference simulator runs on, for host and device.
+//
+// The reference evaluates ATRISK's normal CDF with erf and PBUST with erfc
+// (engine/sim_terms.hpp:221-223, :571) through glibc.  CUDA's erf and erfc are
+// other approximations: they differ from glibc's in the last bit for a share
+// of arguments, which changes a decision whenever a rule's priorities tie to
+// within that bit (GP rules such as (SCORE/ATRISK)*ATRISK do).  So the
+// evaluator computes them with the same published algorithms, evaluated in
+// the same order, as glibc 2.39 on x86-64:
+//
+//   erf, erfc  fdlibm 5.3's rational approximations (Sun Microsystems, 1993):
+//              x + x*P(x^2)/Q(x^2) below 0.84375; erx + P(s)/Q(s) with
+//              s = |x|-1 below 1.25; exp(-z^2-0.5625)*exp((z-x)(z+x)+R/S)/x
+//              with R/S in 1/x^2 (two coefficient sets split at 1/0.35) below
+//              6 (erf) or 28 (erfc); the polynomials evaluated pairwise
+//              (c0 + t*c1) + t^2*(c2 + t*c3) + ..., as glibc's s_erf.c does.
+//   exp        the table-driven exponential of glibc 2.28+ (Szabolcs Nagy,
+//              ARM optimized-routines): x = k*ln2/128 + r, 2^(k/128) from a
+//              128-entry table (sidr_exp_table.h, generated by
+//              gen_exp_table.py), exp(r)-1 by a degree-5 polynomial, with the
+//              multiply-adds fused where glibc's FMA build (the one selected
+//              on every x86-64 CPU with FMA) fuses them.
+//
+// Every other operation is a separately rounded IEEE operation (the device
+// code is compiled with -fmad=false, the host code with -ffp-contract=off).
+// tests/test_libm.py compares these functions with the host's glibc over
+// random arguments in every interval, for the host and the device builds.
+#pragma once
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "sidr_exp_table.h"
+
+#ifdef __CUDACC__
+#define SIDR_HD __host__ __device__ __forceinline__
+// erf and erfc stay out of line on the device: they run only for arguments
+// whose result is not exactly 0 or 1, and inlining them into the neighbour
+// scans would raise their register count
+#define SIDR_HD_CALL __host__ __device__ __noinline__
+#else
+#define SIDR_HD inline
+#define SIDR_HD_CALL inline
+#endif
+
+namespace sidr {
+namespace libm {
+
+#ifdef __CUDACC__
+__device__ const uint64_t kExpTableDev[256] = {SIDR_EXP_TABLE_ENTRIES};
+#endif
+static const uint64_t kExpTableHost[256] = {SIDR_EXP_TABLE_ENTRIES};
+
+SIDR_HD uint64_t bits_of(double x) {
+#ifdef __CUDA_ARCH__
+    return (uint64_t)__double_as_longlong(x);
+#else
+    uint64_t u;
+    memcpy(&u, &x, 8);
+    return u;
+#endif
+}
+
+SIDR_HD double double_of(uint64_t u) {
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)u);
+#else
+    double x;
+    memcpy(&x, &u, 8);
+    return x;
+#endif
+}
+
+SIDR_HD uint64_t exp_table(int i) {
+#ifdef __CUDA_ARCH__
+    return kExpTableDev[i];
+#else
+    return kExpTableHost[i];
+#endif
+}
+
+// a*b + c with one rounding.
+SIDR_HD double fused(double a, double b, double c) { return fma(a, b, c); }
+
+// ------------------------------------------------------------------ exp
+
+// exp(x).  The argument is reduced to r in about [-ln2/256, ln2/256]:
+// k = round(x*128/ln2) through the 1.5*2^52 shift, r = x - k*ln2/128 with
+// ln2/128 in two parts.  Then exp(x) = 2^(k/128) * exp(r)
+// ~= S*(1 + tail + (exp(r)-1)) = S + S*tmp.
+SIDR_HD double exp_(double x) {
+    const double kInvLn2N = 0x1.71547652b82fep0 * 128.0;
+    const double kNegLn2HiN = -0x1.62e42fefa0000p-8;
+    const double kNegLn2LoN = -0x1.cf79abc9e3b3ap-47;
+    const double kShift = 0x1.8p52;
+    const double kC2 = 0x1.ffffffffffdbdp-2, kC3 = 0x1.555555555543cp-3;
+    const double kC4 = 0x1.55555cf172b91p-5, kC5 = 0x1.1111167a4d017p-7;
+
+    const uint32_t top = (uint32_t)(bits_of(x) >> 52) & 0x7ffu;  // biased exponent of |x|
+    bool scaled = false;
+    if (top - 0x3c9u >= 0x408u - 0x3c9u) {  // |x| < 2^-54 or |x| >= 512 (or not finite)
+        if (top < 0x3c9u) return 1.0 + x;    // tiny: rounds to 1 (or 1 + x)
+        if (top >= 0x409u) {                 // |x| >= 1024, inf, nan
+            if (bits_of(x) == 0xfff0000000000000ull) return 0.0;
+            if (top >= 0x7ffu) return 1.0 + x;
+            return (bits_of(x) >> 63) ? 0.0 : HUGE_VAL;
+        }
+        scaled = true;  // 512 <= |x| < 1024: the result's scale needs care
+    }
+    double kd = fused(kInvLn2N, x, kShift);
+    const uint64_t ki = bits_of(kd);
+    kd -= kShift;
+    const double r = fused(kd, kNegLn2LoN, fused(kd, kNegLn2HiN, x));
+    const int idx = (int)(2 * (ki % 128));
+    const double tail = double_of(exp_table(idx));
+    uint64_t sbits = exp_table(idx + 1) + (ki << 45);
+    const double r2 = r * r;
+    const double tmp = fused(r2 * r2, fused(r, kC5, kC4), fused(r2, fused(r, kC3, kC2), tail + r));
+    if (!scaled) {
+        const double scale = double_of(sbits);
+        return fused(scale, tmp, scale);
+    }
+    if ((ki & 0x80000000u) == 0) {  // k > 0: scale by 2^1009 afterwards
+        sbits -= 1009ull << 52;
+        const double scale = double_of(sbits);
+        return 0x1p1009 * fused(scale, tmp, scale);
+    }
+    // k < 0: build the result at 2^1022 times its size and round it once to
+    // the subnormal precision it will have (glibc's FMA build leaves these
+    // products unfused)
+    sbits += 1022ull << 52;
+    const double scale = double_of(sbits);
+    const double st = scale * tmp;
+    double y = scale + st;
+    if (y < 1.0) {
+        double lo = scale - y + st;
+        const double hi = 1.0 + y;
+        lo = 1.0 - hi + y + lo;
+        y = (hi + lo) - 1.0;
+        if (y == 0.0) y = 0.0;
+    }
+    return 0x1p-1022 * y;
+}
+
+// ------------------------------------------------------------- erf, erfc
+
+// fdlibm's coefficients.
+struct ErfCoef {
+    // erf(x) = x + x*PP(z)/QQ(z), z = x^2, |x| < 0.84375
+    static constexpr double efx = 1.28379167095512586316e-01;
+    static constexpr double pp0 = 1.28379167095512558561e-01, pp1 = -3.25042107247001499370e-01,
+                            pp2 = -2.84817495755985104766e-02, pp3 = -5.77027029648944159157e-03,
+                            pp4 = -2.37630166566501626084e-05;
+    static constexpr double qq1 = 3.97917223959155352819e-01, qq2 = 6.50222499887672944485e-02,
+                            qq3 = 5.08130628187576562776e-03, qq4 = 1.32494738004321644526e-04,
+                            qq5 = -3.96022827877536812320e-06;
+    // erf(x) = erx + PA(s)/QA(s), s = |x|-1, 0.84375 <= |x| < 1.25
+    static constexpr double erx = 8.45062911510467529297e-01;
+    static constexpr double pa0 = -2.36211856075265944077e-03, pa1 = 4.14856118683748331666e-01,
+                            pa2 = -3.72207876035701323847e-01, pa3 = 3.18346619901161753674e-01,
+                            pa4 = -1.10894694282396677476e-01, pa5 = 3.54783043256182359371e-02,
+                            pa6 = -2.16637559486879084300e-03;
+    static constexpr double qa1 = 1.06420880400844228286e-01, qa2 = 5.40397917702171048937e-01,
+                            qa3 = 7.18286544141962662868e-02, qa4 = 1.26171219808761642112e-01,
+                            qa5 = 1.36370839120290507362e-02, qa6 = 1.19844998467991074170e-02;
+    // erfc(x) = exp(-x^2-0.5625+RA(t)/SA(t))/x, t = 1/x^2, 1.25 <= |x| < 1/0.35
+    static constexpr double ra0 = -9.86494403484714822705e-03, ra1 = -6.93858572707181764372e-01,
+                            ra2 = -1.05586262253232909814e+01, ra3 = -6.23753324503260060396e+01,
+                            ra4 = -1.62396669462573470355e+02, ra5 = -1.84605092906711035994e+02,
+                            ra6 = -8.12874355063065934246e+01, ra7 = -9.81432934416914548592e+00;
+    static constexpr double sa1 = 1.96512716674392571292e+01, sa2 = 1.37657754143519042600e+02,
+                            sa3 = 4.34565877475229228821e+02, sa4 = 6.45387271733267880336e+02,
+                            sa5 = 4.29008140027567833386e+02, sa6 = 1.08635005541779435134e+02,
+                            sa7 = 6.57024977031928170135e+00, sa8 = -6.04244152148580987438e-02;
+    // the same with RB/SB, |x| >= 1/0.35
+    static constexpr double rb0 = -9.86494292470009928597e-03, rb1 = -7.99283237680523006574e-01,
+                            rb2 = -1.77579549177547519889e+01, rb3 = -1.60636384855821916062e+02,
+                            rb4 = -6.37566443368389627722e+02, rb5 = -1.02509513161107724954e+03,
+                            rb6 = -4.83519191608651397019e+02;
+    static constexpr double sb1 = 3.03380607434824582924e+01, sb2 = 3.25792512996573918826e+02,
+                            sb3 = 1.53672958608443695994e+03, sb4 = 3.19985821950859553908e+03,
+                            sb5 = 2.55305040643316442583e+03, sb6 = 4.74528541206955367215e+02,
+                            sb7 = -2.24409524465858183362e+01;
+};
+
+// PP(z)/QQ(z) for |x| < 0.84375, pairwise.
+SIDR_HD double erf_small_ratio(double z) {
+    using C = ErfCoef;
+    const double z2 = z * z, z4 = z2 * z2;
+    const double p = (C::pp0 + z * C::pp1) + z2 * (C::pp2 + z * C::pp3) + z4 * C::pp4;
+    const double q = (1.0 + z * C::qq1) + z2 * (C::qq2 + z * C::qq3) + z4 * (C::qq4 + z * C::qq5);
+    return p / q;
+}
+
+// PA(s) and QA(s) for 0.84375 <= |x| < 1.25, pairwise.
+SIDR_HD void erf_mid_terms(double s, double& p, double& q) {
+    using C = ErfCoef;
+    const double s2 = s * s, s4 = s2 * s2, s6 = s4 * s2;
+    p = (C::pa0 + s * C::pa1) + s2 * (C::pa2 + s * C::pa3) + s4 * (C::pa4 + s * C::pa5) + s6 * C::pa6;
+    q = (1.0 + s * C::qa1) + s2 * (C::qa2 + s * C::qa3) + s4 * (C::qa4 + s * C::qa5) + s6 * C::qa6;
+}
+
+// The tail numerator for ax = |x| >= 1.25: exp(-z^2-0.5625) *
+// exp((z-ax)(z+ax)+R/S), z = ax with its low 32 bits cleared (so z*z is
+// exact); `near` selects the RA/SA set.
+SIDR_HD double erf_tail_num(double ax, bool near) {
+    using C = ErfCoef;
+    const double t = 1.0 / (ax * ax);
+    const double t2 = t * t, t4 = t2 * t2, t6 = t4 * t2;
+    double R, S;
+    if (near) {
+        const double t8 = t4 * t4;
+        R = (C::ra0 + t * C::ra1) + t2 * (C::ra2 + t * C::ra3) + t4 * (C::ra4 + t * C::ra5) +
+            t6 * (C::ra6 + t * C::ra7);
+        S = (1.0 + t * C::sa1) + t2 * (C::sa2 + t * C::sa3) + t4 * (C::sa4 + t * C::sa5) +
+            t6 * (C::sa6 + t * C::sa7) + t8 * C::sa8;
+    } else {
+        R = (C::rb0 + t * C::rb1) + t2 * (C::rb2 + t * C::rb3) + t4 * (C::rb4 + t * C::rb5) + t6 * C::rb6;
+        S = (1.0 + t * C::sb1) + t2 * (C::sb2 + t * C::sb3) + t4 * (C::sb4 + t * C::sb5) +
+            t6 * (C::sb6 + t * C::sb7);
+    }
+    const double z = double_of(bits_of(ax) & 0xffffffff00000000ull);
+    return exp_(-z * z - 0.5625) * exp_((z - ax) * (z + ax) + R / S);
+}
+
+SIDR_HD_CALL double erf_(double x) {
+    using C = ErfCoef;
+    const uint64_t u = bits_of(x);
+    const bool neg = (u >> 63) != 0;
+    const uint32_t ix = (uint32_t)(u >> 32) & 0x7fffffffu;  // high word of |x|
+    if (ix >= 0x7ff00000u) return (neg ? -1.0 : 1.0) + 1.0 / x;  // nan, +-inf
+    if (ix < 0x3feb0000u) {                                      // |x| < 0.84375
+        if (ix < 0x3e300000u) {                                  // |x| < 2^-28
+            if (ix < 0x00800000u) return 0.0625 * (16.0 * x + (16.0 * C::efx) * x);
+            return x + C::efx * x;
+        }
+        return x + x * erf_small_ratio(x * x);
+    }
+    if (ix < 0x3ff40000u) {  // 0.84375 <= |x| < 1.25
+        double p, q;
+        erf_mid_terms(fabs(x) - 1.0, p, q);
+        return neg ? -C::erx - p / q : C::erx + p / q;
+    }
+    if (ix >= 0x40180000u) return neg ? 1e-300 - 1.0 : 1.0 - 1e-300;  // |x| >= 6
+    const double ax = fabs(x);
+    const double r = erf_tail_num(ax, ix < 0x4006DB6Eu);
+    return neg ? r / ax - 1.0 : 1.0 - r / ax;
+}
+
+SIDR_HD_CALL double erfc_(double x) {
+    using C = ErfCoef;
+    const uint64_t u = bits_of(x);
+    const bool neg = (u >> 63) != 0;
+    const uint32_t hx = (uint32_t)(u >> 32);
+    const uint32_t ix = hx & 0x7fffffffu;
+    if (ix >= 0x7ff00000u) return (double)(neg ? 2 : 0) + 1.0 / x;  // nan, +-inf
+    if (ix < 0x3feb0000u) {                                         // |x| < 0.84375
+        if (ix < 0x3c700000u) return 1.0 - x;                       // |x| < 2^-56
+        const double y = erf_small_ratio(x * x);
+        if ((int32_t)hx < 0x3fd00000) return 1.0 - (x + x * y);  // x < 1/4
+        double r = x * y;
+        r += (x - 0.5);
+        return 0.5 - r;
+    }
+    if (ix < 0x3ff40000u) {  // 0.84375 <= |x| < 1.25
+        double p, q;
+        erf_mid_terms(fabs(x) - 1.0, p, q);
+        if (!neg) return (1.0 - C::erx) - p / q;
+        return 1.0 + (C::erx + p / q);
+    }
+    if (ix < 0x403c0000u) {  // |x| < 28
+        if (neg && ix >= 0x40180000u) return 2.0 - 1e-300;  // x <= -6
+        const double ax = fabs(x);
+        const double r = erf_tail_num(ax, ix < 0x4006DB6Du);
+        return neg ? 2.0 - r / ax : r / ax;
+    }
+    return neg ? 2.0 - 1e-300 : 1e-300 * 1e-300;
+}
+
+}  // namespace libm
+}  // namespace sidr

@@ -66,6 +66,7 @@ EXPORTS = [
     "sidr_kernel_launches", "sidr_rules_check", "sidr_last_transfer_bytes", "sidr_fp64_peak",
     "sidr_evaluate_static", "sidr_multi_create", "sidr_multi_autotune", "sidr_multi_set_shape",
     "sidr_multi_capture", "sidr_multi_run", "sidr_multi_read", "sidr_multi_destroy",
+    "sidr_libm_eval",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -191,6 +192,19 @@ def fp64_peak(device: int = 0, reps: int = 5) -> float:
     v = C.c_double()
     _check(load().sidr_fp64_peak(device, reps, C.byref(v)))
     return v.value
+
+
+LIBM_FUNCS = {"erf": 0, "erfc": 1, "exp": 2}
+
+
+def libm_eval(fn: str, x, device: int = 0) -> np.ndarray:
+    """The evaluator's device erf / erfc / exp on an array (diagnostic)."""
+    L = load()
+    L.sidr_libm_eval.argtypes = [C.c_int32, _dp, C.c_int64, C.c_int, _dp]
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros_like(a)
+    _check(L.sidr_libm_eval(LIBM_FUNCS[fn], _d(a), a.size, device, _d(out)))
+    return out
 
 
 STATIC_SCRATCH_BYTES = 16 << 20  # SIDR_STATIC_SCRATCH_BYTES

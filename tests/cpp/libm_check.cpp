@@ -1,0 +1,80 @@
+// Compares sidr::libm::{erf_, erfc_, exp_} (csrc/sidr_libm.cuh) with the host
+// C library bit for bit over random arguments in every interval of the
+// algorithms.  Usage: libm_check <samples per interval> <seed>; prints one line
+// per interval "name lo hi mismatches samples" and exits 1 on any mismatch.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "sidr_libm.cuh"
+
+namespace {
+
+uint64_t g_state = 88172645463325252ull;
+uint64_t next_u64() {
+    g_state ^= g_state << 13;
+    g_state ^= g_state >> 7;
+    g_state ^= g_state << 17;
+    return g_state;
+}
+double uniform(double a, double b) { return a + (b - a) * ((next_u64() >> 11) * 0x1p-53); }
+uint64_t bits(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return u;
+}
+
+struct Range {
+    const char* fn;
+    double lo, hi;
+};
+
+double ours(const char* fn, double x) {
+    if (fn[1] == 'x') return sidr::libm::exp_(x);
+    if (fn[3] == 'c') return sidr::libm::erfc_(x);
+    return sidr::libm::erf_(x);
+}
+double theirs(const char* fn, double x) {
+    if (fn[1] == 'x') return std::exp(x);
+    if (fn[3] == 'c') return std::erfc(x);
+    return std::erf(x);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    const long n = argc > 1 ? std::atol(argv[1]) : 1000000;
+    if (argc > 2) g_state ^= (uint64_t)std::atoll(argv[2]) * 0x9e3779b97f4a7c15ull;
+    const Range ranges[] = {
+        {"erf", -0x1p-1020, 0x1p-1020}, {"erf", -0x1p-27, 0x1p-27}, {"erf", -0.84375, 0.84375},
+        {"erf", 0.84375, 1.25},         {"erf", -1.25, -0.84375},   {"erf", 1.25, 2.857142857142857},
+        {"erf", 2.857142857142857, 6.0}, {"erf", -6.0, -1.25},      {"erf", -9.0, 9.0},
+        {"erfc", -0x1p-55, 0x1p-55},    {"erfc", -0.25, 0.25},      {"erfc", 0.25, 0.84375},
+        {"erfc", -0.84375, -0.25},      {"erfc", 0.84375, 1.25},    {"erfc", -1.25, -0.84375},
+        {"erfc", 1.25, 2.857142857142857}, {"erfc", 2.857142857142857, 6.0}, {"erfc", 6.0, 28.0},
+        {"erfc", -6.5, -1.25},          {"erfc", 26.0, 30.0},       {"erfc", -40.0, 40.0},
+        {"exp", -0x1p-50, 0x1p-50},     {"exp", -1.0, 1.0},         {"exp", -40.0, 1.0},
+        {"exp", -745.5, -512.0},        {"exp", 512.0, 709.7},      {"exp", -800.0, 800.0},
+    };
+    int bad_total = 0;
+    for (const Range& r : ranges) {
+        long bad = 0;
+        for (long k = 0; k < n; k++) {
+            const double x = uniform(r.lo, r.hi);
+            const double a = ours(r.fn, x), b = theirs(r.fn, x);
+            if (bits(a) != bits(b)) {
+                if (bad < 2) std::printf("# %s(%a): ours %a libc %a\n", r.fn, x, a, b);
+                bad++;
+            }
+        }
+        const double special[] = {0.0, -0.0, 1.0, -1.0, 0.84375, 1.25, 6.0, -6.0, 28.0, 0x1p-1074,
+                                  INFINITY, -INFINITY};
+        for (double x : special)
+            if (bits(ours(r.fn, x)) != bits(theirs(r.fn, x))) bad++;
+        std::printf("%s %a %a %ld %ld\n", r.fn, r.lo, r.hi, bad, n);
+        bad_total += bad != 0;
+    }
+    return bad_total ? 1 : 0;
+}

@@ -92,6 +92,8 @@ struct HostPrograms {
 
 }  // namespace
 
+void sidr::set_last_error(const std::string& msg) { g_err = msg; }
+
 struct sidr_ctx {
     int device = 0;
     int sm_count = 0;

@@ -57,4 +57,8 @@ std::string compile_rule(const int32_t* ops, const int32_t* args, int len, const
 // under 30 or 34; every other slot under its own flag.
 bool slot_active(int slot, const int64_t* mask);
 
+// Sets the text sidr_last_error() returns on this thread (the host drivers'
+// failures share the C-ABI's error slot).
+void set_last_error(const std::string& msg);
+
 }  // namespace sidr

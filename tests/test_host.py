@@ -23,9 +23,18 @@ def bits(a):
 
 # ------------------------------------------------------------ the C-ABI .so
 
+HEADERS = ("sidr.h", "sidr_gp.h", "sidr_campaign.h")
+
+
 def header_symbols():
-    text = open(os.path.join(REPO, "include", "sidr.h")).read()
+    text = "".join(open(os.path.join(REPO, "include", h)).read() for h in HEADERS)
     return sorted(set(re.findall(r"\b(sidr_[a-z0-9_]+)\s*\(", text)))
+
+
+def all_structs():
+    from sidr import campaign, gp
+    return {**sidr.STRUCTS, "sidr_gp_config": gp._Cfg, "sidr_gp_result": gp._Result,
+            **campaign.STRUCTS}
 
 
 def test_library_exports_every_declared_symbol():
@@ -42,8 +51,9 @@ def test_ctypes_structs_match_header(tmp_path):
     mismatch lets the library write past a Python-owned buffer)."""
     import ctypes
     import subprocess
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "sidr.h"', "int main(void){"]
-    for cname, py in sidr.STRUCTS.items():
+    lines = ['#include <stdio.h>', '#include <stddef.h>'] + [f'#include "{h}"' for h in HEADERS]
+    lines.append("int main(void){")
+    for cname, py in all_structs().items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for f, _ in py._fields_:
             lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
@@ -58,7 +68,7 @@ def test_ctypes_structs_match_header(tmp_path):
         if ln:
             a, b, c = ln.split()
             got[(a, b)] = int(c)
-    for cname, py in sidr.STRUCTS.items():
+    for cname, py in all_structs().items():
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)

@@ -258,3 +258,40 @@ def _ref_gp_replay(self, terminals, with_rmod, seed, pop, fits):
 
 
 Reference.gp_replay = _ref_gp_replay
+
+
+REF_GPU_SO = os.path.join(HERE, "_ref", "libsidr_ref_gpu.so")
+
+
+class ReferenceGPU:
+    """The reference's own GPU evaluator (engine/factory.cuh) as its Makefile
+    builds it (oracle/_ref/libsidr_ref_gpu.so): used to show where that build
+    and the CPU simulator differ.  Needs a CUDA device."""
+
+    def __init__(self):
+        if not os.path.exists(REF_GPU_SO):
+            raise FileNotFoundError(REF_GPU_SO)
+        self.lib = C.CDLL(REF_GPU_SO)
+        self.lib.ref_gpu_evaluate_grouped_masks.argtypes = (
+            [C.c_int, C.c_int, C.c_double] + [_dp] * 7 + [_ip] * 4 +
+            [C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _lp, _dp])
+
+    def evaluate_grouped_masks(self, sd, zp, rules, grouped, G, T, group_size, mask_group,
+                               masks):
+        keep = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                (sd.scores, sd.durations, sd.open_t, sd.close_t, sd.dist, sd.dist_to_depot, zp,
+                 grouped)]
+        ints = [np.ascontiguousarray(a, dtype=np.int32) for a in
+                (rules.ops, rules.args, rules.offsets, rules.lengths)]
+        mk = np.ascontiguousarray(masks, dtype=np.int64).reshape(-1)
+        out = np.zeros((rules.P, T))
+        st = self.lib.ref_gpu_evaluate_grouped_masks(
+            sd.n, sd.m, sd.tmax, *[_d(a) for a in keep[:7]], *[a.ctypes.data_as(_ip) for a in ints],
+            rules.P, _d(keep[7]), G, T, group_size, mask_group, mk.ctypes.data_as(_lp), _d(out))
+        if st != 0:
+            raise ValueError("input outside the reference kernel's bounds")
+        return out
+
+    def evaluate(self, sd, zp, rules, sampled, N, mask):
+        return self.evaluate_grouped_masks(sd, zp, rules, sampled, 1, N, max(rules.P, 1),
+                                           max(rules.P, 1), mask)

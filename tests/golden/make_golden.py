@@ -12,9 +12,18 @@ Reads (never copies) the reference tree:
   verify/golden/durations.txt  duration sampling, 3 instances x 3 base seeds x 5
   verify/golden/compile.txt    46 rules with their post-order ops/args
   instances/{solomon,cordeau}  the benchmark instances those cases run on
+  results/ga40/results/trace_<inst>_Sga.json
+                               the campaign's generation traces (c101, r101,
+                               rc101, pr01): per-generation bests and the 30
+                               finals with their held-out gains
+  results/baseline/cap2-results.csv
+                               the NS-GP mean-30 (km) the gains are taken over
+  results/ga40/logs/c101_search.log
+                               the vocabulary GA's stdout on c101 (the lines
+                               up to the third generation, timings dropped)
 
 and writes them as numpy archives (doubles kept bit-exact):
-  sim_cases.npz, gp_cases.npz, durations.npz, compile.npz.
+  sim_cases.npz, gp_cases.npz, durations.npz, compile.npz, campaign.npz.
 Rules are compiled here by sidr.rules.compile_rule; the compile fixture pins
 that compiler against the reference's own compile_rmod output.
 """
@@ -168,12 +177,50 @@ def make_compile(ref: str) -> dict:
     return out
 
 
+CAMPAIGN_INSTANCES = ("c101", "r101", "rc101", "pr01")
+
+
+def baseline_km(ref: str, name: str) -> float:
+    import csv
+    with open(os.path.join(ref, "results", "baseline", "cap2-results.csv")) as f:
+        for row in csv.DictReader(f):
+            if row["instance"] == name:
+                return float(row["baseline_nsgp_mean30"])
+    raise KeyError(name)
+
+
+def make_campaign(ref: str) -> dict:
+    out = {}
+    for nm in CAMPAIGN_INSTANCES:
+        put_inst(out, nm, inst_arrays(ref, nm))
+        out[f"{nm}/km"] = np.array([baseline_km(ref, nm)])
+        with open(os.path.join(ref, "results", "ga40", "results", f"trace_{nm}_Sga.json")) as f:
+            out[f"{nm}/trace"] = np.array(f.read())
+    lines = []
+    with open(os.path.join(ref, "results", "ga40", "logs", "c101_search.log")) as f:
+        for line in f:
+            line = line.rstrip("\r\n")
+            if line.startswith("  batch "):
+                continue
+            lines.append(line)
+            if line.startswith("gen 2 "):
+                break
+    out["c101/search_head"] = np.array(lines)
+    out["instances"] = np.array(CAMPAIGN_INSTANCES)
+    return out
+
+
+MAKERS = {"sim_cases": make_sim, "gp_cases": make_gp, "durations": make_durations,
+          "compile": make_compile, "campaign": make_campaign}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", nargs="*", choices=sorted(MAKERS), help="regenerate these only")
     a = ap.parse_args()
-    for name, fn in (("sim_cases", make_sim), ("gp_cases", make_gp),
-                     ("durations", make_durations), ("compile", make_compile)):
+    for name in a.only or list(MAKERS):
+        fn = MAKERS[name]
         data = fn(a.ref)
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **data)

@@ -184,44 +184,65 @@ struct ErfCoef {
                             sb7 = -2.24409524465858183362e+01;
 };
 
-// PP(z)/QQ(z) for |x| < 0.84375, pairwise.
-SIDR_HD double erf_small_ratio(double z) {
-    using C = ErfCoef;
-    const double z2 = z * z, z4 = z2 * z2;
-    const double p = (C::pp0 + z * C::pp1) + z2 * (C::pp2 + z * C::pp3) + z4 * C::pp4;
-    const double q = (1.0 + z * C::qq1) + z2 * (C::qq2 + z * C::qq3) + z4 * (C::qq4 + z * C::qq5);
-    return p / q;
+// The four rational approximations share one evaluation: every numerator
+// and denominator above is a prefix of
+//   ((((c0 + t*c1) + t2*(c2 + t*c3)) + t4*(c4 + t*c5)) + t6*(c6 + t*c7)) + t8*(c8 + t*c9)
+// with t2 = t*t, t4 = t2*t2, t6 = t4*t2, t8 = t4*t4 (a trailing single term
+// such as z4*pp4 is t4*(c4 + t*0)); the missing coefficients are zero, and a
+// zero term adds +0, which changes no value, so the result is the same
+// double.  One code path for all intervals keeps the lanes of a warp together
+// when their arguments fall in different intervals.  Rows: small |x|, mid
+// |x|, tail with RA/SA, tail with RB/SB; in each row 10 numerator then 10
+// denominator coefficients.
+#define SIDR_ERF_ROWS                                                                             \
+    {ErfCoef::pp0, ErfCoef::pp1, ErfCoef::pp2, ErfCoef::pp3, ErfCoef::pp4, 0.0, 0.0, 0.0, 0.0, 0.0, \
+     1.0, ErfCoef::qq1, ErfCoef::qq2, ErfCoef::qq3, ErfCoef::qq4, ErfCoef::qq5, 0.0, 0.0, 0.0, 0.0, \
+     ErfCoef::pa0, ErfCoef::pa1, ErfCoef::pa2, ErfCoef::pa3, ErfCoef::pa4, ErfCoef::pa5,           \
+     ErfCoef::pa6, 0.0, 0.0, 0.0,                                                                 \
+     1.0, ErfCoef::qa1, ErfCoef::qa2, ErfCoef::qa3, ErfCoef::qa4, ErfCoef::qa5, ErfCoef::qa6,      \
+     0.0, 0.0, 0.0,                                                                               \
+     ErfCoef::ra0, ErfCoef::ra1, ErfCoef::ra2, ErfCoef::ra3, ErfCoef::ra4, ErfCoef::ra5,           \
+     ErfCoef::ra6, ErfCoef::ra7, 0.0, 0.0,                                                        \
+     1.0, ErfCoef::sa1, ErfCoef::sa2, ErfCoef::sa3, ErfCoef::sa4, ErfCoef::sa5, ErfCoef::sa6,      \
+     ErfCoef::sa7, ErfCoef::sa8, 0.0,                                                             \
+     ErfCoef::rb0, ErfCoef::rb1, ErfCoef::rb2, ErfCoef::rb3, ErfCoef::rb4, ErfCoef::rb5,           \
+     ErfCoef::rb6, 0.0, 0.0, 0.0,                                                                 \
+     1.0, ErfCoef::sb1, ErfCoef::sb2, ErfCoef::sb3, ErfCoef::sb4, ErfCoef::sb5, ErfCoef::sb6,      \
+     ErfCoef::sb7, 0.0, 0.0}
+
+#ifdef __CUDACC__
+__device__ const double kErfRowsDev[80] = SIDR_ERF_ROWS;
+#endif
+static const double kErfRowsHost[80] = SIDR_ERF_ROWS;
+
+SIDR_HD double erf_coef(int i) {
+#ifdef __CUDA_ARCH__
+    return kErfRowsDev[i];
+#else
+    return kErfRowsHost[i];
+#endif
 }
 
-// PA(s) and QA(s) for 0.84375 <= |x| < 1.25, pairwise.
-SIDR_HD void erf_mid_terms(double s, double& p, double& q) {
-    using C = ErfCoef;
-    const double s2 = s * s, s4 = s2 * s2, s6 = s4 * s2;
-    p = (C::pa0 + s * C::pa1) + s2 * (C::pa2 + s * C::pa3) + s4 * (C::pa4 + s * C::pa5) + s6 * C::pa6;
-    q = (1.0 + s * C::qa1) + s2 * (C::qa2 + s * C::qa3) + s4 * (C::qa4 + s * C::qa5) + s6 * C::qa6;
-}
-
-// The tail numerator for ax = |x| >= 1.25: exp(-z^2-0.5625) *
-// exp((z-ax)(z+ax)+R/S), z = ax with its low 32 bits cleared (so z*z is
-// exact); `near` selects the RA/SA set.
-SIDR_HD double erf_tail_num(double ax, bool near) {
-    using C = ErfCoef;
-    const double t = 1.0 / (ax * ax);
-    const double t2 = t * t, t4 = t2 * t2, t6 = t4 * t2;
-    double R, S;
-    if (near) {
-        const double t8 = t4 * t4;
-        R = (C::ra0 + t * C::ra1) + t2 * (C::ra2 + t * C::ra3) + t4 * (C::ra4 + t * C::ra5) +
-            t6 * (C::ra6 + t * C::ra7);
-        S = (1.0 + t * C::sa1) + t2 * (C::sa2 + t * C::sa3) + t4 * (C::sa4 + t * C::sa5) +
-            t6 * (C::sa6 + t * C::sa7) + t8 * C::sa8;
-    } else {
-        R = (C::rb0 + t * C::rb1) + t2 * (C::rb2 + t * C::rb3) + t4 * (C::rb4 + t * C::rb5) + t6 * C::rb6;
-        S = (1.0 + t * C::sb1) + t2 * (C::sb2 + t * C::sb3) + t4 * (C::sb4 + t * C::sb5) +
-            t6 * (C::sb6 + t * C::sb7);
+// Numerator / denominator of row `row` at t, both pairwise as above.
+SIDR_HD double erf_ratio(int row, double t) {
+    const int o = row * 20;
+    const double t2 = t * t, t4 = t2 * t2, t6 = t4 * t2, t8 = t4 * t4;
+    double pq[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int c = o + 10 * h;
+        pq[h] = (erf_coef(c) + t * erf_coef(c + 1)) + t2 * (erf_coef(c + 2) + t * erf_coef(c + 3)) +
+                t4 * (erf_coef(c + 4) + t * erf_coef(c + 5)) + t6 * (erf_coef(c + 6) + t * erf_coef(c + 7)) +
+                t8 * (erf_coef(c + 8) + t * erf_coef(c + 9));
     }
+    return pq[0] / pq[1];
+}
+
+// exp(-z^2-0.5625) * exp((z-ax)(z+ax) + rs), z = ax with its low 32 bits
+// cleared (so z*z is exact): x*erfc(x) for the tail rows.
+SIDR_HD double erf_tail(double ax, double rs) {
     const double z = double_of(bits_of(ax) & 0xffffffff00000000ull);
-    return exp_(-z * z - 0.5625) * exp_((z - ax) * (z + ax) + R / S);
+    return exp_(-z * z - 0.5625) * exp_((z - ax) * (z + ax) + rs);
 }
 
 SIDR_HD_CALL double erf_(double x) {
@@ -230,21 +251,18 @@ SIDR_HD_CALL double erf_(double x) {
     const bool neg = (u >> 63) != 0;
     const uint32_t ix = (uint32_t)(u >> 32) & 0x7fffffffu;  // high word of |x|
     if (ix >= 0x7ff00000u) return (neg ? -1.0 : 1.0) + 1.0 / x;  // nan, +-inf
-    if (ix < 0x3feb0000u) {                                      // |x| < 0.84375
-        if (ix < 0x3e300000u) {                                  // |x| < 2^-28
-            if (ix < 0x00800000u) return 0.0625 * (16.0 * x + (16.0 * C::efx) * x);
-            return x + C::efx * x;
-        }
-        return x + x * erf_small_ratio(x * x);
-    }
-    if (ix < 0x3ff40000u) {  // 0.84375 <= |x| < 1.25
-        double p, q;
-        erf_mid_terms(fabs(x) - 1.0, p, q);
-        return neg ? -C::erx - p / q : C::erx + p / q;
+    if (ix < 0x3e300000u) {                                      // |x| < 2^-28
+        if (ix < 0x00800000u) return 0.0625 * (16.0 * x + (16.0 * C::efx) * x);
+        return x + C::efx * x;
     }
     if (ix >= 0x40180000u) return neg ? 1e-300 - 1.0 : 1.0 - 1e-300;  // |x| >= 6
     const double ax = fabs(x);
-    const double r = erf_tail_num(ax, ix < 0x4006DB6Eu);
+    const int row = ix < 0x3feb0000u ? 0 : ix < 0x3ff40000u ? 1 : ix < 0x4006DB6Eu ? 2 : 3;
+    const double t = row == 0 ? x * x : row == 1 ? ax - 1.0 : 1.0 / (ax * ax);
+    const double pq = erf_ratio(row, t);
+    if (row == 0) return x + x * pq;                              // |x| < 0.84375
+    if (row == 1) return neg ? -C::erx - pq : C::erx + pq;        // |x| < 1.25
+    const double r = erf_tail(ax, pq);                            // |x| < 6
     return neg ? r / ax - 1.0 : 1.0 - r / ax;
 }
 
@@ -255,27 +273,22 @@ SIDR_HD_CALL double erfc_(double x) {
     const uint32_t hx = (uint32_t)(u >> 32);
     const uint32_t ix = hx & 0x7fffffffu;
     if (ix >= 0x7ff00000u) return (double)(neg ? 2 : 0) + 1.0 / x;  // nan, +-inf
-    if (ix < 0x3feb0000u) {                                         // |x| < 0.84375
-        if (ix < 0x3c700000u) return 1.0 - x;                       // |x| < 2^-56
-        const double y = erf_small_ratio(x * x);
-        if ((int32_t)hx < 0x3fd00000) return 1.0 - (x + x * y);  // x < 1/4
-        double r = x * y;
+    if (ix < 0x3c700000u) return 1.0 - x;                           // |x| < 2^-56
+    if (ix >= 0x403c0000u) return neg ? 2.0 - 1e-300 : 1e-300 * 1e-300;  // |x| >= 28
+    if (neg && ix >= 0x40180000u) return 2.0 - 1e-300;                // x <= -6
+    const double ax = fabs(x);
+    const int row = ix < 0x3feb0000u ? 0 : ix < 0x3ff40000u ? 1 : ix < 0x4006DB6Du ? 2 : 3;
+    const double t = row == 0 ? x * x : row == 1 ? ax - 1.0 : 1.0 / (ax * ax);
+    const double pq = erf_ratio(row, t);
+    if (row == 0) {  // |x| < 0.84375
+        if ((int32_t)hx < 0x3fd00000) return 1.0 - (x + x * pq);  // x < 1/4
+        double r = x * pq;
         r += (x - 0.5);
         return 0.5 - r;
     }
-    if (ix < 0x3ff40000u) {  // 0.84375 <= |x| < 1.25
-        double p, q;
-        erf_mid_terms(fabs(x) - 1.0, p, q);
-        if (!neg) return (1.0 - C::erx) - p / q;
-        return 1.0 + (C::erx + p / q);
-    }
-    if (ix < 0x403c0000u) {  // |x| < 28
-        if (neg && ix >= 0x40180000u) return 2.0 - 1e-300;  // x <= -6
-        const double ax = fabs(x);
-        const double r = erf_tail_num(ax, ix < 0x4006DB6Du);
-        return neg ? 2.0 - r / ax : r / ax;
-    }
-    return neg ? 2.0 - 1e-300 : 1e-300 * 1e-300;
+    if (row == 1) return neg ? 1.0 + (C::erx + pq) : (1.0 - C::erx) - pq;  // |x| < 1.25
+    const double r = erf_tail(ax, pq);                                     // |x| < 28
+    return neg ? 2.0 - r / ax : r / ax;
 }
 
 }  // namespace libm

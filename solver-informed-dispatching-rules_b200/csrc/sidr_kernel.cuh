@@ -450,22 +450,21 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
 
     SIDR_SEC_ADD(2, t_setup);
     SIDR_SEC_MARK(t_fused)
-    const uint32_t fused = kNeedNSFused | kNeedRegret | kNeedRob | kNeedAfterC | kNeedAtRisk;
+    const uint32_t fused = kNeedNSFused | kNeedRegret | kNeedRob | kNeedAfterC;
     if (need & fused) {
         // neighbour-major pairs of origin i+1: {F, R} and {G, dist} at j*ld + i+1
         const double2* FRi = reinterpret_cast<const double2*>(I.FR) + (i + 1);
         const double2* GDi = reinterpret_cast<const double2*>(I.GD) + (i + 1);
         const bool need_gd =
-            (need & (kNeedRob | kNeedNSTW | kNeedStruct | kNeedPBust | kNeedAtRisk)) != 0;
-        const double* P1i = I.P1T + i;
+            (need & (kNeedRob | kNeedNSTW | kNeedStruct | kNeedPBust)) != 0;
         const uint32_t* zlti = I.zlt + (size_t)(i + 1) * I.nw;
         const uint32_t* zlei = I.zle + (size_t)(i + 1) * I.nw;
-        unsigned long long scan = 0, heavy = 0;
+        unsigned long long scan = 0;
 
         // One neighbour j (bit b of its word): every accumulator is updated in
         // ascending j, as each reference loop runs.
         auto visit = [&](int j, int b, double2 fr, double2 gd, uint32_t zl, uint32_t ze,
-                         uint32_t nowb, uint32_t atb) {
+                         uint32_t nowb) {
             if (COUNT) scan++;
             const double Fj = fr.x, Rj = fr.y;
             const double sj = I.scores[j];
@@ -528,49 +527,6 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     }
                 }
             }
-            if (need & kNeedAtRisk) {
-                if ((atb >> b) & 1u) {
-                    if (COUNT) heavy++;
-                    const double cj = I.close_t[j], oj = I.open_t[j];
-                    const double marr = fin_c + gd.y;
-                    // norm_cdf(d/s) = 0.5*(1 + erf((d/s)*0.7071067811865476)).  The
-                    // reference's erf (glibc) is exactly +-1 for |x| >= 6, so for
-                    // |d| >= 8.5 s (x >= 6.01 after both roundings) the result is 1
-                    // or 0 with no erf call.
-                    double pw;
-                    const double dw = cj - marr;
-                    if (sd_c > 1e-9) {
-                        if (dw >= 8.5 * sd_c) pw = 1.0;
-                        else if (dw <= -8.5 * sd_c) pw = 0.0;
-                        else pw = 0.5 * (1.0 + libm::erf_((dw / sd_c) * 0.7071067811865476));
-                    } else {
-                        pw = marr <= cj ? 1.0 : 0.0;
-                    }
-                    if (pw == 0.0) {
-                        eloss += sj * 1.0;  // sj * (1.0 - 0.0 * p_bud), p_bud finite
-                    } else {
-                        double mst, pv;
-                        if (marr > oj) {
-                            mst = marr;
-                            pv = P1i[(size_t)j * n];
-                        } else {
-                            mst = oj;
-                            pv = I.P0[j];
-                        }
-                        const double mb = mst + I.durations[j] + I.d2d[j];
-                        double pb;
-                        if (pv >= 0.0) {
-                            const double db = tmax - mb;
-                            if (db >= 8.5 * pv) pb = 1.0;
-                            else if (db <= -8.5 * pv) pb = 0.0;
-                            else pb = 0.5 * (1.0 + libm::erf_((db / pv) * 0.7071067811865476));
-                        } else {
-                            pb = mb <= tmax ? 1.0 : 0.0;
-                        }
-                        eloss += sj * (1.0 - pw * pb);
-                    }
-                }
-            }
         };
 
         for (int w = 0; w < I.nw; w++) {
@@ -578,7 +534,6 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
             if (!bits) continue;
             const uint32_t zl = zlti[w], ze = zlei[w];
             const uint32_t nowb = S.feas[w];
-            const uint32_t atb = S.atr[w];
             // two neighbours per iteration, both loads issued before either visit
             while (bits) {
                 const int b0 = __ffs(bits) - 1;
@@ -594,14 +549,74 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
                     gd0 = GDi[(size_t)j0 * ld];
                     gd1 = GDi[(size_t)j1 * ld];
                 }
-                visit(j0, b0, fr0, gd0, zl, ze, nowb, atb);
-                if (has1) visit(j1, b1, fr1, gd1, zl, ze, nowb, atb);
+                visit(j0, b0, fr0, gd0, zl, ze, nowb);
+                if (has1) visit(j1, b1, fr1, gd1, zl, ze, nowb);
             }
         }
         if (COUNT) {
             wc.scan += scan;
+            wc.ops += scan * rm.scan_ops;
+        }
+    }
+
+    // ATRISK (engine/sim_terms.hpp:225-257) in its own ascending pass over the
+    // customers reachable before their close: its erf calls run outside the
+    // register-heavy fused scan.
+    if (need & kNeedAtRisk) {
+        const double2* GDa = reinterpret_cast<const double2*>(I.GD) + (i + 1);
+        const double* P1i = I.P1T + i;
+        unsigned long long heavy = 0;
+        for (int w = 0; w < I.nw; w++) {
+            uint32_t bits = S.atr[w] & ~bit_in_word(i, w);
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const int j = (w << 5) + b;
+                const double sj = I.scores[j];
+                if (COUNT) heavy++;
+                const double cj = I.close_t[j], oj = I.open_t[j];
+                const double marr = fin_c + GDa[(size_t)j * ld].y;
+                // norm_cdf(d/s) = 0.5*(1 + erf((d/s)*0.7071067811865476)).  The
+                // reference's erf (glibc) is exactly +-1 for |x| >= 6, so for
+                // |d| >= 8.5 s (x >= 6.01 after both roundings) the result is 1
+                // or 0 with no erf call.
+                double pw;
+                const double dw = cj - marr;
+                if (sd_c > 1e-9) {
+                    if (dw >= 8.5 * sd_c) pw = 1.0;
+                    else if (dw <= -8.5 * sd_c) pw = 0.0;
+                    else pw = 0.5 * (1.0 + libm::erf_((dw / sd_c) * 0.7071067811865476));
+                } else {
+                    pw = marr <= cj ? 1.0 : 0.0;
+                }
+                if (pw == 0.0) {
+                    eloss += sj * 1.0;  // sj * (1.0 - 0.0 * p_bud), p_bud finite
+                } else {
+                    double mst, pv;
+                    if (marr > oj) {
+                        mst = marr;
+                        pv = P1i[(size_t)j * n];
+                    } else {
+                        mst = oj;
+                        pv = I.P0[j];
+                    }
+                    const double mb = mst + I.durations[j] + I.d2d[j];
+                    double pb;
+                    if (pv >= 0.0) {
+                        const double db = tmax - mb;
+                        if (db >= 8.5 * pv) pb = 1.0;
+                        else if (db <= -8.5 * pv) pb = 0.0;
+                        else pb = 0.5 * (1.0 + libm::erf_((db / pv) * 0.7071067811865476));
+                    } else {
+                        pb = mb <= tmax ? 1.0 : 0.0;
+                    }
+                    eloss += sj * (1.0 - pw * pb);
+                }
+            }
+        }
+        if (COUNT) {
             wc.heavy += heavy;
-            wc.ops += scan * rm.scan_ops + heavy * kOpsAtRisk;
+            wc.ops += heavy * kOpsAtRisk;
         }
     }
 

@@ -233,16 +233,28 @@ def run_reference(args, rank, world):
 # ------------------------------------------------------------------ ours
 
 def profile_traffic():
-    """Per-launch DRAM traffic of the evaluator kernel from the committed ncu
-    summary (profiles/), scaled to this workload; None when absent."""
-    p = os.path.join(REPO, "profiles", "eval_kernel_traffic.json")
+    """Per-launch DRAM bytes (read + write) of the evaluator kernel on this
+    workload, from the committed ncu summary
+    profiles/eval_kernel_gp_generation_traffic.md (its "bytes_per_launch:"
+    line); None when absent."""
+    p = os.path.join(REPO, "profiles", "eval_kernel_gp_generation_traffic.md")
     if not os.path.exists(p):
         return None
+    with open(p) as f:
+        for line in f:
+            if line.startswith("bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+def measured_hbm_gbs():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
         with open(p) as f:
-            return json.load(f).get("bytes_per_launch")
+            d = json.load(f)
+        return float(d.get("hbm_gbs")), "measured (MEASURED_PEAKS.json)"
     except Exception:
-        return None
+        return 6650.0, "fallback"
 
 
 def run_ours(args, rank, world, local):
@@ -344,11 +356,18 @@ def run_ours(args, rank, world, local):
                 "peak_source": "measured on this GPU by sidr_fp64_peak (DFMA chains over all SMs)",
                 "op_model": "sidr_counts.fp64_ops (include/sidr.h)"}
 
+    hbm_peak, hbm_src = measured_hbm_gbs()
+    hbm = None
+    if traffic is not None:
+        hbm = {"achieved": traffic / avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+               "frac": traffic / avg_s / 1e9 / hbm_peak, "peak_source": hbm_src,
+               "traffic_bytes_per_launch": traffic}
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_of(args.P, args.S, world),
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "hbm": hbm, "clocks": clk,
             "counts": counts, "repeat_runs_identical": same}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, zp, args.cpu_seconds, gpu_out=ref_out)

@@ -65,6 +65,11 @@ def parse_args():
     ap.add_argument("--multi", action="store_true",
                     help="also time the uneven multi-instance batch (40 instances of 25-288 "
                          "customers) in one autotuned, graph-captured launch")
+    ap.add_argument("--campaign", action="store_true",
+                    help="also time the reference campaign's c101 generation trace (30 seeds x "
+                         "1024 rules x 51 generations + held-out) and its vocabulary GA's first "
+                         "batch (13 genomes x 16 seeds x 51 generations), both checked against "
+                         "the reference's own artefacts in tests/golden/campaign.npz")
     ap.add_argument("--multi-rules", type=int, default=100)
     ap.add_argument("--multi-S", type=int, default=100)
     return ap.parse_args()
@@ -375,6 +380,8 @@ def run_ours(args, rank, world, local):
         line["gp"] = gp_leg(ctx, w, args)
     if args.multi and rank == 0:
         line["multi"] = multi_leg(args, stream)
+    if args.campaign and rank == 0:
+        line["campaign"] = campaign_leg()
     batch.close()
     ctx.close()
     if dist:
@@ -413,6 +420,49 @@ def multi_leg(args, stream):
             "evaluations": P * mw.S, "seconds": t, "evals_per_s": P * mw.S / t,
             "shapes_ms": ms, "chosen_shape": list(sidr.Multi.SHAPES[chosen]),
             "host_prep_seconds": prep}
+
+
+def campaign_leg():
+    """The reference campaign's c101 workloads on the evaluator: the generation
+    trace of s3_generation/gen_trace.cu (compared with the reference's trace
+    file seed by seed) and the first batch_score call of s4_selection/ga.cu's
+    search (13 genomes of the 18-terminal universe x 16 seeds x 51 generations
+    + the 64-scenario TRAIN block; its proxies give the search log's 'gen 0'
+    line only with the next batches, so here they are timed)."""
+    import numpy as np
+    import sidr
+    from sidr import campaign
+    from sidr import rules as R
+    from sidr.instance import SimData
+    z = np.load(os.path.join(REPO, "tests", "golden", "campaign.npz"))
+    sd = SimData.from_arrays(*[z[f"c101/inst_{k}"] for k in
+                               ("x", "y", "score", "open", "close", "dur", "tmax")], m=3)
+    km = float(z["c101/km"][0])
+    expected = json.loads(str(z["c101/trace"]))
+    ctx = sidr.Context(sd, sidr.zstats(sd))
+    t0 = time.perf_counter()
+    text, _ = campaign.gen_trace(ctx, "c101", expected["vocab_extra"], km, n_seeds=30)
+    t_trace = time.perf_counter() - t0
+    got = json.loads(text)
+    same = sum(1 for s in range(30) if got["trace"][s] == expected["trace"][s]
+               and got["finals"][s] == expected["finals"][s])
+    trace_evals = 30 * 1024 * 52 + 30 * 500
+    # the search's first batch: genomes 0 and the 18 singletons sorted, first 13
+    genomes = sorted([0] + [1 << b for b in range(18)])[:13]
+    t0 = time.perf_counter()
+    _, res = campaign.batch_score(ctx, R.EXTRA, genomes, 16, 51, bmax=13)
+    t_batch = time.perf_counter() - t0
+    ctx.close()
+    return {"trace": {"workload": "c101 gen_trace: 30 seeds x 1024 rules x 51 generations + "
+                                  "30 x 500 held-out, 17 terminals",
+                      "wall_seconds": t_trace, "evaluations": trace_evals,
+                      "evals_per_s": trace_evals / t_trace,
+                      "seeds_identical_to_reference_trace": same},
+            "ga_batch": {"workload": "c101 batch_score: 13 genomes x 16 seeds x 1024 rules x 51 "
+                                     "generations + 64-scenario TRAIN block",
+                         "wall_seconds": t_batch, "eval_seconds": res.eval_seconds,
+                         "host_seconds": res.host_seconds, "evaluations": res.evaluations,
+                         "evals_per_s": res.evaluations / t_batch}}
 
 
 def gp_leg(ctx, w, args):

@@ -27,6 +27,34 @@ extern "C" {
 #define SIDR_MLP_INPUTS 40
 #define SIDR_MLP_HIDDEN 256
 
+/* Decision situations: `rule` (one rule, P = 1) rolled out on S scenarios
+ * (sampled [S][n]) under `mask` by the evaluator, recording its first
+ * max_decisions decisions of every rollout: for decision d of scenario s and
+ * candidate c < max_cand (candidates in ascending customer order),
+ * terms[((s*max_decisions + d)*max_cand + c)*61 + slot] holds the candidate's
+ * 61-slot terminal table as pick_best fills it (engine/sim_core.hpp:84-197:
+ * every slot active under the mask; inactive slots 0), cust[...] (may be
+ * NULL) its customer index, and info[(s*max_decisions + d)*2] = {candidate
+ * count, chosen customer or -1}; a rollout's unused decision entries have
+ * candidate count 0. */
+sidr_status sidr_capture_situations(sidr_ctx* ctx, const sidr_rules_desc* rule, const double* sampled,
+                                    int32_t S, const int64_t* mask, int32_t max_decisions,
+                                    int32_t max_cand, double* terms, int32_t* cust, int32_t* info);
+
+/* Phenotype features of P rules over n_sit situations (terms
+ * [n_sit][max_cand][61], ncand[n_sit] candidates each, ref[n_sit] = the
+ * position of a reference choice among them): for situation j the rule's
+ * priorities (eval_tree, engine/sim_core.hpp:11-41, NaN -> -1e300) rank the
+ * candidates as pick_best does (strict >, lower position first on ties), and
+ * feature j is the reference choice's place in that ranking / (ncand - 1).
+ * Then 8 token-count features: length/255, depth/16, leaves/128, distinct
+ * slots/32, constants/32, and the shares of +/-, * and /, and min/max/rmod
+ * among the operators.  features[P][n_sit + 8]; n_sit = 32 gives the model's
+ * 40 inputs. */
+sidr_status sidr_phenotype(const sidr_rules_desc* rules, const double* terms, const int32_t* ncand,
+                           const int32_t* ref, int32_t n_sit, int32_t max_cand, int device,
+                           float* features);
+
 /* C[M x N] (FP32) = A[M x K] * B[N x K]^T with BF16 operands given as raw
  * 16-bit patterns, on the tensor-core kernel the model uses (diagnostic).
  * splits > 1 splits K over CTAs that accumulate atomically.  N <= 256. */
@@ -58,6 +86,52 @@ sidr_status sidr_mlp_gradients(sidr_mlp* m, const float* x, const float* t, int3
  * without replacement from (x[n][40], t[n]), reshuffled every pass. */
 sidr_status sidr_mlp_train(sidr_mlp* m, const float* x, const float* t, int32_t n, int32_t steps,
                            int32_t batch, float lr, uint64_t seed, float* final_loss);
+
+/* The surrogate-assisted GP's settings (defaults in brackets). */
+typedef struct sidr_sgp_config {
+    int32_t screen;            /* [8192] offspring bred and screened per generation */
+    int32_t train_steps;       /* [200] Adam steps per generation */
+    int32_t batch;             /* [1024] rows per step */
+    float lr;                  /* [1e-3] */
+    int32_t audit;             /* [128] screened offspring also simulated for the audit */
+    double rho_min;            /* [0.8] audit Spearman rho below which the generation breeds plainly */
+    int32_t history;           /* [3] generations of simulated fitness the model trains on */
+    int32_t n_situations;      /* [32] decision situations of the phenotype (n_situations + 8 = 40) */
+    int32_t capture_scenarios; /* [16] rollouts of the first generation's best rule they are sampled from */
+    int32_t max_cand;          /* [64] candidates kept per situation */
+    uint64_t model_seed;       /* [1] */
+    int32_t use_surrogate;     /* [1] 0: the same driver with plain breeding (the comparison run) */
+    int32_t device;            /* [0] device of the model and of the phenotype kernel */
+} sidr_sgp_config;
+
+void sidr_sgp_default_config(sidr_sgp_config* cfg);
+
+typedef struct sidr_sgp_result {
+    double eval_seconds;   /* in the evaluator (population, audit, held-out, capture) */
+    double model_seconds;  /* phenotypes, training, prediction */
+    double host_seconds;   /* the rest: breeding, compiling, bookkeeping */
+    int64_t evaluations;
+    int32_t generations_screened, generations_fallback;
+} sidr_sgp_result;
+
+/* A GP run (engine/gp.hpp semantics, Mt19937(seed), train blocks of
+ * cfg->train_samples scenarios from base seed seed*10000+gen) whose
+ * offspring are pre-screened: each generation the model is trained on the
+ * last `history` generations' simulated fitness (standardised), `screen`
+ * offspring are bred by gp_step's loop, their phenotypes predicted, `audit`
+ * of them simulated for Spearman's rho; at rho >= rho_min the next
+ * population is the elites plus the best-predicted offspring, otherwise
+ * plain gp_step.  The decision situations come from the first generation's
+ * best rule.  Every fitness reported is simulated.  Per generation g:
+ * best_train[g], held_out[g] (the generation's best rule on test_samples
+ * scenarios from test_seed), rho[g] (NaN when not audited), gen_seconds[g]
+ * (wall clock since the start); best_rule: the last generation's best rule
+ * as prefix text. */
+sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
+                         const sidr_sgp_config* sc, const char* terminals_csv, const int64_t* mask,
+                         uint64_t seed, int64_t test_seed, double* best_train, double* held_out,
+                         double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
+                         sidr_sgp_result* result);
 
 #ifdef __cplusplus
 }

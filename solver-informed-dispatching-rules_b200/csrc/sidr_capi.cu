@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/sidr.h"
+#include "../../include/sidr_surrogate.h"
 #include "sidr_host.hpp"
 #include "sidr_kernel.cuh"
 
@@ -135,7 +136,7 @@ sidr_status check_rules(const sidr_rules_desc* r) {
 // Compile every rule under its mask row: row p/mask_group, or row_of[p] when
 // given (multi-instance batches, where it is also the rule's instance).
 sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask_group,
-                        HostPrograms& hp, const int32_t* row_of = nullptr) {
+                        HostPrograms& hp, const int32_t* row_of = nullptr, bool all_active_rows = false) {
     hp = HostPrograms();
     hp.meta.resize(r->P);
     CompiledRule cr;
@@ -143,7 +144,7 @@ sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask
         const int row = row_of ? row_of[p] : p / mask_group;
         const int64_t* M = masks + (size_t)row * kTerms;
         std::string e = compile_rule(r->ops + r->offsets[p], r->args + 2 * (size_t)r->offsets[p],
-                                     r->lengths[p], M, cr);
+                                     r->lengths[p], M, cr, all_active_rows);
         if (!e.empty()) {
             const sidr_status s = (e.find("MAX_") != std::string::npos) ? SIDR_ERR_TOO_LARGE
                                                                         : SIDR_ERR_RULE;
@@ -380,6 +381,95 @@ sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s) {
     // each fused multiply-add is one instruction of the FP64 pipe = one op here
     const double ops = (double)blocks * threads * iters * 8.0;
     *ops_per_s = ops / (best * 1e-3);
+    return SIDR_OK;
+}
+
+sidr_status sidr_capture_situations(sidr_ctx* c, const sidr_rules_desc* r, const double* sampled,
+                                    int32_t S, const int64_t* mask, int32_t max_decisions,
+                                    int32_t max_cand, double* terms, int32_t* cust, int32_t* info) {
+    if (!c || !r || !mask || !sampled || !terms || !info) return fail(SIDR_ERR_INVALID, "null argument");
+    if (r->P != 1) return fail(SIDR_ERR_INVALID, "capture takes exactly one rule");
+    if (S < 1 || max_decisions < 1 || max_cand < 1) return fail(SIDR_ERR_INVALID, "S, max_decisions, max_cand >= 1");
+    sidr_status s = check_rules(r);
+    if (s) return s;
+    const size_t n_smp = (size_t)S * c->h.n;
+    if ((s = check_finite(sampled, n_smp))) return s;
+    HostPrograms hp;
+    if ((s = compile_all(r, mask, 1, hp, nullptr, true))) return s;
+    const int K = hp.meta[0].K;
+    std::vector<int> slot_of(hp.slots.begin(), hp.slots.begin() + K);  // row -> slot
+    SIDR_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    SIDR_CUDA(upload(c->prog, hp.prog, st));
+    SIDR_CUDA(upload(c->consts, hp.consts, st));
+    SIDR_CUDA(upload(c->slots, hp.slots, st));
+    SIDR_CUDA(upload(c->meta, hp.meta, st));
+    SIDR_CUDA(c->sampled.ensure(n_smp * sizeof(double)));
+    SIDR_CUDA(cudaMemcpyAsync(c->sampled.p, sampled, n_smp * sizeof(double), cudaMemcpyHostToDevice, st));
+    SIDR_CUDA(c->out.ensure((size_t)S * sizeof(double)));
+    SIDR_CUDA(c->counter.ensure(sizeof(unsigned long long)));
+    SIDR_CUDA(c->error.ensure(sizeof(int)));
+    SIDR_CUDA(cudaMemsetAsync(c->error.p, 0, sizeof(int), st));
+    const size_t slots_n = (size_t)S * max_decisions, cand_n = slots_n * max_cand;
+    double* d_rows = nullptr;
+    int32_t *d_cust = nullptr, *d_info = nullptr;
+    cudaError_t e = cudaMalloc(&d_rows, cand_n * K * sizeof(double));
+    if (!e) e = cudaMalloc(&d_cust, cand_n * sizeof(int32_t));
+    if (!e) e = cudaMalloc(&d_info, slots_n * 2 * sizeof(int32_t));
+    if (!e) e = cudaMemsetAsync(d_info, 0, slots_n * 2 * sizeof(int32_t), st);
+    if (!e) e = cudaMemsetAsync(c->counter.p, 0, sizeof(unsigned long long), st);
+    DevBatch b{};
+    b.P = 1;
+    b.T = S;
+    b.group_size = 1;
+    b.n = c->h.n;
+    b.prog = (const uint32_t*)c->prog.p;
+    b.consts = (const double*)c->consts.p;
+    b.slots = (const uint8_t*)c->slots.p;
+    b.meta = (const RuleMeta*)c->meta.p;
+    b.sampled = (const double*)c->sampled.p;
+    b.out = (double*)c->out.p;
+    b.counter = (unsigned long long*)c->counter.p;
+    b.error = (int*)c->error.p;
+    b.rows = hp.rows;
+    b.prog_cap = hp.prog_cap;
+    b.const_cap = hp.const_cap;
+    CaptureBuf cb{d_rows, d_cust, d_info, max_decisions, max_cand, K};
+    const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
+    const int wpb = SIDR_WARPS_PER_BLOCK;
+    const size_t smem = slice * wpb;
+    if (!e && smem > c->smem_optin) e = cudaErrorInvalidValue;
+    if (!e) e = cudaFuncSetAttribute(capture_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (!e) {
+        const int grid = std::max(1, std::min((S + wpb - 1) / wpb, c->sm_count * 2));
+        capture_kernel<<<grid, 32 * wpb, smem, st>>>(c->inst, b, cb);
+        e = cudaGetLastError();
+        g_launches++;
+    }
+    std::vector<double> rows;
+    std::vector<int32_t> cu;
+    if (!e) {
+        rows.resize(cand_n * K);
+        cu.resize(cand_n);
+        e = cudaMemcpyAsync(rows.data(), d_rows, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+    }
+    if (!e) e = cudaMemcpyAsync(cu.data(), d_cust, cu.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaMemcpyAsync(info, d_info, slots_n * 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    cudaFree(d_rows);
+    cudaFree(d_cust);
+    cudaFree(d_info);
+    if (e) return fail(SIDR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    // rows -> 61-slot tables: captured slots, C1..C5 where active, zero elsewhere
+    static const double kC[5] = {0.1, 0.2, 0.3, 0.4, 0.5};
+    for (size_t q = 0; q < cand_n; q++) {
+        double* t = terms + q * kTerms;
+        for (int k = 0; k < kTerms; k++) t[k] = 0.0;
+        for (int k = 36; k <= 40; k++)
+            if (slot_active(k, mask)) t[k] = kC[k - 36];
+        for (int k = 0; k < K; k++) t[slot_of[k]] = rows[q * K + k];
+    }
+    if (cust) std::memcpy(cust, cu.data(), cu.size() * sizeof(int32_t));
     return SIDR_OK;
 }
 

@@ -384,6 +384,31 @@ struct Gp {
         pop.swap(next);
     }
 
+    // gp_step's breeding loop (engine/gp.hpp:178-192) on its own: `count`
+    // children of the current population (crossover pairs, mutation,
+    // reproduction, each parent by tournament), no elites.
+    std::vector<Rule> breed(const std::vector<double>& fit, size_t count) {
+        std::vector<Rule> next;
+        next.reserve(count);
+        while (next.size() < count) {
+            const double r = rng.random();
+            if (r < cfg.crossover_rate) {
+                const Rule& p1 = tournament(fit);
+                const Rule& p2 = tournament(fit);
+                Rule c1, c2;
+                crossover(p1, p2, c1, c2);
+                next.push_back(std::move(c1));
+                if (next.size() < count) next.push_back(std::move(c2));
+            } else if (r < cfg.crossover_rate + cfg.mutation_rate) {
+                const Rule& p = tournament(fit);
+                next.push_back(mutate(p));
+            } else {
+                next.push_back(tournament(fit));
+            }
+        }
+        return next;
+    }
+
     std::string text() const {
         std::string out;
         for (const Rule& r : pop) {

@@ -318,7 +318,7 @@ void slot_needs(int s, uint32_t& need, int& reach_k, uint64_t& explore) {
 }  // namespace
 
 std::string compile_rule(const int32_t* ops, const int32_t* args, int len, const int64_t* M,
-                         CompiledRule& out) {
+                         CompiledRule& out, bool all_active_rows) {
     out = CompiledRule();
     if (len < 1) return "empty rule";
     if (len > kMaxTree) return "rule longer than MAX_TREE (1024)";
@@ -326,6 +326,12 @@ std::string compile_rule(const int32_t* ops, const int32_t* args, int len, const
     int sp = 0, maxsp = 0;
     int slot_row[kTerms];
     for (int s = 0; s < kTerms; s++) slot_row[s] = -1;
+    if (all_active_rows)
+        for (int s = 0; s < kTerms; s++)
+            if (slot_active(s, M) && !(s >= 36 && s <= 40)) {
+                slot_row[s] = out.K++;
+                out.slots.push_back((uint8_t)s);
+            }
     for (int k = 0; k < len; k++) {
         const int o = ops[k];
         if (o == -1) {

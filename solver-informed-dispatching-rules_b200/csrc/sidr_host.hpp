@@ -49,8 +49,11 @@ struct CompiledRule {
 // interpreter's contract -- opcodes in {-2,-1,0..6}, slots < 61, no stack
 // underflow, stack depth <= 32, exactly one value left -- and compiles it
 // under `mask` (61 flags).  Returns an empty string or the error text.
+// all_active_rows: rows 0.. hold every slot active under the mask (ascending,
+// the constants C1..C5 excepted) whether the rule reads it or not -- the
+// terminal table a decision-situation capture records.
 std::string compile_rule(const int32_t* ops, const int32_t* args, int len, const int64_t* mask,
-                         CompiledRule& out);
+                         CompiledRule& out, bool all_active_rows = false);
 
 // Slot activity under a mask, as pick_best assigns terms[] (engine/sim_core.hpp:
 // 84-197): slots 0-9 always; 11 under mask 11 or 33; 14 under 14 or 32; 30

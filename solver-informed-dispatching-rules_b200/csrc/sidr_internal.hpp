@@ -142,4 +142,15 @@ struct DevBatch {
     const int32_t* order;
 };
 
+// Decision-situation capture (capture_kernel only): for scenario s and its
+// d-th decision (d < dec), candidate c (< cand) -> its k terminal rows at
+// rows[((s*dec + d)*cand + c)*k] and its customer at cust[(s*dec + d)*cand + c];
+// info[(s*dec + d)*2] = {candidates, chosen customer (-1: none)}.
+struct CaptureBuf {
+    double* rows;
+    int32_t* cust;
+    int32_t* info;
+    int dec, cand, k;
+};
+
 }  // namespace sidr

@@ -807,10 +807,18 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
     return pri;
 }
 
-// One decision: returns the chosen customer or -1 (pick_best).
-template <bool COUNT>
+// Where a capture launch records one decision (slot < 0: not recorded).
+struct CaptureAt {
+    const CaptureBuf* C;
+    int slot;
+};
+
+// One decision: returns the chosen customer or -1 (pick_best).  CAPTURE:
+// every candidate's terminal rows (the first B.cap_k rows: the rule was
+// compiled with all active slots as rows) and the choice are recorded.
+template <bool COUNT, bool CAPTURE = false>
 __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, Decision& d,
-                      WarpCounts& wc) {
+                      WarpCounts& wc, CaptureAt cap = CaptureAt{nullptr, -1}) {
     const int lane = threadIdx.x & 31;
     const int n = I.n, ld = I.ld, nw = I.nw;
     const uint32_t need = rm.need;
@@ -886,6 +894,12 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         if (k < ncand) {
             idx = S.cand[k];
             pri = score_candidate<COUNT>(I, S, rm, d, idx, wc);
+            if (CAPTURE && cap.slot >= 0 && k < cap.C->cand) {
+                const CaptureBuf& C = *cap.C;
+                const size_t at = (size_t)cap.slot * C.cand + k;
+                for (int r = 0; r < C.k; r++) C.rows[at * C.k + r] = S.rows[r * 32 + lane];
+                C.cust[at] = idx;
+            }
         }
         SIDR_SEC_MARK(t_argmax)
 #pragma unroll
@@ -903,14 +917,19 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         }
         SIDR_SEC_ADD(8, t_argmax);
     }
+    if (CAPTURE && cap.slot >= 0 && lane == 0) {
+        cap.C->info[2 * cap.slot] = ncand;
+        cap.C->info[2 * cap.slot + 1] = best;
+    }
     return best;
 }
 
 // sim_one (engine/sim_core.hpp:207-238) for one pair; every lane returns the
 // same total.
-template <bool COUNT>
+template <bool COUNT, bool CAPTURE = false>
 __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
-                          const double* smp, WarpCounts& wc) {
+                          const double* smp, WarpCounts& wc, const CaptureBuf* capC = nullptr,
+                          int scenario = 0) {
     const int lane = threadIdx.x & 31;
     const int n = I.n, ld = I.ld;
     for (int w = lane; w < I.nw; w += 32) {
@@ -920,13 +939,21 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
     }
     __syncwarp();
     double total = 0.0;
+    int dec_no = 0;
     for (int v = 0; v < I.m; v++) {
         Decision d;
         d.remaining = I.m - v - 1;
         d.cur = 0;
         d.ct = 0.0;
         for (;;) {
-            const int b = decide<COUNT>(I, S, rm, d, wc);
+            int b;
+            if constexpr (CAPTURE) {
+                CaptureAt cap{capC, dec_no < capC->dec ? scenario * capC->dec + dec_no : -1};
+                dec_no++;
+                b = decide<COUNT, true>(I, S, rm, d, wc, cap);
+            } else {
+                b = decide<COUNT>(I, S, rm, d, wc);
+            }
             if (b < 0) break;
             SIDR_SEC_MARK(t_upd)
             const double arrive = d.ct + I.dist[(size_t)d.cur * ld + b + 1];
@@ -944,8 +971,9 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
 
 // The persistent work loop.  MULTI: every rule carries its instance; the
 // warp stages the instance descriptor with the rule's program.
-template <bool COUNT, bool MULTI>
-__device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B) {
+template <bool COUNT, bool MULTI, bool CAPTURE = false>
+__device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
+                                          const CaptureBuf* capC = nullptr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -982,7 +1010,9 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B) 
         const double* smp =
             MULTI ? B.sampled + B.smp_off[rm.inst] + (size_t)s * I.n
                   : B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
-        const double tot = rollout<COUNT>(I, S, rm, smp, wc);
+        double tot;
+        if constexpr (CAPTURE) tot = rollout<COUNT, true>(I, S, rm, smp, wc, capC, s);
+        else tot = rollout<COUNT>(I, S, rm, smp, wc);
         if (lane == 0) B.out[(size_t)p * B.T + s] = tot;
     }
     if (COUNT) {
@@ -1004,6 +1034,13 @@ template <bool COUNT>
 __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
     eval_kernel(const DevInst I, const DevBatch B) {
     eval_body<COUNT, false>(I, B);
+}
+
+// Decision-situation capture: one rule on B.T scenarios, every decision's
+// candidate terminal tables recorded (DevBatch cap_* fields).
+__global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
+    capture_kernel(const DevInst I, const DevBatch B, const CaptureBuf C) {
+    eval_body<false, false, true>(I, B, &C);
 }
 
 // Multi-instance evaluator, one instantiation per block shape (warps per

@@ -1,0 +1,320 @@
+// sidr_sgp.cpp -- the surrogate-assisted GP driver (include/sidr_surrogate.h):
+// the GP of sidr_gp_core.hpp whose offspring are pre-screened by the MLP of
+// sidr_surrogate.cu on their phenotypes, with the evaluator as the judge of
+// every fitness and plain breeding whenever the model's audit rank
+// correlation is too low.
+#include <chrono>
+#include <numeric>
+
+#include "../../include/sidr_surrogate.h"
+#include "sidr_gp_core.hpp"
+
+using namespace sidr::gp;
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Packed {
+    std::vector<int32_t> ops, args, off, len;
+    sidr_rules_desc desc() {
+        return sidr_rules_desc{ops.data(), args.data(), off.data(), len.data(), (int32_t)off.size(),
+                               (int64_t)ops.size()};
+    }
+};
+
+void pack_rules(const std::vector<Rule>& rules, const Vocab& v, Packed& pk) {
+    for (const Rule& r : rules) {
+        pk.off.push_back((int32_t)pk.ops.size());
+        size_t k = 0;
+        compile_at(r, k, v, pk.ops, pk.args, pk.ops.size());
+        pk.len.push_back((int32_t)pk.ops.size() - pk.off.back());
+    }
+}
+
+// Ranks with ties sharing their average rank.
+std::vector<double> ranks_of(const std::vector<double>& x) {
+    const size_t n = x.size();
+    std::vector<size_t> o(n);
+    std::iota(o.begin(), o.end(), 0);
+    std::stable_sort(o.begin(), o.end(), [&](size_t a, size_t b) { return x[a] < x[b]; });
+    std::vector<double> r(n);
+    for (size_t i = 0; i < n;) {
+        size_t j = i;
+        while (j + 1 < n && x[o[j + 1]] == x[o[i]]) j++;
+        const double avg = 0.5 * (double)(i + j);
+        for (size_t k = i; k <= j; k++) r[o[k]] = avg;
+        i = j + 1;
+    }
+    return r;
+}
+
+// Spearman's rank correlation (Pearson correlation of the ranks).
+double spearman(const std::vector<double>& a, const std::vector<double>& b) {
+    const std::vector<double> ra = ranks_of(a), rb = ranks_of(b);
+    const double n = (double)a.size();
+    double ma = 0, mb = 0;
+    for (size_t i = 0; i < a.size(); i++) {
+        ma += ra[i];
+        mb += rb[i];
+    }
+    ma /= n;
+    mb /= n;
+    double sab = 0, saa = 0, sbb = 0;
+    for (size_t i = 0; i < a.size(); i++) {
+        sab += (ra[i] - ma) * (rb[i] - mb);
+        saa += (ra[i] - ma) * (ra[i] - ma);
+        sbb += (rb[i] - mb) * (rb[i] - mb);
+    }
+    if (saa <= 0 || sbb <= 0) return 0.0;
+    return sab / std::sqrt(saa * sbb);
+}
+
+}  // namespace
+
+extern "C" {
+
+void sidr_sgp_default_config(sidr_sgp_config* c) {
+    if (!c) return;
+    c->screen = 8192;
+    c->train_steps = 200;
+    c->batch = 1024;
+    c->lr = 1e-3f;
+    c->audit = 128;
+    c->rho_min = 0.8;
+    c->history = 3;
+    c->n_situations = SIDR_MLP_INPUTS - 8;
+    c->capture_scenarios = 16;
+    c->max_cand = 64;
+    c->model_seed = 1;
+    c->use_surrogate = 1;
+    c->device = 0;
+}
+
+sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
+                         const sidr_sgp_config* sc, const char* terminals_csv, const int64_t* mask,
+                         uint64_t seed, int64_t test_seed, double* best_train, double* held_out,
+                         double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
+                         sidr_sgp_result* result) {
+    std::string err;
+    if (!ctx || !inst || !sc || !mask) return gp_fail(SIDR_ERR_INVALID, "null argument");
+    if (!valid_config(cfg, err)) return gp_fail(SIDR_ERR_INVALID, err);
+    if (sc->n_situations + 8 != SIDR_MLP_INPUTS)
+        return gp_fail(SIDR_ERR_INVALID, "n_situations + 8 must equal the model's 40 inputs");
+    if (sc->screen < cfg->population || sc->audit < 3 || sc->history < 1 || sc->batch < 1 ||
+        sc->capture_scenarios < 1 || sc->max_cand < 2 || cfg->test_samples < 1)
+        return gp_fail(SIDR_ERR_INVALID, "surrogate settings out of range");
+    std::vector<std::string> terms;
+    if (!parse_terminals(terminals_csv, terms, err)) return gp_fail(SIDR_ERR_INVALID, err);
+    const int n = inst->n, ps = cfg->population, T = cfg->train_samples, G = cfg->generations;
+    const int NS = sc->n_situations, NF = SIDR_MLP_INPUTS;
+    const double t_start = now_s();
+    double t_eval = 0.0, t_model = 0.0;
+    int64_t evals = 0;
+    int screened = 0, fallback = 0;
+
+    Gp gp(*cfg, seed);
+    gp.vocab.terminals = terms;
+    gp.vocab.n_funcs = cfg->with_rmod ? 7 : 6;
+    gp.init();
+
+    auto simulate = [&](const std::vector<Rule>& rules, long long block_seed, int S,
+                        std::vector<double>& fit) -> sidr_status {
+        Packed pk;
+        pack_rules(rules, gp.vocab, pk);
+        std::vector<double> smp((size_t)S * n);
+        sidr_gen_durations(n, inst->durations, 0.2, S, block_seed, smp.data());
+        sidr_rules_desc r = pk.desc();
+        std::vector<double> out((size_t)r.P * S);
+        const double t0 = now_s();
+        const sidr_status st = sidr_evaluate(ctx, &r, smp.data(), S, mask, out.data());
+        t_eval += now_s() - t0;
+        evals += (int64_t)r.P * S;
+        if (st != SIDR_OK) return gp_fail(st, std::string("evaluation: ") + sidr_last_error());
+        fit.assign(r.P, 0.0);
+        for (int p = 0; p < r.P; p++) {
+            double acc = 0.0;
+            for (int s = 0; s < S; s++) acc += out[(size_t)p * S + s];
+            fit[p] = acc / S;
+        }
+        return SIDR_OK;
+    };
+
+    // decision situations and the model (created on first use)
+    std::vector<double> sit_terms;
+    std::vector<int32_t> sit_nc, sit_ref;
+    sidr_mlp* model = nullptr;
+    struct ModelGuard {
+        sidr_mlp*& m;
+        ~ModelGuard() {
+            if (m) sidr_mlp_destroy(m);
+        }
+    } guard{model};
+    auto features_of = [&](const std::vector<Rule>& rules, std::vector<float>& f) -> sidr_status {
+        Packed pk;
+        pack_rules(rules, gp.vocab, pk);
+        sidr_rules_desc r = pk.desc();
+        f.assign((size_t)r.P * NF, 0.0f);
+        const double t0 = now_s();
+        const sidr_status st = sidr_phenotype(&r, sit_terms.data(), sit_nc.data(), sit_ref.data(), NS,
+                                              sc->max_cand, sc->device, f.data());
+        t_model += now_s() - t0;
+        return st;
+    };
+    std::vector<std::vector<float>> hist_x;
+    std::vector<std::vector<double>> hist_t;
+
+    std::vector<double> fit;
+    for (int g = 0; g < G; g++) {
+        sidr_status st = simulate(gp.pop, (long long)seed * 10000 + g, T, fit);
+        if (st != SIDR_OK) return st;
+        size_t bi = 0;
+        for (size_t p = 1; p < fit.size(); p++)
+            if (fit[p] > fit[bi]) bi = p;
+        if (best_train) best_train[g] = fit[bi];
+        {
+            std::vector<double> ho;
+            if ((st = simulate({gp.pop[bi]}, test_seed, cfg->test_samples, ho)) != SIDR_OK) return st;
+            if (held_out) held_out[g] = ho[0];
+        }
+        if (rho) rho[g] = std::nan("");
+        if (sc->use_surrogate && g == 0) {
+            // situations from the first generation's best rule
+            Packed pk;
+            pack_rules({gp.pop[bi]}, gp.vocab, pk);
+            sidr_rules_desc r = pk.desc();
+            const int S = sc->capture_scenarios, D = 64, C = sc->max_cand;
+            std::vector<double> smp((size_t)S * n), cap_terms((size_t)S * D * C * 61);
+            std::vector<int32_t> cap_cust((size_t)S * D * C), cap_info((size_t)S * D * 2);
+            sidr_gen_durations(n, inst->durations, 0.2, S, (long long)seed * 10000 + 7777, smp.data());
+            const double t0 = now_s();
+            st = sidr_capture_situations(ctx, &r, smp.data(), S, mask, D, C, cap_terms.data(),
+                                         cap_cust.data(), cap_info.data());
+            t_eval += now_s() - t0;
+            if (st != SIDR_OK) return st;
+            std::vector<int> pool;  // decisions with 2..C candidates and a choice
+            for (int q = 0; q < S * D; q++)
+                if (cap_info[2 * q] >= 2 && cap_info[2 * q] <= C && cap_info[2 * q + 1] >= 0) pool.push_back(q);
+            if ((int)pool.size() < NS) return gp_fail(SIDR_ERR_INVALID, "too few decision situations captured");
+            Mt19937 srng(seed * 7919 + 17);
+            const std::vector<size_t> pick = srng.sample(pool.size(), (size_t)NS);
+            sit_terms.assign((size_t)NS * C * 61, 0.0);
+            for (int j = 0; j < NS; j++) {
+                const int q = pool[pick[j]];
+                const int nc = cap_info[2 * q], chosen = cap_info[2 * q + 1];
+                int ref = -1;
+                for (int c = 0; c < nc; c++)
+                    if (cap_cust[(size_t)q * C + c] == chosen) ref = c;
+                if (ref < 0) return gp_fail(SIDR_ERR_KERNEL, "captured choice not among the candidates");
+                std::copy(cap_terms.begin() + (size_t)q * C * 61, cap_terms.begin() + (size_t)(q + 1) * C * 61,
+                          sit_terms.begin() + (size_t)j * C * 61);
+                sit_nc.push_back(nc);
+                sit_ref.push_back(ref);
+            }
+            if ((st = sidr_mlp_create(sc->device, sc->model_seed, &model)) != SIDR_OK) return st;
+        }
+        if (sc->use_surrogate) {
+            std::vector<float> f;
+            if ((st = features_of(gp.pop, f)) != SIDR_OK) return st;
+            hist_x.push_back(f);
+            hist_t.push_back(fit);
+        }
+        if (g < G - 1) {
+            bool screened_gen = false;
+            if (sc->use_surrogate) {
+                while ((int)hist_x.size() > sc->history * 2) {  // population + audit entries per generation
+                    hist_x.erase(hist_x.begin());
+                    hist_t.erase(hist_t.begin());
+                }
+                // train on the recent simulated fitness, standardised
+                std::vector<float> X, Y;
+                double mu = 0, sd = 0;
+                size_t cnt = 0;
+                for (auto& t : hist_t)
+                    for (double v : t) {
+                        mu += v;
+                        cnt++;
+                    }
+                mu /= cnt;
+                for (auto& t : hist_t)
+                    for (double v : t) sd += (v - mu) * (v - mu);
+                sd = std::sqrt(sd / cnt) + 1e-9;
+                for (size_t h = 0; h < hist_x.size(); h++) {
+                    X.insert(X.end(), hist_x[h].begin(), hist_x[h].end());
+                    for (double v : hist_t[h]) Y.push_back((float)((v - mu) / sd));
+                }
+                float loss = 0.0f;
+                double t0 = now_s();
+                st = sidr_mlp_train(model, X.data(), Y.data(), (int32_t)Y.size(), sc->train_steps, sc->batch,
+                                    sc->lr, seed * 131 + g, &loss);
+                t_model += now_s() - t0;
+                if (st != SIDR_OK) return st;
+                // screen: breed `screen` candidates, predict, audit a random sample
+                std::vector<Rule> cand = gp.breed(fit, (size_t)sc->screen);
+                std::vector<float> cf;
+                if ((st = features_of(cand, cf)) != SIDR_OK) return st;
+                std::vector<float> pred(cand.size());
+                t0 = now_s();
+                st = sidr_mlp_predict(model, cf.data(), (int32_t)cand.size(), pred.data());
+                t_model += now_s() - t0;
+                if (st != SIDR_OK) return st;
+                const std::vector<size_t> aud = gp.rng.sample(cand.size(), (size_t)sc->audit);
+                std::vector<Rule> aud_rules;
+                for (size_t a : aud) aud_rules.push_back(cand[a]);
+                std::vector<double> aud_fit;
+                if ((st = simulate(aud_rules, (long long)seed * 10000 + g, T, aud_fit)) != SIDR_OK) return st;
+                std::vector<double> aud_pred;
+                std::vector<float> aud_x;
+                for (size_t a : aud) {
+                    aud_pred.push_back(pred[a]);
+                    aud_x.insert(aud_x.end(), cf.begin() + a * NF, cf.begin() + (a + 1) * NF);
+                }
+                const double r_s = spearman(aud_pred, aud_fit);
+                if (rho) rho[g] = r_s;
+                hist_x.push_back(aud_x);
+                hist_t.push_back(aud_fit);
+                if (r_s >= sc->rho_min) {
+                    // elites of the current population, then the best-predicted candidates
+                    std::vector<int> order(ps);
+                    std::iota(order.begin(), order.end(), 0);
+                    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return fit[a] > fit[b]; });
+                    std::vector<Rule> next;
+                    for (int e = 0; e < cfg->elitism && e < ps; e++) next.push_back(gp.pop[order[e]]);
+                    std::vector<int> co(cand.size());
+                    std::iota(co.begin(), co.end(), 0);
+                    std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return pred[a] > pred[b]; });
+                    for (size_t k = 0; (int)next.size() < ps && k < co.size(); k++) next.push_back(cand[co[k]]);
+                    gp.pop.swap(next);
+                    screened_gen = true;
+                    screened++;
+                } else {
+                    fallback++;
+                }
+            }
+            if (!screened_gen) gp.step(fit);
+        }
+        if (gen_seconds) gen_seconds[g] = now_s() - t_start;
+    }
+    // the last generation's best rule
+    size_t bi = 0;
+    for (size_t p = 1; p < fit.size(); p++)
+        if (fit[p] > fit[bi]) bi = p;
+    std::string text;
+    size_t k = 0;
+    prefix_at(gp.pop[bi], k, gp.vocab, text);
+    if (best_rule && rule_cap > (int64_t)text.size()) std::memcpy(best_rule, text.c_str(), text.size() + 1);
+    if (result) {
+        result->eval_seconds = t_eval;
+        result->model_seconds = t_model;
+        result->host_seconds = now_s() - t_start - t_eval - t_model;
+        result->evaluations = evals;
+        result->generations_screened = screened;
+        result->generations_fallback = fallback;
+    }
+    return SIDR_OK;
+}
+
+}  // extern "C"

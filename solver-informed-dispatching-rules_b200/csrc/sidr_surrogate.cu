@@ -158,6 +158,61 @@ __global__ void gather_rows_kernel(const float* src, const float* tsrc, const in
     }
 }
 
+// eval_tree (engine/sim_core.hpp:11-41) over one 61-slot terminal table.
+__device__ double eval_rule(const int32_t* ops, const int32_t* args, int len, const double* t) {
+    double st[32];
+    int sp = 0;
+    for (int k = 0; k < len; k++) {
+        const int o = ops[k];
+        if (o == -1) {
+            st[sp++] = t[args[2 * k]];
+        } else if (o == -2) {
+            st[sp++] = args[2 * k] / 1000.0;
+        } else {
+            const double b = st[sp - 1], a = st[sp - 2];
+            sp -= 2;
+            double r;
+            if (o == 0) r = a + b;
+            else if (o == 1) r = a - b;
+            else if (o == 2) r = a * b;
+            else if (o == 3) r = fabs(b) < 1e-10 ? 1.0 : a / b;
+            else if (o == 4) r = a < b ? a : b;
+            else if (o == 5) r = a > b ? a : b;
+            else {
+                const double base = a > 0.0 ? a : 0.0;
+                const double e = b < 0.0 ? 0.0 : (b > 1.0 ? 1.0 : b);
+                r = pow(base, 1.0 + e);
+            }
+            st[sp++] = r;
+        }
+    }
+    const double v = st[0];
+    return v != v ? -1e300 : v;
+}
+
+// One thread per (rule, situation): the position of the situation's
+// reference choice in the rule's ranking of the candidates (strict >, lower
+// position first on ties), scaled to [0, 1].
+__global__ void phenotype_kernel(const int32_t* ops, const int32_t* args, const int32_t* off,
+                                 const int32_t* len, int P, const double* terms, const int32_t* ncand,
+                                 const int32_t* ref, int n_sit, int max_cand, float* feat, int n_feat) {
+    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (id >= (long long)P * n_sit) return;
+    const int p = (int)(id / n_sit), j = (int)(id % n_sit);
+    const int nc = ncand[j], r = ref[j];
+    const int32_t* o = ops + off[p];
+    const int32_t* a = args + 2 * (size_t)off[p];
+    const double* base = terms + (size_t)j * max_cand * 61;
+    const double pr = eval_rule(o, a, len[p], base + (size_t)r * 61);
+    int pos = 0;
+    for (int c = 0; c < nc; c++) {
+        if (c == r) continue;
+        const double pc = eval_rule(o, a, len[p], base + (size_t)c * 61);
+        if (pc > pr || (pc == pr && c < r)) pos++;
+    }
+    feat[(size_t)p * n_feat + j] = nc > 1 ? (float)pos / (float)(nc - 1) : 0.0f;
+}
+
 int grid_for(long long n, int threads = 256) {
     return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148 * 8));
 }
@@ -384,6 +439,110 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
     if (s) return s;
     if (e) return fail_s(SIDR_ERR_CUDA, std::string("gemm: ") + cudaGetErrorString(e));
     if (h) return fail_s(SIDR_ERR_KERNEL, "gemm: an MMA did not complete within its wait limit");
+    return SIDR_OK;
+}
+
+sidr_status sidr_phenotype(const sidr_rules_desc* r, const double* terms, const int32_t* ncand,
+                           const int32_t* ref, int32_t n_sit, int32_t max_cand, int device,
+                           float* features) {
+    if (!r || !terms || !ncand || !ref || !features || n_sit < 1 || max_cand < 1)
+        return fail_s(SIDR_ERR_INVALID, "bad argument");
+    const int P = r->P, nf = n_sit + 8;
+    for (int j = 0; j < n_sit; j++)
+        if (ncand[j] < 1 || ncand[j] > max_cand || ref[j] < 0 || ref[j] >= ncand[j])
+            return fail_s(SIDR_ERR_INVALID, "situation " + std::to_string(j) + ": bad candidate count or choice");
+    // host: rule validity (the device interpreter trusts it) and token features
+    for (int p = 0; p < P; p++) {
+        const int32_t* o = r->ops + r->offsets[p];
+        const int32_t* a = r->args + 2 * (size_t)r->offsets[p];
+        const int L = r->lengths[p];
+        if (L < 1 || L > 1024) return fail_s(SIDR_ERR_RULE, "rule " + std::to_string(p) + ": bad length");
+        int sp = 0, depth_max = 0, leaves = 0, consts = 0, addsub = 0, muldiv = 0, other = 0;
+        std::vector<int> dstack;
+        bool seen[61] = {false};
+        int distinct = 0;
+        for (int k = 0; k < L; k++) {
+            if (o[k] == -1 || o[k] == -2) {
+                if (o[k] == -1) {
+                    if (a[2 * k] < 0 || a[2 * k] >= 61) return fail_s(SIDR_ERR_RULE, "slot out of range");
+                    if (!seen[a[2 * k]]) distinct++;
+                    seen[a[2 * k]] = true;
+                } else {
+                    consts++;
+                }
+                leaves++;
+                dstack.push_back(0);
+                sp++;
+            } else if (o[k] >= 0 && o[k] <= 6) {
+                if (sp < 2) return fail_s(SIDR_ERR_RULE, "stack underflow");
+                const int d1 = dstack.back();
+                dstack.pop_back();
+                const int d0 = dstack.back();
+                dstack.pop_back();
+                dstack.push_back(1 + std::max(d0, d1));
+                depth_max = std::max(depth_max, dstack.back());
+                sp--;
+                if (o[k] <= 1) addsub++;
+                else if (o[k] <= 3) muldiv++;
+                else other++;
+            } else {
+                return fail_s(SIDR_ERR_RULE, "unknown opcode");
+            }
+            if (sp > 32) return fail_s(SIDR_ERR_RULE, "stack deeper than 32");
+        }
+        if (sp != 1) return fail_s(SIDR_ERR_RULE, "rule leaves more than one value");
+        const int ops_n = std::max(1, addsub + muldiv + other);
+        float* f = features + (size_t)p * nf + n_sit;
+        f[0] = L / 255.0f;
+        f[1] = depth_max / 16.0f;
+        f[2] = leaves / 128.0f;
+        f[3] = distinct / 32.0f;
+        f[4] = consts / 32.0f;
+        f[5] = (float)addsub / ops_n;
+        f[6] = (float)muldiv / ops_n;
+        f[7] = (float)other / ops_n;
+    }
+    if (P == 0) return SIDR_OK;
+    SIDR_SCHECK(cudaSetDevice(device));
+    const size_t nodes = (size_t)r->n_nodes;
+    int32_t *d_ops = nullptr, *d_args = nullptr, *d_off = nullptr, *d_len = nullptr, *d_nc = nullptr,
+            *d_ref = nullptr;
+    double* d_terms = nullptr;
+    float* d_feat = nullptr;
+    const size_t tn = (size_t)n_sit * max_cand * 61;
+    cudaError_t e = cudaMalloc(&d_ops, nodes * 4);
+    if (!e) e = cudaMalloc(&d_args, nodes * 8);
+    if (!e) e = cudaMalloc(&d_off, (size_t)P * 4);
+    if (!e) e = cudaMalloc(&d_len, (size_t)P * 4);
+    if (!e) e = cudaMalloc(&d_nc, (size_t)n_sit * 4);
+    if (!e) e = cudaMalloc(&d_ref, (size_t)n_sit * 4);
+    if (!e) e = cudaMalloc(&d_terms, tn * 8);
+    if (!e) e = cudaMalloc(&d_feat, (size_t)P * nf * 4);
+    if (!e) e = cudaMemcpy(d_ops, r->ops, nodes * 4, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d_args, r->args, nodes * 8, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d_off, r->offsets, (size_t)P * 4, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d_len, r->lengths, (size_t)P * 4, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d_nc, ncand, (size_t)n_sit * 4, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d_ref, ref, (size_t)n_sit * 4, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d_terms, terms, tn * 8, cudaMemcpyHostToDevice);
+    if (!e) {
+        const long long items = (long long)P * n_sit;
+        phenotype_kernel<<<(int)((items + 127) / 128), 128>>>(d_ops, d_args, d_off, d_len, P, d_terms, d_nc,
+                                                              d_ref, n_sit, max_cand, d_feat, nf);
+        e = cudaGetLastError();
+    }
+    // the kernel wrote the ranking columns; the token columns come from the host
+    std::vector<float> got;
+    if (!e) {
+        got.resize((size_t)P * nf);
+        e = cudaMemcpy(got.data(), d_feat, got.size() * 4, cudaMemcpyDeviceToHost);
+    }
+    for (void* q : {(void*)d_ops, (void*)d_args, (void*)d_off, (void*)d_len, (void*)d_nc, (void*)d_ref,
+                    (void*)d_terms, (void*)d_feat})
+        cudaFree(q);
+    if (e) return fail_s(SIDR_ERR_CUDA, std::string("phenotype: ") + cudaGetErrorString(e));
+    for (int p = 0; p < P; p++)
+        for (int j = 0; j < n_sit; j++) features[(size_t)p * nf + j] = got[(size_t)p * nf + j];
     return SIDR_OK;
 }
 

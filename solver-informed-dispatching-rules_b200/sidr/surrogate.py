@@ -114,3 +114,109 @@ class MLP:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------ situations, phenotype
+
+class _SgpCfg(C.Structure):
+    _fields_ = [("screen", C.c_int32), ("train_steps", C.c_int32), ("batch", C.c_int32),
+                ("lr", C.c_float), ("audit", C.c_int32), ("rho_min", C.c_double),
+                ("history", C.c_int32), ("n_situations", C.c_int32),
+                ("capture_scenarios", C.c_int32), ("max_cand", C.c_int32),
+                ("model_seed", C.c_uint64), ("use_surrogate", C.c_int32), ("device", C.c_int32)]
+
+
+class _SgpResult(C.Structure):
+    _fields_ = [("eval_seconds", C.c_double), ("model_seconds", C.c_double),
+                ("host_seconds", C.c_double), ("evaluations", C.c_int64),
+                ("generations_screened", C.c_int32), ("generations_fallback", C.c_int32)]
+
+
+STRUCTS = {"sidr_sgp_config": _SgpCfg, "sidr_sgp_result": _SgpResult}
+
+
+def _lib2():
+    L = _lib()
+    if not getattr(L, "_sgp_ready", False):
+        from . import _Inst, _Rules
+        from .gp import _Cfg
+        L.sidr_capture_situations.argtypes = [C.c_void_p, C.POINTER(_Rules), _dp, C.c_int32,
+                                              C.POINTER(C.c_int64), C.c_int32, C.c_int32, _dp, _ip, _ip]
+        L.sidr_phenotype.argtypes = [C.POINTER(_Rules), _dp, _ip, _ip, C.c_int32, C.c_int32, C.c_int,
+                                     _fp]
+        L.sidr_sgp_default_config.argtypes = [C.POINTER(_SgpCfg)]
+        L.sidr_sgp_run.argtypes = [C.c_void_p, C.POINTER(_Inst), C.POINTER(_Cfg), C.POINTER(_SgpCfg),
+                                   C.c_char_p, C.POINTER(C.c_int64), C.c_uint64, C.c_int64, _dp, _dp,
+                                   _dp, _dp, C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
+        L._sgp_ready = True
+    return L
+
+
+def capture_situations(ctx, rule, sampled, mask, max_decisions: int = 64, max_cand: int = 64):
+    """Terminal tables of every decision of `rule` (PackedRules with P = 1) on
+    the scenarios: terms [S, D, C, 61], cust [S, D, C], info [S, D, 2]."""
+    from . import _Keep
+    L = _lib2()
+    k = _Keep()
+    smp = np.ascontiguousarray(sampled, dtype=np.float64)
+    S = smp.shape[0]
+    terms = np.zeros((S, max_decisions, max_cand, 61))
+    cust = np.zeros((S, max_decisions, max_cand), np.int32)
+    info = np.zeros((S, max_decisions, 2), np.int32)
+    r = k.rules(rule)
+    _check(L.sidr_capture_situations(ctx.h, C.byref(r), smp.ctypes.data_as(_dp), S, k.i64(mask),
+                                     max_decisions, max_cand, terms.ctypes.data_as(_dp),
+                                     cust.ctypes.data_as(_ip), info.ctypes.data_as(_ip)))
+    return terms, cust, info
+
+
+def phenotype(rules, terms, ncand, ref, device: int = 0) -> np.ndarray:
+    """features [P, n_sit + 8] of the rules on situations terms [n_sit, C, 61]."""
+    from . import _Keep
+    L = _lib2()
+    k = _Keep()
+    t = np.ascontiguousarray(terms, dtype=np.float64)
+    n_sit, max_cand = t.shape[0], t.shape[1]
+    nc = np.ascontiguousarray(ncand, dtype=np.int32)
+    rf = np.ascontiguousarray(ref, dtype=np.int32)
+    out = np.zeros((rules.P, n_sit + 8), np.float32)
+    r = k.rules(rules)
+    _check(L.sidr_phenotype(C.byref(r), t.ctypes.data_as(_dp), nc.ctypes.data_as(_ip),
+                            rf.ctypes.data_as(_ip), n_sit, max_cand, device,
+                            out.ctypes.data_as(_fp)))
+    return out
+
+
+def sgp_config(**kw) -> _SgpCfg:
+    c = _SgpCfg()
+    _lib2().sidr_sgp_default_config(C.byref(c))
+    for k_, v in kw.items():
+        setattr(c, k_, v)
+    return c
+
+
+def sgp_run(ctx, terminals, mask, seed: int = 0, test_seed: int = 1000000,
+            gp: Optional[dict] = None, **sgp_kw) -> dict:
+    """The surrogate-assisted GP (use_surrogate=0: the same driver breeding
+    plainly); per-generation best train fitness, held-out score, audit rho and
+    wall clock."""
+    from . import _Keep
+    from .gp import config
+    L = _lib2()
+    c = config(**(gp or {}))
+    s = sgp_config(**sgp_kw)
+    k = _Keep()
+    inst = k.inst(ctx.sd)
+    G = c.generations
+    bt, ho, rho, secs = np.zeros(G), np.zeros(G), np.zeros(G), np.zeros(G)
+    buf = C.create_string_buffer(1 << 16)
+    res = _SgpResult()
+    _check(L.sidr_sgp_run(ctx.h, C.byref(inst), C.byref(c), C.byref(s),
+                          ",".join(terminals).encode(), k.i64(mask), seed, test_seed,
+                          bt.ctypes.data_as(_dp), ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp),
+                          secs.ctypes.data_as(_dp), buf, 1 << 16, C.byref(res)))
+    return {"best_train": bt, "held_out": ho, "rho": rho, "seconds": secs,
+            "best_rule": buf.value.decode(), "eval_seconds": res.eval_seconds,
+            "model_seconds": res.model_seconds, "host_seconds": res.host_seconds,
+            "evaluations": res.evaluations, "screened": res.generations_screened,
+            "fallback": res.generations_fallback}

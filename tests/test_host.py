@@ -23,7 +23,7 @@ def bits(a):
 
 # ------------------------------------------------------------ the C-ABI .so
 
-HEADERS = ("sidr.h", "sidr_gp.h", "sidr_campaign.h")
+HEADERS = ("sidr.h", "sidr_gp.h", "sidr_campaign.h", "sidr_surrogate.h")
 
 
 def header_symbols():
@@ -32,9 +32,9 @@ def header_symbols():
 
 
 def all_structs():
-    from sidr import campaign, gp
+    from sidr import campaign, gp, surrogate
     return {**sidr.STRUCTS, "sidr_gp_config": gp._Cfg, "sidr_gp_result": gp._Result,
-            **campaign.STRUCTS}
+            **campaign.STRUCTS, **surrogate.STRUCTS}
 
 
 def test_library_exports_every_declared_symbol():

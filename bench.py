@@ -65,6 +65,11 @@ def parse_args():
     ap.add_argument("--multi", action="store_true",
                     help="also time the uneven multi-instance batch (40 instances of 25-288 "
                          "customers) in one autotuned, graph-captured launch")
+    ap.add_argument("--sgp", action="store_true",
+                    help="also run the surrogate-assisted GP against plain GP on the benchmark "
+                         "instance (population 1024, 500 training scenarios, screening 8192 "
+                         "offspring per generation) and report wall clock to equal held-out fitness")
+    ap.add_argument("--sgp-generations", type=int, default=50)
     ap.add_argument("--campaign", action="store_true",
                     help="also time the reference campaign's c101 generation trace (30 seeds x "
                          "1024 rules x 51 generations + held-out) and its vocabulary GA's first "
@@ -380,6 +385,8 @@ def run_ours(args, rank, world, local):
         line["gp"] = gp_leg(ctx, w, args)
     if args.multi and rank == 0:
         line["multi"] = multi_leg(args, stream)
+    if args.sgp and rank == 0:
+        line["sgp"] = sgp_leg(ctx, w, args)
     if args.campaign and rank == 0:
         line["campaign"] = campaign_leg()
     batch.close()
@@ -463,6 +470,39 @@ def campaign_leg():
                          "wall_seconds": t_batch, "eval_seconds": res.eval_seconds,
                          "host_seconds": res.host_seconds, "evaluations": res.evaluations,
                          "evals_per_s": res.evaluations / t_batch}}
+
+
+def sgp_leg(ctx, w, args):
+    """Surrogate-assisted GP vs plain GP through the same driver (the plain arm
+    breeds with gp_step every generation): both runs record each generation's
+    best rule on the held-out 500 scenarios and the wall clock; the result is
+    the time each run needs to reach the plain run's final held-out score
+    (within 0.5 %)."""
+    from sidr import surrogate as SG
+    from sidr.workload import MENU29
+    G = args.sgp_generations
+    cfg = dict(population=args.P, generations=G, train_samples=args.S, test_samples=500)
+    plain = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=0)
+    sgp = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=1)
+    target = plain["held_out"][-1] * (1.0 - 0.005)
+
+    def first_time(r):
+        for g in range(G):
+            if r["held_out"][g] >= target:
+                return float(r["seconds"][g]), g
+        return None, None
+
+    tp, gp_ = first_time(plain)
+    ts, gs = first_time(sgp)
+    summary = lambda r: {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in r.items()}  # noqa: E731
+    return {"generations": G, "population": args.P, "train_scenarios": args.S,
+            "plain_final_held_out": float(plain["held_out"][-1]),
+            "surrogate_final_held_out": float(sgp["held_out"][-1]),
+            "target_held_out": target,
+            "plain_seconds_to_target": tp, "plain_generation_at_target": gp_,
+            "surrogate_seconds_to_target": ts, "surrogate_generation_at_target": gs,
+            "time_ratio": (ts / tp) if (ts is not None and tp) else None,
+            "plain": summary(plain), "surrogate": summary(sgp)}
 
 
 def gp_leg(ctx, w, args):

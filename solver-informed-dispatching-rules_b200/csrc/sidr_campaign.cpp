@@ -132,6 +132,20 @@ struct Packed {
 
 void pack_rule(const Gp& g, size_t p, Packed& pk) { g.packed(pk.ops, pk.args, pk.off, pk.len, p, 1); }
 
+// Every population's rules, compiled on the host's cores, concatenated in
+// population order (offsets as if packed one after another).
+void pack_all(const std::vector<std::unique_ptr<Gp>>& pops, Packed& pk) {
+    std::vector<Packed> part(pops.size());
+    parallel_for((int)pops.size(), [&](int i) { pops[i]->packed(part[i].ops, part[i].args, part[i].off, part[i].len); });
+    for (const Packed& q : part) {
+        const int32_t base = (int32_t)pk.ops.size();
+        for (int32_t o : q.off) pk.off.push_back(o + base);
+        pk.len.insert(pk.len.end(), q.len.begin(), q.len.end());
+        pk.ops.insert(pk.ops.end(), q.ops.begin(), q.ops.end());
+        pk.args.insert(pk.args.end(), q.args.begin(), q.args.end());
+    }
+}
+
 std::vector<double> durations_block(const sidr_instance_desc* inst, int S, long long seed) {
     std::vector<double> v((size_t)S * inst->n);
     sidr_gen_durations(inst->n, inst->durations, 0.2, S, seed, v.data());
@@ -187,7 +201,7 @@ struct Scorer {
         std::vector<std::vector<double>> f;
         auto gfit = [&](int gen_id) -> sidr_status {
             Packed pk;
-            for (auto& g : pops) g->packed(pk.ops, pk.args, pk.off, pk.len);
+            pack_all(pops, pk);
             // the train block of seed s repeats for every genome
             std::vector<double> grouped((size_t)kb * n * T * nn);
             for (int s = 0; s < n; s++) {
@@ -237,7 +251,7 @@ struct Scorer {
         std::vector<std::vector<double>> f;
         auto gfit = [&](int gen_id) -> sidr_status {
             Packed pk;
-            for (auto& p : pops) p->packed(pk.ops, pk.args, pk.off, pk.len);
+            pack_all(pops, pk);
             std::vector<double> grouped((size_t)n * T * nn);
             for (int s = 0; s < n; s++) {
                 const std::vector<double> one = durations_block(inst, T, (long long)s * 10000 + gen_id);
@@ -1034,7 +1048,7 @@ sidr_status sidr_gen_trace(sidr_ctx* ctx, const sidr_instance_desc* inst,
     std::vector<std::vector<double>> f;
     auto gfit = [&](int gen_id) -> sidr_status {
         Packed pk;
-        for (auto& p : pops) p->packed(pk.ops, pk.args, pk.off, pk.len);
+        pack_all(pops, pk);
         std::vector<double> grouped((size_t)n_seeds * T * nn);
         for (int s = 0; s < n_seeds; s++) {
             const std::vector<double> one = durations_block(inst, T, (long long)s * 10000 + gen_id);

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sidr.h"
@@ -139,17 +140,37 @@ sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask
                         HostPrograms& hp, const int32_t* row_of = nullptr, bool all_active_rows = false) {
     hp = HostPrograms();
     hp.meta.resize(r->P);
-    CompiledRule cr;
+    // compile every rule (independently, on the host's cores for large sets) ...
+    std::vector<CompiledRule> crs(r->P);
+    std::vector<std::string> errs(r->P);
+    auto compile_range = [&](int lo, int hi) {
+        for (int p = lo; p < hi; p++) {
+            const int row = row_of ? row_of[p] : p / mask_group;
+            const int64_t* M = masks + (size_t)row * kTerms;
+            errs[p] = compile_rule(r->ops + r->offsets[p], r->args + 2 * (size_t)r->offsets[p],
+                                   r->lengths[p], M, crs[p], all_active_rows);
+        }
+    };
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = r->P >= 2048 ? std::min(hw, 16) : 1;
+    if (nt == 1) {
+        compile_range(0, r->P);
+    } else {
+        std::vector<std::thread> ts;
+        const int per = (r->P + nt - 1) / nt;
+        for (int t = 0; t < nt; t++)
+            ts.emplace_back(compile_range, std::min(r->P, t * per), std::min(r->P, (t + 1) * per));
+        for (auto& t : ts) t.join();
+    }
+    // ... then lay them out in rule order
     for (int p = 0; p < r->P; p++) {
-        const int row = row_of ? row_of[p] : p / mask_group;
-        const int64_t* M = masks + (size_t)row * kTerms;
-        std::string e = compile_rule(r->ops + r->offsets[p], r->args + 2 * (size_t)r->offsets[p],
-                                     r->lengths[p], M, cr, all_active_rows);
+        const std::string& e = errs[p];
         if (!e.empty()) {
             const sidr_status s = (e.find("MAX_") != std::string::npos) ? SIDR_ERR_TOO_LARGE
                                                                         : SIDR_ERR_RULE;
             return fail(s, "rule " + std::to_string(p) + ": " + e);
         }
+        const CompiledRule& cr = crs[p];
         RuleMeta& m = hp.meta[p];
         m.prog_off = (int32_t)hp.prog.size();
         m.const_off = (int32_t)hp.consts.size();

@@ -474,7 +474,9 @@ def campaign_leg():
 
 def sgp_leg(ctx, w, args):
     """Surrogate-assisted GP vs plain GP through the same driver (the plain arm
-    breeds with gp_step every generation): both runs record each generation's
+    breeds with gp_step every generation; the surrogate arms keep the
+    best-predicted distinct offspring overall, or pre-select the best of each
+    group of 8): every run records each generation's
     best rule on the held-out 500 scenarios and the wall clock; the result is
     the time each run needs to reach the plain run's final held-out score
     (within 0.5 %)."""
@@ -484,6 +486,8 @@ def sgp_leg(ctx, w, args):
     cfg = dict(population=args.P, generations=G, train_samples=args.S, test_samples=500)
     plain = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=0)
     sgp = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=1)
+    pre = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=1,
+                     selection=1)
     target = plain["held_out"][-1] * (1.0 - 0.005)
 
     def first_time(r):
@@ -494,6 +498,7 @@ def sgp_leg(ctx, w, args):
 
     tp, gp_ = first_time(plain)
     ts, gs = first_time(sgp)
+    tq, gq = first_time(pre)
     summary = lambda r: {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in r.items()}  # noqa: E731
     return {"generations": G, "population": args.P, "train_scenarios": args.S,
             "plain_final_held_out": float(plain["held_out"][-1]),
@@ -502,7 +507,10 @@ def sgp_leg(ctx, w, args):
             "plain_seconds_to_target": tp, "plain_generation_at_target": gp_,
             "surrogate_seconds_to_target": ts, "surrogate_generation_at_target": gs,
             "time_ratio": (ts / tp) if (ts is not None and tp) else None,
-            "plain": summary(plain), "surrogate": summary(sgp)}
+            "preselection_final_held_out": float(pre["held_out"][-1]),
+            "preselection_seconds_to_target": tq, "preselection_generation_at_target": gq,
+            "preselection_time_ratio": (tq / tp) if (tq is not None and tp) else None,
+            "plain": summary(plain), "surrogate": summary(sgp), "preselection": summary(pre)}
 
 
 def gp_leg(ctx, w, args):

@@ -102,6 +102,9 @@ typedef struct sidr_sgp_config {
     uint64_t model_seed;       /* [1] */
     int32_t use_surrogate;     /* [1] 0: the same driver with plain breeding (the comparison run) */
     int32_t device;            /* [0] device of the model and of the phenotype kernel */
+    int32_t selection;         /* [0] 0: the best-predicted distinct offspring overall;
+                                  1: pre-selection, the best-predicted of each group of
+                                  screen / (population - elites) consecutive offspring */
 } sidr_sgp_config;
 
 void sidr_sgp_default_config(sidr_sgp_config* cfg);
@@ -120,8 +123,8 @@ typedef struct sidr_sgp_result {
  * last `history` generations' simulated fitness (standardised), `screen`
  * offspring are bred by gp_step's loop, their phenotypes predicted, `audit`
  * of them simulated for Spearman's rho; at rho >= rho_min the next
- * population is the elites plus the best-predicted offspring, otherwise
- * plain gp_step.  The decision situations come from the first generation's
+ * population is the elites plus the screened offspring (`selection`),
+ * otherwise plain gp_step.  The decision situations come from the first generation's
  * best rule.  Every fitness reported is simulated.  Per generation g:
  * best_train[g], held_out[g] (the generation's best rule on test_samples
  * scenarios from test_seed), rho[g] (NaN when not audited), gen_seconds[g]

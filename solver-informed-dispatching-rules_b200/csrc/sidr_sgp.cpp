@@ -5,6 +5,7 @@
 // correlation is too low.
 #include <chrono>
 #include <numeric>
+#include <set>
 
 #include "../../include/sidr_surrogate.h"
 #include "sidr_gp_core.hpp"
@@ -92,6 +93,7 @@ void sidr_sgp_default_config(sidr_sgp_config* c) {
     c->model_seed = 1;
     c->use_surrogate = 1;
     c->device = 0;
+    c->selection = 0;
 }
 
 sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
@@ -277,16 +279,34 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                 hist_x.push_back(aud_x);
                 hist_t.push_back(aud_fit);
                 if (r_s >= sc->rho_min) {
-                    // elites of the current population, then the best-predicted candidates
+                    // elites of the current population, then the screened offspring
                     std::vector<int> order(ps);
                     std::iota(order.begin(), order.end(), 0);
                     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return fit[a] > fit[b]; });
                     std::vector<Rule> next;
                     for (int e = 0; e < cfg->elitism && e < ps; e++) next.push_back(gp.pop[order[e]]);
-                    std::vector<int> co(cand.size());
-                    std::iota(co.begin(), co.end(), 0);
-                    std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return pred[a] > pred[b]; });
-                    for (size_t k = 0; (int)next.size() < ps && k < co.size(); k++) next.push_back(cand[co[k]]);
+                    const int need = ps - (int)next.size();
+                    if (sc->selection == 1) {
+                        // pre-selection: the best-predicted child of each group of
+                        // screen/need consecutive (independently bred) children
+                        const int per = std::max(1, (int)cand.size() / std::max(need, 1));
+                        for (int q = 0; q < need; q++) {
+                            int b = q * per;
+                            for (int c = q * per + 1; c < (q + 1) * per && c < (int)cand.size(); c++)
+                                if (pred[c] > pred[b]) b = c;
+                            next.push_back(cand[b]);
+                        }
+                    } else {
+                        // global: the best-predicted distinct children
+                        std::vector<int> co(cand.size());
+                        std::iota(co.begin(), co.end(), 0);
+                        std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return pred[a] > pred[b]; });
+                        std::set<Rule> seen;
+                        for (size_t k = 0; (int)next.size() < ps && k < co.size(); k++)
+                            if (seen.insert(cand[co[k]]).second) next.push_back(cand[co[k]]);
+                        for (size_t k = 0; (int)next.size() < ps && k < co.size(); k++)
+                            next.push_back(cand[co[k]]);  // fewer distinct children than slots
+                    }
                     gp.pop.swap(next);
                     screened_gen = true;
                     screened++;

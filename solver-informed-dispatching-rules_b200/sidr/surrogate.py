@@ -123,7 +123,8 @@ class _SgpCfg(C.Structure):
                 ("lr", C.c_float), ("audit", C.c_int32), ("rho_min", C.c_double),
                 ("history", C.c_int32), ("n_situations", C.c_int32),
                 ("capture_scenarios", C.c_int32), ("max_cand", C.c_int32),
-                ("model_seed", C.c_uint64), ("use_surrogate", C.c_int32), ("device", C.c_int32)]
+                ("model_seed", C.c_uint64), ("use_surrogate", C.c_int32), ("device", C.c_int32),
+                ("selection", C.c_int32)]
 
 
 class _SgpResult(C.Structure):
@@ -220,3 +221,36 @@ def sgp_run(ctx, terminals, mask, seed: int = 0, test_seed: int = 1000000,
             "model_seconds": res.model_seconds, "host_seconds": res.host_seconds,
             "evaluations": res.evaluations, "screened": res.generations_screened,
             "fallback": res.generations_fallback}
+
+
+def _main(argv=None) -> int:
+    """python -m sidr.surrogate [--rows R] [--steps K] [--batch B]: trains the
+    model on R random 40-feature rows for K Adam steps of B rows and prints
+    the step rate and the tensor-core GEMM throughput it implies."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(prog="python -m sidr.surrogate")
+    ap.add_argument("--rows", type=int, default=8192)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=1024)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(0)
+    x = rng.random((a.rows, INPUTS), dtype=np.float32)
+    t = (x[:, :8].sum(axis=1) - 4.0).astype(np.float32)
+    m = MLP(seed=1)
+    m.train(x, t, steps=3, batch=a.batch)  # warm-up
+    t0 = time.perf_counter()
+    loss = m.train(x, t, steps=a.steps, batch=a.batch)
+    dt = time.perf_counter() - t0
+    # GEMM FLOPs per step: forward 2B(48*256 + 256*256), backward dW2, dH1, dW1
+    flops = 2.0 * a.batch * (48 * 256 + 256 * 256) + 2.0 * a.batch * (256 * 256 * 2 + 256 * 48)
+    print(json.dumps({"steps": a.steps, "batch": a.batch, "seconds": dt,
+                      "steps_per_s": a.steps / dt, "gemm_tflops": flops * a.steps / dt / 1e12,
+                      "final_loss": loss}))
+    m.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())

@@ -615,7 +615,8 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle},
         {h.FR.data(), h.FR.size() * 8, (const void**)&I.FR},
         {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
-        {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T},
+        {h.DP.data(), h.DP.size() * 8, (const void**)&I.DP},
+        {h.CU.data(), h.CU.size() * 8, (const void**)&I.CU},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
         {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},
@@ -918,7 +919,8 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
         {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle, 0},
         {h.FR.data(), h.FR.size() * 8, (const void**)&I.FR, 0},
         {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD, 0},
-        {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T, 0},
+        {h.DP.data(), h.DP.size() * 8, (const void**)&I.DP, 0},
+        {h.CU.data(), h.CU.size() * 8, (const void**)&I.CU, 0},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord, 0},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF, 0},
         {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG, 0},
@@ -1171,7 +1173,8 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
             {h.zle.data(), h.zle.size() * 4, (const void**)&I.zle},
             {h.FR.data(), h.FR.size() * 8, (const void**)&I.FR},
             {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
-            {h.P1T.data(), h.P1T.size() * 8, (const void**)&I.P1T},
+            {h.DP.data(), h.DP.size() * 8, (const void**)&I.DP},
+            {h.CU.data(), h.CU.size() * 8, (const void**)&I.CU},
             {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
             {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
             {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},

@@ -204,7 +204,17 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
     // neighbour j) at pair index j*ld + o.
     h.FR.assign(2 * rows, 0.0);
     h.GD.assign(2 * rows, 0.0);
-    h.P1T.assign((size_t)n * n, 0.0);
+    h.DP.assign(2 * (size_t)n * n, 0.0);
+    h.CU.assign(6 * (size_t)n, 0.0);
+    for (int j = 0; j < n; j++) {
+        double* u = &h.CU[6 * (size_t)j];
+        u[0] = h.close_t[j];
+        u[1] = h.open_t[j];
+        u[2] = h.P0[j];
+        u[3] = h.durations[j];
+        u[4] = h.d2d[j];
+        u[5] = h.scores[j];
+    }
     for (int o = 0; o < ld; o++)
         for (int j = 0; j < n; j++) {
             const size_t a = (size_t)o * n + j, t = 2 * ((size_t)j * ld + o);
@@ -214,7 +224,11 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
             h.GD[t + 1] = D(h, o, j + 1);
         }
     for (int c = 0; c < n; c++)
-        for (int j = 0; j < n; j++) h.P1T[(size_t)j * n + c] = h.P1[(size_t)c * n + j];
+        for (int j = 0; j < n; j++) {
+            const size_t t = 2 * ((size_t)j * n + c);
+            h.DP[t] = D(h, c + 1, j + 1);
+            h.DP[t + 1] = h.P1[(size_t)c * n + j];
+        }
     // Per-origin neighbour lists by (R desc, index asc), rows padded to a
     // multiple of 4 entries; bit 14 of an index marks a coincident location.
     // cnt_pos / cnt_gm1 = how many leading entries have a ratio > 0 / > -1.

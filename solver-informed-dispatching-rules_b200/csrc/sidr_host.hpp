@@ -15,7 +15,8 @@ struct HostInstance {
     std::vector<double> scores, durations, open_t, close_t, d2d, dist;  // SimData arrays
     std::vector<double> F, G, R, P1, P0;                                 // lookup tables
     std::vector<uint32_t> zlt, zle;
-    std::vector<double> FR, GD, P1T;                                     // neighbour-major
+    std::vector<double> FR, GD, DP;                                      // neighbour-major
+    std::vector<double> CU;                                              // per customer
     int ns = 0;                                                          // sorted row stride
     std::vector<int16_t> ord;                                            // sorted lists
     std::vector<double> sF, sG;

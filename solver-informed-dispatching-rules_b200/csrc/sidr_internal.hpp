@@ -42,9 +42,12 @@ constexpr int kOrdCoincident = 1 << 14;       // flag bit of the sorted neighbou
 //
 // Two further layouts of the same values serve the two access patterns:
 //   * neighbour-major pair tables FR = {F, R} and GD = {G, dist[o][j+1]} at
-//     pair index j*ld + o, and P1T[j*n + c]: in the fused candidate scan all
-//     lanes visit the same neighbour j from different origins, so one warp's
-//     16-byte loads stay in one row;
+//     pair index j*ld + o, and DP = {dist[c+1][j+1], P1[c*n + j]} at pair
+//     index j*n + c: in the fused candidate scan and in ATRISK all lanes
+//     visit the same neighbour j from different origins, so one warp's
+//     16-byte loads stay in one row (ATRISK reads both of its per-pair values
+//     with one load), and CU = {close, open, P0, dur, d2d, score} per customer
+//     (three 16-byte loads for the per-customer values ATRISK's pairs read);
 //   * per-origin neighbour lists ord[o*ns + k] sorted by (R desc, index asc),
 //     rows padded to ns = a multiple of 4, with sF/sG (F and G in that order),
 //     bit 14 of ord marking coincident locations, and cnt_pos[o] / cnt_gm1[o]
@@ -59,7 +62,8 @@ struct DevInst {
     const double *scores, *durations, *open_t, *close_t, *d2d, *dist;
     const double *F, *G, *R, *P1, *P0;
     const uint32_t *zlt, *zle;
-    const double *FR, *GD, *P1T;  // FR/GD: interleaved pairs
+    const double *FR, *GD, *DP;   // interleaved pairs
+    const double* CU;              // [n][6] per-customer pack
     int ns;                        // sorted-list row stride
     const int16_t* ord;
     const double *sF, *sG;

@@ -61,7 +61,7 @@ __device__ unsigned long long sidr_section_cycles[16];
 // Shared-memory slice of one warp.
 struct WarpSmem {
     DevInst* inst;     // the rule's instance (multi-instance batches)
-    double* rows;      // [rows][32]
+    double* rows;      // [rows][32]; between rounds also ATRISK's erf queue
     double* cst;       // [const_cap]
     uint32_t* prog;    // [prog_cap]
     int16_t* cand;     // [kMaxN]
@@ -69,6 +69,7 @@ struct WarpSmem {
     uint32_t* feas;    // [kMaxWords] feasible-now & unvisited
     uint32_t* atr;     // [kMaxWords] ATRISK's arrive-by-close filter
     uint8_t* slots;    // [64] compact row -> terminal slot
+    int qcap;          // doubles in the ATRISK queue (carved rows * 32)
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -77,9 +78,16 @@ __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a -
 // closes every warp's slice.
 constexpr size_t kInstBytes = (sizeof(DevInst) + 15) / 16 * 16;
 
+// The value rows double as ATRISK's queue of erf arguments, which runs
+// before a round's terminals are written: at least kQueueRows rows
+// (kQueueRows * 16 queue entries of two doubles) are carved.
+constexpr int kQueueRows = 16;
+
+__host__ __device__ inline int carved_rows(int rows) { return rows < kQueueRows ? kQueueRows : rows; }
+
 __host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int prog_cap) {
     size_t b = kInstBytes;
-    b += (size_t)rows * 32 * sizeof(double);
+    b += (size_t)carved_rows(rows) * 32 * sizeof(double);
     b += (size_t)const_cap * sizeof(double);
     b += align_up((size_t)prog_cap * sizeof(uint32_t), 8);
     b += (size_t)kMaxN * sizeof(int16_t);
@@ -94,7 +102,7 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, int rows, int con
     s.inst = reinterpret_cast<DevInst*>(base);
     base += kInstBytes;
     s.rows = reinterpret_cast<double*>(base);
-    s.cst = s.rows + (size_t)rows * 32;
+    s.cst = s.rows + (size_t)carved_rows(rows) * 32;
     s.prog = reinterpret_cast<uint32_t*>(s.cst + const_cap);
     s.cand = reinterpret_cast<int16_t*>(
         reinterpret_cast<unsigned char*>(s.prog) + align_up((size_t)prog_cap * 4, 8));
@@ -102,6 +110,7 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, int rows, int con
     s.feas = s.unv + kMaxWords;
     s.atr = s.feas + kMaxWords;
     s.slots = reinterpret_cast<uint8_t*>(s.atr + kMaxWords);
+    s.qcap = carved_rows(rows) * 32;
     return s;
 }
 
@@ -416,11 +425,248 @@ struct WarpCounts {
     unsigned long long dec, cand, scan, heavy, hop, ops;
 };
 
+// What the ATRISK pass of one lane reads, as plain values (held in registers
+// across the out-of-line call): the per-customer pack CU, the scores, the
+// candidate's column of DP, the decision's customer set and the erf queue in
+// shared memory, and the candidate's mean finish and deviation.
+struct AtRiskView {
+    const double2* CU;      // per customer {close, open}, {P0, dur}, {d2d, score}
+    const double* scores;
+    const double2* DPc;     // DP + ci: {dist(ci, j), P1(ci, j)} at j * n
+    const uint32_t* atr;
+    double* Q;
+    int n, nw, cap, ci;
+    double tmax, fin_c, sd_c;
+};
+
+// One (candidate, customer) pair of ATRISK, classified without branches.  The
+// term is sj * (1 - p_win * p_bud).  A normal-CDF factor whose argument lies
+// at least 8.5 standard deviations from the mean is exactly 0 or 1 -- the
+// reference's erf (glibc) returns +-1 for |x| >= 6, and |d| >= 8.5 s gives
+// x >= 6.01 after both roundings -- and so is one whose deviation is
+// degenerate.  When both factors are exact the term is sj (a product of 0)
+// or +0 (a product of 1, which leaves the sum unchanged); p_bud is not
+// needed when p_win is exactly 0.  Only the rest (about 5% of pairs on the
+// benchmark workloads) need erf of (num / den) * 1/sqrt(2): ew / eb.
+struct AtRiskClass {
+    bool add;        // both factors exact and the term is sj
+    bool ew, eb;     // p_win / p_bud need erf (p_win is otherwise exactly 1 when eb)
+    bool pb1;        // p_bud exactly 1 (when ew and not eb)
+    double wnum;     // p_win's numerator (denominator sd_c)
+    double bnum, bden;
+};
+
+__device__ __forceinline__ AtRiskClass at_risk_class(const AtRiskView& v, int j, bool live,
+                                                     double hw, double lw) {
+    const int js = live ? j : 0;
+    const double2 dp = v.DPc[(size_t)js * v.n];
+    const double2* cu = v.CU + 3 * (size_t)js;
+    const double2 co = cu[0], pd = cu[1], es = cu[2];
+    const double cj = co.x, oj = co.y, p0 = pd.x, dj = pd.y, ej = es.x;
+    const double marr = v.fin_c + dp.x;
+    const double dw = cj - marr;
+    const bool sdv = v.sd_c > 1e-9;
+    const bool ew = sdv && !(dw >= hw) && !(dw <= lw);
+    const bool pw1 = sdv ? dw >= hw : marr <= cj;  // p_win exactly 1, when not ew
+    const bool late = marr > oj;
+    const double mst = late ? marr : oj;
+    const double pv = late ? dp.y : p0;
+    const double mb = mst + dj + ej;
+    const double db = v.tmax - mb;
+    const bool pvv = pv >= 0.0;
+    const double hb = 8.5 * pv, lb = -8.5 * pv;
+    const bool eb = (ew || pw1) && pvv && !(db >= hb) && !(db <= lb);
+    AtRiskClass c;
+    c.pb1 = pvv ? db >= hb : mb <= v.tmax;
+    c.ew = live && ew;
+    c.eb = live && eb;
+    c.add = live && !ew && !eb && !(pw1 && c.pb1);
+    c.wnum = dw;
+    c.bnum = db;
+    c.bden = pv;
+    return c;
+}
+
+__device__ __forceinline__ double norm_cdf_ratio(double num, double den) {
+    return 0.5 * (1.0 + libm::erf_((num / den) * 0.7071067811865476));
+}
+
+constexpr int kAtRiskUnroll = 2;
+
+// ATRISK (t_eloss_chance, engine/sim_terms.hpp:225-257) of each lane's
+// candidate v.ci (-1: the lane has none), called by the whole warp at the
+// start of a scoring round.  The reference adds the terms of the unvisited
+// customers j != ci that can still be reached before their close in
+// ascending j; that set (S.atr) is the decision's, so every lane walks the
+// same list, the per-customer loads are broadcasts and the lanes' pair loads
+// fall in one row of DP.  The list is taken 32 customers (one word) at a
+// time.  Pass 1 classifies the word's pairs, kAtRiskUnroll independent ones
+// per step, into per-lane bit masks, and queues the (numerator,
+// denominator) of every erf argument warp-wide in the value rows; the warp
+// evaluates the queue 32 entries at a time; pass 2 adds the terms in order
+// from the masks, the word's scores (one per lane, shuffled) and the queue
+// (positions from the same ballots).  A word whose arguments overflow the
+// queue is added by at_risk_word_direct.
+template <bool COUNT>
+__device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc);
+
+// The pairs of word w of the customer set in ascending order, one at a
+// time with erf inline: the path of a word whose erf arguments overflow the
+// queue.  Returns eloss with the word's terms added.
+__device__ __noinline__ double at_risk_word_direct(const AtRiskView v, int w, uint32_t word,
+                                                   double eloss) {
+    const double hw = 8.5 * v.sd_c, lw = -8.5 * v.sd_c;
+    for (uint32_t bits = word; bits;) {
+        const int j = (w << 5) + __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (v.ci < 0 || j == v.ci) continue;
+        const AtRiskClass c = at_risk_class(v, j, true, hw, lw);
+        const double sj = v.scores[j];
+        if (c.add) {
+            eloss += sj;
+        } else if (c.ew || c.eb) {
+            const double fw = c.ew ? norm_cdf_ratio(c.wnum, v.sd_c) : 1.0;
+            const double fb = c.eb ? norm_cdf_ratio(c.bnum, c.bden) : (c.pb1 ? 1.0 : 0.0);
+            eloss += sj * (1.0 - fw * fb);
+        }
+    }
+    return eloss;
+}
+
+template <bool COUNT>
+__device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
+    constexpr int U = kAtRiskUnroll;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const double hw = 8.5 * v.sd_c, lw = -8.5 * v.sd_c;
+    const bool has = v.ci >= 0;
+    double* const Q = v.Q;
+    double eloss = 0.0;
+    unsigned long long heavy = 0;
+
+    for (int w = 0; w < v.nw; w++) {
+        const uint32_t word = v.atr[w];
+        if (word == 0) continue;
+        const uint32_t own = has ? bit_in_word(v.ci, w) : 0u;
+        if (COUNT && has) heavy += __popc(word & ~own);
+        __syncwarp();  // the previous word's queue reads are done
+        uint32_t addm = 0, ewm = 0, ebm = 0, pbm = 0;
+        int qn = 0;
+        for (uint32_t bits = word; bits;) {
+            int b[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                b[u] = bits ? __ffs(bits) - 1 : -1;
+                bits &= bits - 1;
+            }
+            AtRiskClass c[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool live = has && b[u] >= 0 && !((own >> (b[u] & 31)) & 1u);
+                c[u] = at_risk_class(v, (w << 5) + b[u], live, hw, lw);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (b[u] < 0) break;  // warp-uniform
+                const uint32_t m = 1u << b[u];
+                addm |= c[u].add ? m : 0u;
+                ewm |= c[u].ew ? m : 0u;
+                ebm |= c[u].eb ? m : 0u;
+                pbm |= c[u].pb1 ? m : 0u;
+                const uint32_t bw = __ballot_sync(kFull, c[u].ew);
+                const uint32_t bb = __ballot_sync(kFull, c[u].eb);
+                const int pw = qn + __popc(bw & lt);
+                qn += __popc(bw);
+                const int pb = qn + __popc(bb & lt);
+                qn += __popc(bb);
+                if (c[u].ew && pw < v.cap) {
+                    Q[2 * pw] = c[u].wnum;
+                    Q[2 * pw + 1] = v.sd_c;
+                }
+                if (c[u].eb && pb < v.cap) {
+                    Q[2 * pb] = c[u].bnum;
+                    Q[2 * pb + 1] = c[u].bden;
+                }
+            }
+        }
+        if (qn > v.cap) {  // warp-uniform
+            eloss = at_risk_word_direct(v, w, word, eloss);
+            continue;
+        }
+        if (qn) {
+            __syncwarp();
+            for (int k = lane; k < qn; k += 32) Q[2 * k] = norm_cdf_ratio(Q[2 * k], Q[2 * k + 1]);
+            __syncwarp();
+        }
+        const int jl = (w << 5) + lane;
+        const double sw = jl < v.n ? v.scores[jl] : 0.0;
+        const uint32_t anym = addm | ewm | ebm;
+        qn = 0;
+        for (uint32_t bits = word; bits;) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const uint32_t m = 1u << b;
+            const double sj = __shfl_sync(kFull, sw, b);
+            const bool ew = (ewm & m) != 0, eb = (ebm & m) != 0;
+            const uint32_t bw = __ballot_sync(kFull, ew);
+            const uint32_t bb = __ballot_sync(kFull, eb);
+            const int pw = qn + __popc(bw & lt);
+            qn += __popc(bw);
+            const int pb = qn + __popc(bb & lt);
+            qn += __popc(bb);
+            if (anym & m) {
+                if (addm & m) {
+                    eloss += sj;
+                } else {
+                    const double fw = ew ? Q[2 * pw] : 1.0;
+                    const double fb = eb ? Q[2 * pb] : ((pbm & m) ? 1.0 : 0.0);
+                    eloss += sj * (1.0 - fw * fb);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (COUNT) {
+        wc.heavy += heavy;
+        wc.ops += heavy * kOpsAtRisk;
+    }
+    return eloss;
+}
+
+// The view of lane's candidate ci (-1: none) at decision d.
+__device__ __forceinline__ AtRiskView at_risk_view(const DevInst& I, const WarpSmem& S,
+                                                   const Decision& d, int ci) {
+    AtRiskView v;
+    v.CU = reinterpret_cast<const double2*>(I.CU);
+    v.scores = I.scores;
+    v.DPc = reinterpret_cast<const double2*>(I.DP);
+    v.atr = S.atr;
+    v.Q = S.rows;
+    v.n = I.n;
+    v.nw = I.nw;
+    v.cap = S.qcap / 2;
+    v.ci = ci;
+    v.tmax = I.tmax;
+    v.fin_c = 0.0;
+    v.sd_c = 0.0;
+    if (ci >= 0) {
+        const double ta = I.dist[(size_t)d.cur * I.ld + ci + 1];
+        const double open_i = I.open_t[ci], dur_i = I.durations[ci];
+        const double arr_c = d.ct + ta;
+        const double st_c = arr_c > open_i ? arr_c : open_i;
+        v.fin_c = st_c + dur_i;
+        v.sd_c = kSigma * dur_i;
+        v.DPc += ci;
+    }
+    return v;
+}
+
 // Terminals of candidate i into the lane's value rows, then the rule program.
-// Returns the priority (NaN mapped to -1e300).
+// Returns the priority (NaN mapped to -1e300).  eloss: the candidate's ATRISK
+// value (at_risk), when the rule reads it.
 template <bool COUNT>
 __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
-                                  const Decision& d, int i, WarpCounts& wc) {
+                                  const Decision& d, int i, double eloss, WarpCounts& wc) {
     const int lane = threadIdx.x & 31;
     const int n = I.n, ld = I.ld;
     const uint32_t need = rm.need;
@@ -441,11 +687,10 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
     const double st_c = arr_c > open_i ? arr_c : open_i;
     const double fin_c = st_c + dur_i;           // finish_c of the cascade family
     const double frob = fin + dur_i * kSigma;    // robust finish
-    const double sd_c = kSigma * dur_i;
     if (COUNT) wc.ops += kOpsCandidate + rm.n_ins;
 
     double ns = 0.0, maxn = 0.0, r2v = 0.0, nstw = 0.0, regret = 0.0, nsrob = 0.0, r2rv = 0.0;
-    double fcnt = 0.0, fsc = 0.0, smin = 1e18, sbv = -1.0, k1v = -1.0, eloss = 0.0;
+    double fcnt = 0.0, fsc = 0.0, smin = 1e18, sbv = -1.0, k1v = -1.0;
     int r2j = -1, r2rj = -1, sbq = -1, k1q = -1;
 
     SIDR_SEC_ADD(2, t_setup);
@@ -556,67 +801,6 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         if (COUNT) {
             wc.scan += scan;
             wc.ops += scan * rm.scan_ops;
-        }
-    }
-
-    // ATRISK (engine/sim_terms.hpp:225-257) in its own ascending pass over the
-    // customers reachable before their close: its erf calls run outside the
-    // register-heavy fused scan.
-    if (need & kNeedAtRisk) {
-        const double2* GDa = reinterpret_cast<const double2*>(I.GD) + (i + 1);
-        const double* P1i = I.P1T + i;
-        unsigned long long heavy = 0;
-        for (int w = 0; w < I.nw; w++) {
-            uint32_t bits = S.atr[w] & ~bit_in_word(i, w);
-            while (bits) {
-                const int b = __ffs(bits) - 1;
-                bits &= bits - 1;
-                const int j = (w << 5) + b;
-                const double sj = I.scores[j];
-                if (COUNT) heavy++;
-                const double cj = I.close_t[j], oj = I.open_t[j];
-                const double marr = fin_c + GDa[(size_t)j * ld].y;
-                // norm_cdf(d/s) = 0.5*(1 + erf((d/s)*0.7071067811865476)).  The
-                // reference's erf (glibc) is exactly +-1 for |x| >= 6, so for
-                // |d| >= 8.5 s (x >= 6.01 after both roundings) the result is 1
-                // or 0 with no erf call.
-                double pw;
-                const double dw = cj - marr;
-                if (sd_c > 1e-9) {
-                    if (dw >= 8.5 * sd_c) pw = 1.0;
-                    else if (dw <= -8.5 * sd_c) pw = 0.0;
-                    else pw = 0.5 * (1.0 + libm::erf_((dw / sd_c) * 0.7071067811865476));
-                } else {
-                    pw = marr <= cj ? 1.0 : 0.0;
-                }
-                if (pw == 0.0) {
-                    eloss += sj * 1.0;  // sj * (1.0 - 0.0 * p_bud), p_bud finite
-                } else {
-                    double mst, pv;
-                    if (marr > oj) {
-                        mst = marr;
-                        pv = P1i[(size_t)j * n];
-                    } else {
-                        mst = oj;
-                        pv = I.P0[j];
-                    }
-                    const double mb = mst + I.durations[j] + I.d2d[j];
-                    double pb;
-                    if (pv >= 0.0) {
-                        const double db = tmax - mb;
-                        if (db >= 8.5 * pv) pb = 1.0;
-                        else if (db <= -8.5 * pv) pb = 0.0;
-                        else pb = 0.5 * (1.0 + libm::erf_((db / pv) * 0.7071067811865476));
-                    } else {
-                        pb = mb <= tmax ? 1.0 : 0.0;
-                    }
-                    eloss += sj * (1.0 - pw * pb);
-                }
-            }
-        }
-        if (COUNT) {
-            wc.heavy += heavy;
-            wc.ops += heavy * kOpsAtRisk;
         }
     }
 
@@ -891,9 +1075,11 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         const int k = base + lane;
         double pri = -1e300;
         int idx = 0x7fffffff;
+        const double eloss =
+            need_atr ? at_risk<COUNT>(at_risk_view(I, S, d, k < ncand ? S.cand[k] : -1), wc) : 0.0;
         if (k < ncand) {
             idx = S.cand[k];
-            pri = score_candidate<COUNT>(I, S, rm, d, idx, wc);
+            pri = score_candidate<COUNT>(I, S, rm, d, idx, eloss, wc);
             if (CAPTURE && cap.slot >= 0 && k < cap.C->cand) {
                 const CaptureBuf& C = *cap.C;
                 const size_t at = (size_t)cap.slot * C.cand + k;

@@ -620,6 +620,8 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
         {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},
+        {h.bF.data(), h.bF.size() * 8, (const void**)&I.bF},
+        {h.bG.data(), h.bG.size() * 8, (const void**)&I.bG},
         {h.cnt_pos.data(), h.cnt_pos.size() * 4, (const void**)&I.cnt_pos},
         {h.cnt_gm1.data(), h.cnt_gm1.size() * 4, (const void**)&I.cnt_gm1},
         {zp, 80, (const void**)&I.zp},
@@ -924,6 +926,8 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord, 0},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF, 0},
         {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG, 0},
+        {h.bF.data(), h.bF.size() * 8, (const void**)&I.bF, 0},
+        {h.bG.data(), h.bG.size() * 8, (const void**)&I.bG, 0},
         {h.cnt_pos.data(), h.cnt_pos.size() * 4, (const void**)&I.cnt_pos, 0},
         {h.cnt_gm1.data(), h.cnt_gm1.size() * 4, (const void**)&I.cnt_gm1, 0},
         {zp, 80, (const void**)&I.zp, 0},
@@ -1178,6 +1182,8 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
             {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
             {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
             {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},
+            {h.bF.data(), h.bF.size() * 8, (const void**)&I.bF},
+            {h.bG.data(), h.bG.size() * 8, (const void**)&I.bG},
             {h.cnt_pos.data(), h.cnt_pos.size() * 4, (const void**)&I.cnt_pos},
             {h.cnt_gm1.data(), h.cnt_gm1.size() * 4, (const void**)&I.cnt_gm1},
             {zps + 10 * (size_t)k, 80, (const void**)&I.zp},

@@ -255,6 +255,22 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
             if (Ro[j] > -1.0) h.cnt_gm1[o] = k + 1;
         }
     }
+    const int nc = h.ns / 4;
+    h.bF.assign(2 * (size_t)ld * nc, -INFINITY);
+    h.bG.assign(2 * (size_t)ld * nc, -INFINITY);
+    for (int o = 0; o < ld; o++)
+        for (int pass = 0; pass < 2; pass++) {
+            const double* src = (pass ? h.sG : h.sF).data() + (size_t)o * h.ns;
+            double* dst = (pass ? h.bG : h.bF).data() + 2 * (size_t)o * nc;
+            double suffix = -INFINITY;
+            for (int c = nc - 1; c >= 0; c--) {
+                double mx = -INFINITY;
+                for (int e = 0; e < 4; e++) mx = src[4 * c + e] > mx ? src[4 * c + e] : mx;
+                suffix = mx > suffix ? mx : suffix;
+                dst[2 * c] = mx;
+                dst[2 * c + 1] = suffix;
+            }
+        }
     return "";
 }
 

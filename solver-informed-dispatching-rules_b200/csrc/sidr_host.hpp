@@ -20,6 +20,7 @@ struct HostInstance {
     int ns = 0;                                                          // sorted row stride
     std::vector<int16_t> ord;                                            // sorted lists
     std::vector<double> sF, sG;
+    std::vector<double> bF, bG;                                          // chunk maxima
     std::vector<int32_t> cnt_pos, cnt_gm1;
 };
 

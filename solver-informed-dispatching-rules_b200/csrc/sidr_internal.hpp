@@ -55,7 +55,11 @@ constexpr int kOrdCoincident = 1 << 14;       // flag bit of the sorted neighbou
 //     "best feasible neighbour by ratio" search -- strict > over ascending
 //     index from an initial best of 0 or -1, as in REACH2's second hop and
 //     REACH-k -- returns the first feasible entry among those, so it stops
-//     early.
+//     early.  bF / bG hold, per row and chunk of 4 entries, {the largest sF
+//     / sG of the chunk, the largest of the chunk and every later one}: a
+//     search at time tm skips a chunk whose largest threshold is below tm
+//     (no entry of it passes tm <= threshold) and stops at a chunk whose
+//     suffix maximum is.
 struct DevInst {
     int n, m, ld, nw;
     double tmax;
@@ -67,6 +71,7 @@ struct DevInst {
     int ns;                        // sorted-list row stride
     const int16_t* ord;
     const double *sF, *sG;
+    const double *bF, *bG;         // [ld][ns/4] {chunk max, suffix max}
     const int32_t *cnt_pos, *cnt_gm1;
     const double* zp;  // [10]
 };

@@ -163,20 +163,27 @@ __device__ __forceinline__ Chunk4 load_chunk(const double* sT, const int16_t* or
 // REACH2's second loop (engine/sim_terms.hpp:112-126, robust :175-189): the
 // best unvisited customer outside {x0, x1} by score/time from origin node o at
 // time tm, skipping coincident locations, init 0.0.  `table` is sF (standard)
-// or sG (robust).  The argmax with strict > over ascending index is the first
-// feasible entry among the cnt_pos[o] leading entries of o's sorted list (those
-// whose ratio exceeds 0.0).  Returns the chosen customer's score, or 0.0.
+// or sG (robust), `bmax` its chunk maxima bF / bG.  The argmax with strict >
+// over ascending index is the first feasible entry among the cnt_pos[o]
+// leading entries of o's sorted list (those whose ratio exceeds 0.0); chunks
+// whose thresholds are all below tm hold none.  Returns the chosen customer's
+// score, or 0.0.
 template <bool COUNT>
 __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const double* table,
-                                   int o, double tm, int x0, int x1, unsigned long long& hops) {
+                                   const double* bmax, int o, double tm, int x0, int x1,
+                                   unsigned long long& hops) {
     const size_t row = (size_t)o * I.ns;
     const int16_t* ord = I.ord + row;
     const double* sT = table + row;
+    const double2* bm = reinterpret_cast<const double2*>(bmax) + row / 4;
     const int cnt = I.cnt_pos[o];
     double res = 0.0;
     // The scan leaves both loops by flags rather than returning from inside
     // the unrolled body, which keeps the warp's exit point single.
     for (int k = 0; k < cnt; k += 4) {
+        const double2 mx = bm[k >> 2];
+        if (tm > mx.y) break;
+        if (tm > mx.x) continue;
         const Chunk4 c = load_chunk(sT, ord, k);
         bool hit = false;
 #pragma unroll
@@ -198,16 +205,21 @@ __device__ double second_hop_score(const DevInst& I, const WarpSmem& S, const do
 // One REACH-k greedy step (engine/sim_terms.hpp:415-431): the best unvisited
 // customer outside the walk by score/max(t,1e-10) under the standard test, no
 // coincident skip, init -1.0 -- the first feasible entry among the cnt_gm1[o]
-// leading entries of o's sorted list.  p0..p4: the walk so far (-1 = unused).
+// leading entries of o's sorted list (chunks skipped as in second_hop_score).
+// p0..p4: the walk so far (-1 = unused).
 template <bool COUNT>
 __device__ int reach_step(const DevInst& I, const WarpSmem& S, int o, double tm, int p0, int p1,
                           int p2, int p3, int p4, unsigned long long& hops) {
     const size_t row = (size_t)o * I.ns;
     const int16_t* ord = I.ord + row;
     const double* sF = I.sF + row;
+    const double2* bm = reinterpret_cast<const double2*>(I.bF) + row / 4;
     const int cnt = I.cnt_gm1[o];
     int res = -1;
     for (int k = 0; k < cnt; k += 4) {
+        const double2 mx = bm[k >> 2];
+        if (tm > mx.y) break;
+        if (tm > mx.x) continue;
         const Chunk4 c = load_chunk(sF, ord, k);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
@@ -812,13 +824,13 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         const double arrive = fin + I.dist[(size_t)(i + 1) * ld + r2j + 1];
         const double st = arrive > I.open_t[r2j] ? arrive : I.open_t[r2j];
         const double fj = st + I.durations[r2j];
-        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.sF, r2j + 1, fj, i, r2j, wc.hop);
+        reach2 = I.scores[r2j] + second_hop_score<COUNT>(I, S, I.sF, I.bF, r2j + 1, fj, i, r2j, wc.hop);
     }
     if ((need & kNeedReach2Rob) && r2rj >= 0) {
         const double arrive = frob + I.dist[(size_t)(i + 1) * ld + r2rj + 1];
         const double st = arrive > I.open_t[r2rj] ? arrive : I.open_t[r2rj];
         const double fj = st + I.durations[r2rj] * (1.0 + kSigma);
-        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.sG, r2rj + 1, fj, i, r2rj, wc.hop);
+        reach2rob = I.scores[r2rj] + second_hop_score<COUNT>(I, S, I.sG, I.bG, r2rj + 1, fj, i, r2rj, wc.hop);
     }
 
     // REACH-1/3/5 share one greedy path (each is the running total after

@@ -30,12 +30,15 @@ namespace sidr {
 constexpr unsigned kFull = 0xffffffffu;
 
 // Block shape of the evaluator: warps per block and the minimum resident
-// blocks per SM that bound its registers (__launch_bounds__).
+// blocks per SM that bound its registers (__launch_bounds__).  The kernel is
+// latency-bound (dependent FP64 chains and L1-missing table loads), so 16
+// warps per SM at 128 registers, with a few spills, beat 12 at 168 and 20 at
+// 96 (measured on gp-generation and evolved populations).
 #ifndef SIDR_WARPS_PER_BLOCK
 #define SIDR_WARPS_PER_BLOCK 4
 #endif
 #ifndef SIDR_MIN_BLOCKS
-#define SIDR_MIN_BLOCKS 3
+#define SIDR_MIN_BLOCKS 4
 #endif
 
 // Section-cycle hooks for profiling builds only (-DSIDR_SECTION_CLOCKS): the

@@ -70,6 +70,9 @@ def parse_args():
                          "instance (population 1024, 500 training scenarios, screening 8192 "
                          "offspring per generation) and report wall clock to equal held-out fitness")
     ap.add_argument("--sgp-generations", type=int, default=50)
+    ap.add_argument("--sgp-ablation", action="store_true",
+                    help="with --sgp: also run the surrogate arms that change one screening "
+                         "setting each (about 3 minutes per arm)")
     ap.add_argument("--campaign", action="store_true",
                     help="also time the reference campaign's c101 generation trace (30 seeds x "
                          "1024 rules x 51 generations + held-out) and its vocabulary GA's first "
@@ -473,22 +476,34 @@ def campaign_leg():
 
 
 def sgp_leg(ctx, w, args):
-    """Surrogate-assisted GP vs plain GP through the same driver (the plain arm
-    breeds with gp_step every generation; the surrogate arms keep the
-    best-predicted distinct offspring overall, or pre-select the best of each
-    group of 8): every run records each generation's
-    best rule on the held-out 500 scenarios and the wall clock; the result is
-    the time each run needs to reach the plain run's final held-out score
-    (within 0.5 %)."""
+    """Surrogate-assisted GP vs plain GP through the same driver.  The plain
+    arm breeds with gp_step every generation; the "surrogate" arm (the
+    driver's defaults) trains the model on rank scores and fills the
+    non-elite slots of a screened generation with the best-predicted
+    offspring, one per ranking of the decision situations.  --sgp-ablation
+    adds arms that change one setting each: one child per distinct rule
+    ("rule_distinct"), that plus standardised fitness targets
+    ("standardised"), the best-predicted of each group of 8 offspring
+    ("preselection"), half the slots bred plainly ("half_screened").  Every run records
+    each generation's best rule on the held-out 500 scenarios and the wall
+    clock; the result is the time each run needs to reach the plain run's
+    final held-out score (within 0.5 %), as a ratio to the plain run's own
+    time to that score and to the plain run's whole wall clock."""
     from sidr import surrogate as SG
     from sidr.workload import MENU29
     G = args.sgp_generations
     cfg = dict(population=args.P, generations=G, train_samples=args.S, test_samples=500)
-    plain = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=0)
-    sgp = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=1)
-    pre = SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, use_surrogate=1,
-                     selection=1)
+    arms = {"plain": dict(use_surrogate=0), "surrogate": dict(use_surrogate=1)}
+    if args.sgp_ablation:
+        arms.update({"rule_distinct": dict(use_surrogate=1, distinct=0),
+                     "standardised": dict(use_surrogate=1, distinct=0, target=0),
+                     "preselection": dict(use_surrogate=1, selection=1),
+                     "half_screened": dict(use_surrogate=1, screen_fraction=0.5)})
+    runs = {k: SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, **kw)
+            for k, kw in arms.items()}
+    plain = runs["plain"]
     target = plain["held_out"][-1] * (1.0 - 0.005)
+    plain_total = float(plain["seconds"][-1])
 
     def first_time(r):
         for g in range(G):
@@ -496,21 +511,23 @@ def sgp_leg(ctx, w, args):
                 return float(r["seconds"][g]), g
         return None, None
 
-    tp, gp_ = first_time(plain)
-    ts, gs = first_time(sgp)
-    tq, gq = first_time(pre)
-    summary = lambda r: {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in r.items()}  # noqa: E731
-    return {"generations": G, "population": args.P, "train_scenarios": args.S,
-            "plain_final_held_out": float(plain["held_out"][-1]),
-            "surrogate_final_held_out": float(sgp["held_out"][-1]),
-            "target_held_out": target,
-            "plain_seconds_to_target": tp, "plain_generation_at_target": gp_,
-            "surrogate_seconds_to_target": ts, "surrogate_generation_at_target": gs,
-            "time_ratio": (ts / tp) if (ts is not None and tp) else None,
-            "preselection_final_held_out": float(pre["held_out"][-1]),
-            "preselection_seconds_to_target": tq, "preselection_generation_at_target": gq,
-            "preselection_time_ratio": (tq / tp) if (tq is not None and tp) else None,
-            "plain": summary(plain), "surrogate": summary(sgp), "preselection": summary(pre)}
+    tp, _ = first_time(plain)
+    out = {"generations": G, "population": args.P, "train_scenarios": args.S,
+           "target_held_out": target, "plain_wall_seconds": plain_total}
+    for k, r in runs.items():
+        t, g = first_time(r)
+        out[k] = {"final_held_out": float(r["held_out"][-1]),
+                  "best_held_out": float(max(r["held_out"])),
+                  "seconds_to_target": t, "generation_at_target": g,
+                  "ratio_to_plain_time_to_target": (t / tp) if (t is not None and tp) else None,
+                  "ratio_to_plain_wall": (t / plain_total) if t is not None else None,
+                  "wall_seconds": float(r["seconds"][-1]), "eval_seconds": r["eval_seconds"],
+                  "model_seconds": r["model_seconds"], "screened": r["screened"],
+                  "fallback": r["fallback"],
+                  "held_out": [float(v) for v in r["held_out"]],
+                  "seconds": [float(v) for v in r["seconds"]],
+                  "rho": [None if v != v else float(v) for v in r["rho"]]}
+    return out
 
 
 def gp_leg(ctx, w, args):

@@ -104,7 +104,17 @@ typedef struct sidr_sgp_config {
     int32_t device;            /* [0] device of the model and of the phenotype kernel */
     int32_t selection;         /* [0] 0: the best-predicted distinct offspring overall;
                                   1: pre-selection, the best-predicted of each group of
-                                  screen / (population - elites) consecutive offspring */
+                                  screen / (slots screened) consecutive offspring */
+    int32_t target;            /* [1] what the model is trained on: 0 the simulated fitness
+                                  standardised over the history; 1 its ranks over the
+                                  history as uniform scores (mean 0, variance 1), which
+                                  keeps the order and drops the skew of broken rules */
+    double screen_fraction;    /* [1.0] share of the non-elite slots filled by screened
+                                  offspring in a screened generation; the rest are bred
+                                  plainly (gp_step's loop), which keeps diversity */
+    int32_t distinct;          /* [1] selection 0 keeps one child per 0: rule; 1: ranking of
+                                  the decision situations (phenotype), so near-clones of one
+                                  behaviour do not fill the population */
 } sidr_sgp_config;
 
 void sidr_sgp_default_config(sidr_sgp_config* cfg);
@@ -120,11 +130,12 @@ typedef struct sidr_sgp_result {
 /* A GP run (engine/gp.hpp semantics, Mt19937(seed), train blocks of
  * cfg->train_samples scenarios from base seed seed*10000+gen) whose
  * offspring are pre-screened: each generation the model is trained on the
- * last `history` generations' simulated fitness (standardised), `screen`
+ * last `history` generations' simulated fitness (`target`), `screen`
  * offspring are bred by gp_step's loop, their phenotypes predicted, `audit`
  * of them simulated for Spearman's rho; at rho >= rho_min the next
- * population is the elites plus the screened offspring (`selection`),
- * otherwise plain gp_step.  The decision situations come from the first generation's
+ * population is the elites plus the screened offspring (`selection`) in
+ * `screen_fraction` of the remaining slots and plainly bred offspring in the
+ * rest, otherwise plain gp_step.  The decision situations come from the first generation's
  * best rule.  Every fitness reported is simulated.  Per generation g:
  * best_train[g], held_out[g] (the generation's best rule on test_samples
  * scenarios from test_seed), rho[g] (NaN when not audited), gen_seconds[g]

@@ -94,6 +94,9 @@ void sidr_sgp_default_config(sidr_sgp_config* c) {
     c->use_surrogate = 1;
     c->device = 0;
     c->selection = 0;
+    c->target = 1;
+    c->screen_fraction = 1.0;
+    c->distinct = 1;
 }
 
 sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
@@ -109,6 +112,9 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
     if (sc->screen < cfg->population || sc->audit < 3 || sc->history < 1 || sc->batch < 1 ||
         sc->capture_scenarios < 1 || sc->max_cand < 2 || cfg->test_samples < 1)
         return gp_fail(SIDR_ERR_INVALID, "surrogate settings out of range");
+    if (sc->selection < 0 || sc->selection > 1 || sc->target < 0 || sc->target > 1 ||
+        !(sc->screen_fraction >= 0.0 && sc->screen_fraction <= 1.0) || sc->distinct < 0 || sc->distinct > 1)
+        return gp_fail(SIDR_ERR_INVALID, "selection, target, screen_fraction or distinct out of range");
     std::vector<std::string> terms;
     if (!parse_terminals(terminals_csv, terms, err)) return gp_fail(SIDR_ERR_INVALID, err);
     const int n = inst->n, ps = cfg->population, T = cfg->train_samples, G = cfg->generations;
@@ -231,22 +237,25 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                     hist_x.erase(hist_x.begin());
                     hist_t.erase(hist_t.begin());
                 }
-                // train on the recent simulated fitness, standardised
+                // train on the recent simulated fitness: standardised, or as
+                // uniform scores of its ranks over the whole history
                 std::vector<float> X, Y;
-                double mu = 0, sd = 0;
-                size_t cnt = 0;
-                for (auto& t : hist_t)
-                    for (double v : t) {
-                        mu += v;
-                        cnt++;
-                    }
-                mu /= cnt;
-                for (auto& t : hist_t)
-                    for (double v : t) sd += (v - mu) * (v - mu);
-                sd = std::sqrt(sd / cnt) + 1e-9;
+                std::vector<double> all;
                 for (size_t h = 0; h < hist_x.size(); h++) {
                     X.insert(X.end(), hist_x[h].begin(), hist_x[h].end());
-                    for (double v : hist_t[h]) Y.push_back((float)((v - mu) / sd));
+                    all.insert(all.end(), hist_t[h].begin(), hist_t[h].end());
+                }
+                const double cnt = (double)all.size();
+                if (sc->target == 1) {
+                    const std::vector<double> rk = ranks_of(all);
+                    for (double r : rk) Y.push_back((float)(((r + 0.5) / cnt - 0.5) * std::sqrt(12.0)));
+                } else {
+                    double mu = 0, sd = 0;
+                    for (double v : all) mu += v;
+                    mu /= cnt;
+                    for (double v : all) sd += (v - mu) * (v - mu);
+                    sd = std::sqrt(sd / cnt) + 1e-9;
+                    for (double v : all) Y.push_back((float)((v - mu) / sd));
                 }
                 float loss = 0.0f;
                 double t0 = now_s();
@@ -285,7 +294,8 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return fit[a] > fit[b]; });
                     std::vector<Rule> next;
                     for (int e = 0; e < cfg->elitism && e < ps; e++) next.push_back(gp.pop[order[e]]);
-                    const int need = ps - (int)next.size();
+                    const int slots = ps - (int)next.size();
+                    const int need = (int)std::lround(sc->screen_fraction * slots);
                     if (sc->selection == 1) {
                         // pre-selection: the best-predicted child of each group of
                         // screen/need consecutive (independently bred) children
@@ -297,15 +307,35 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                             next.push_back(cand[b]);
                         }
                     } else {
-                        // global: the best-predicted distinct children
+                        // global: the best-predicted distinct children (distinct
+                        // rules, or distinct rankings of the decision situations)
                         std::vector<int> co(cand.size());
                         std::iota(co.begin(), co.end(), 0);
                         std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return pred[a] > pred[b]; });
                         std::set<Rule> seen;
-                        for (size_t k = 0; (int)next.size() < ps && k < co.size(); k++)
-                            if (seen.insert(cand[co[k]]).second) next.push_back(cand[co[k]]);
-                        for (size_t k = 0; (int)next.size() < ps && k < co.size(); k++)
-                            next.push_back(cand[co[k]]);  // fewer distinct children than slots
+                        std::set<std::vector<float>> seen_ph;
+                        std::vector<char> taken(cand.size(), 0);
+                        const size_t upto = next.size() + (size_t)need;
+                        for (size_t k = 0; next.size() < upto && k < co.size(); k++) {
+                            const int c = co[k];
+                            const bool fresh =
+                                sc->distinct == 1
+                                    ? seen_ph.insert(std::vector<float>(cf.begin() + (size_t)c * NF,
+                                                                        cf.begin() + (size_t)c * NF + NS))
+                                          .second
+                                    : seen.insert(cand[c]).second;
+                            if (fresh) {
+                                next.push_back(cand[c]);
+                                taken[c] = 1;
+                            }
+                        }
+                        for (size_t k = 0; next.size() < upto && k < co.size(); k++)
+                            if (!taken[co[k]]) next.push_back(cand[co[k]]);  // fewer distinct children than slots
+                    }
+                    if ((int)next.size() < ps) {
+                        // the slots left to plain breeding
+                        std::vector<Rule> plain = gp.breed(fit, (size_t)(ps - (int)next.size()));
+                        for (Rule& r : plain) next.push_back(std::move(r));
                     }
                     gp.pop.swap(next);
                     screened_gen = true;

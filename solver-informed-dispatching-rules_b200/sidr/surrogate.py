@@ -124,7 +124,8 @@ class _SgpCfg(C.Structure):
                 ("history", C.c_int32), ("n_situations", C.c_int32),
                 ("capture_scenarios", C.c_int32), ("max_cand", C.c_int32),
                 ("model_seed", C.c_uint64), ("use_surrogate", C.c_int32), ("device", C.c_int32),
-                ("selection", C.c_int32)]
+                ("selection", C.c_int32), ("target", C.c_int32), ("screen_fraction", C.c_double),
+                ("distinct", C.c_int32)]
 
 
 class _SgpResult(C.Structure):

@@ -152,6 +152,29 @@ def test_surrogate_run_reports_simulated_fitness(setup):
     assert res2["screened"] == 0 and res2["fallback"] == 4
 
 
+def test_mixed_screening_with_rank_targets(setup):
+    """Half the slots screened (one child per situation ranking), the model
+    trained on rank scores: every generation is screened, the reported
+    fitness is still simulated, and settings out of range are refused."""
+    w, ctx = setup
+    cfg = dict(population=64, generations=4, train_samples=4, test_samples=16)
+    res = SG.sgp_run(ctx, workload.MENU29, w.mask, seed=5, test_seed=556, gp=cfg, screen=512,
+                     audit=32, train_steps=30, batch=128, rho_min=-1.0, capture_scenarios=4,
+                     target=1, screen_fraction=0.5, distinct=1)
+    assert res["screened"] == 3 and res["fallback"] == 0
+    rule = R.pack([res["best_rule"]])
+    test = GP.gen_durations(w.sd.durations, 0.2, 16, 556)
+    out = ctx.evaluate(rule, test, 16, w.mask)[0]
+    acc = 0.0
+    for v in out:
+        acc += float(v)
+    assert acc / 16 == res["held_out"][-1]
+    for bad in (dict(screen_fraction=1.5), dict(target=2), dict(selection=3), dict(distinct=2)):
+        with pytest.raises(sidr.SidrError):
+            SG.sgp_run(ctx, workload.MENU29, w.mask, seed=5, test_seed=556, gp=cfg, screen=512,
+                       audit=32, **bad)
+
+
 def test_screening_gain_over_random_offspring(setup):
     """Train the model on three simulated generations of one GP run, then
     take 4096 offspring bred by four other runs (their third generation):

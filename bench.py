@@ -70,6 +70,7 @@ def parse_args():
                          "instance (population 1024, 500 training scenarios, screening 8192 "
                          "offspring per generation) and report wall clock to equal held-out fitness")
     ap.add_argument("--sgp-generations", type=int, default=50)
+    ap.add_argument("--sgp-seed", type=int, default=0, help="with --sgp: the GP seed of every arm")
     ap.add_argument("--sgp-ablation", action="store_true",
                     help="with --sgp: also run the surrogate arms that change one screening "
                          "setting each (about 3 minutes per arm)")
@@ -499,7 +500,7 @@ def sgp_leg(ctx, w, args):
                      "standardised": dict(use_surrogate=1, distinct=0, target=0),
                      "preselection": dict(use_surrogate=1, selection=1),
                      "half_screened": dict(use_surrogate=1, screen_fraction=0.5)})
-    runs = {k: SG.sgp_run(ctx, MENU29, w.mask, seed=0, test_seed=1000000, gp=cfg, **kw)
+    runs = {k: SG.sgp_run(ctx, MENU29, w.mask, seed=args.sgp_seed, test_seed=1000000, gp=cfg, **kw)
             for k, kw in arms.items()}
     plain = runs["plain"]
     target = plain["held_out"][-1] * (1.0 - 0.005)
@@ -512,7 +513,7 @@ def sgp_leg(ctx, w, args):
         return None, None
 
     tp, _ = first_time(plain)
-    out = {"generations": G, "population": args.P, "train_scenarios": args.S,
+    out = {"generations": G, "population": args.P, "train_scenarios": args.S, "seed": args.sgp_seed,
            "target_held_out": target, "plain_wall_seconds": plain_total}
     for k, r in runs.items():
         t, g = first_time(r)

@@ -79,6 +79,10 @@ def parse_args():
                          "1024 rules x 51 generations + held-out) and its vocabulary GA's first "
                          "batch (13 genomes x 16 seeds x 51 generations), both checked against "
                          "the reference's own artefacts in tests/golden/campaign.npz")
+    ap.add_argument("--multi-shape", type=int, default=-1,
+                    help="with --multi: use this block shape (index into sidr.Multi.SHAPES) "
+                         "instead of autotuning, e.g. at full size (--multi-rules 1000 --multi-S 500), "
+                         "where each autotuning launch takes about a minute")
     ap.add_argument("--multi-rules", type=int, default=100)
     ap.add_argument("--multi-S", type=int, default=100)
     return ap.parse_args()
@@ -413,7 +417,11 @@ def multi_leg(args, stream):
     zps = [sidr.zstats(sd) for sd in mw.sds]
     m = sidr.Multi(mw.sds, zps, mw.rules, mw.sampled, mw.S, mw.masks)
     prep = time.perf_counter() - t0
-    chosen, ms = m.autotune(reps=1)
+    if args.multi_shape >= 0:
+        chosen, ms = args.multi_shape, None
+        m.set_shape(chosen)
+    else:
+        chosen, ms = m.autotune(reps=1)
     m.capture()
     m.run(stream.cuda_stream)
     torch.cuda.synchronize()
@@ -426,11 +434,22 @@ def multi_leg(args, stream):
     torch.cuda.synchronize()
     t = min(e0.elapsed_time(e1) for e0, e1 in ev) / 1e3
     P = sum(r.P for r in mw.rules)
+    res = m.read()
     m.close()
+    # spot check: every 125th rule of instances 3 (288 customers) and 38 by the single-instance path
+    import numpy as np
+    mism, pairs = 0, 0
+    for k in (3, 38):
+        ctx = sidr.Context(mw.sds[k], zps[k])
+        idx = list(range(0, mw.rules[k].P, 125))
+        want = ctx.evaluate(mw.rules[k].subset(idx), mw.sampled[k], mw.S, mw.masks[k])
+        mism += int((res[k][idx].view(np.uint64) != want.view(np.uint64)).sum())
+        pairs += want.size
+        ctx.close()
     return {"workload": f"40 instances x {args.multi_rules} rules x {args.multi_S} scenarios",
             "evaluations": P * mw.S, "seconds": t, "evals_per_s": P * mw.S / t,
             "shapes_ms": ms, "chosen_shape": list(sidr.Multi.SHAPES[chosen]),
-            "host_prep_seconds": prep}
+            "host_prep_seconds": prep, "spot_check_pairs": pairs, "spot_check_mismatches": mism}
 
 
 def campaign_leg():

@@ -17,6 +17,10 @@ evaluation sizes the benchmark names, with the reference's own rule generator
                     mixed layouts, m in {2,3,4}, H in {230,1000}, each with 1000
                     rules of log-uniform length 3-255 and 500 scenarios, for the
                     multi-instance launch.
+  large_combined    10 instances of 288 customers (clustered with 12 clusters or
+                    uniform), m=4, H=1000, each with the initial populations of
+                    30 GP seeds x 4096 rules and 2000 scenarios, for the
+                    multi-instance launch (tests use reduced counts).
 """
 from __future__ import annotations
 
@@ -117,6 +121,29 @@ def batched_uneven(K: int = 40, rules_per_instance: int = 1000, S: int = 500) ->
         sampled.append(gen_durations(sd.durations, sd.sigma, S, 1 + 1000 * k))
         masks.append(term_mask_from(MENU29))
     return MultiWorkload("batched_uneven", sds, rules, sampled, masks, S)
+
+
+def large_combined(K: int = 10, seeds: int = 30, rules_per_seed: int = 4096, S: int = 2000) -> MultiWorkload:
+    """The large combined run's evaluation batch: K instances of 288 customers
+    (even k clustered around 12 Gaussian centres, odd k uniform), m=4,
+    H=1000; instance k carries the initial populations of `seeds` independent
+    GP runs (ramped half-and-half, depth 2-8, the 29-terminal menu, Mt19937
+    seed 1000k + s), rules_per_seed rules each, and S scenarios (base seed
+    1 + 1000k).  The full size (10 x 30 x 4096 rules x 2000 scenarios) is
+    2.5 G evaluations; tests use reduced counts."""
+    sds, rules, sampled, masks = [], [], [], []
+    for k in range(K):
+        layout = "clustered" if k % 2 == 0 else "uniform"
+        text = generate_instance(288, layout, 1000.0, 500 + k, n_clusters=12)
+        sd = SimData.from_instance(parse_solomon_text(text), m=4)
+        sds.append(sd)
+        trees = []
+        for s in range(seeds):
+            trees += ramped_half_and_half(MENU29, FUNCTIONS, 2, 8, 1000 * k + s, rules_per_seed)
+        rules.append(pack(trees))
+        sampled.append(gen_durations(sd.durations, sd.sigma, S, 1 + 1000 * k))
+        masks.append(term_mask_from(MENU29))
+    return MultiWorkload("large_combined", sds, rules, sampled, masks, S)
 
 
 WORKLOADS = {"plain_eval": plain_eval, "gp_generation": gp_generation}

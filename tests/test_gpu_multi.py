@@ -47,6 +47,22 @@ def test_multi_matches_per_instance(oracle):
     m.close()
 
 
+def test_large_combined_shape_matches_oracle(oracle):
+    """The large combined run's batch at reduced counts: 288-customer
+    instances (12-cluster and uniform layouts), m = 4, H = 1000, the initial
+    populations of three GP seeds per instance, all in one launch, bit for
+    bit against the C oracle."""
+    mw = workload.large_combined(K=2, seeds=3, rules_per_seed=6, S=3)
+    zps = [sidr.zstats(sd) for sd in mw.sds]
+    m = sidr.Multi(mw.sds, zps, mw.rules, mw.sampled, mw.S, mw.masks)
+    m.run()
+    got = m.read()
+    m.close()
+    for k in range(2):
+        want = oracle.eval_pairs(mw.sds[k], zps[k], mw.rules[k], mw.sampled[k], mw.S, mw.masks[k])
+        assert np.array_equal(bits(got[k]), bits(want)), k
+
+
 def test_multi_rejects_bad_layouts():
     mw = workload.batched_uneven(K=2, rules_per_instance=2, S=2)
     zps = [sidr.zstats(sd) for sd in mw.sds]

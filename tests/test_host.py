@@ -224,3 +224,17 @@ def test_workload_oracle_equals_reference(oracle, reference):
     a = oracle.eval_pairs(w.sd, zp, w.rules, w.sampled, w.S, w.mask)
     b = reference.eval_pairs(w.sd, zp, w.rules, w.sampled, w.S, w.mask)
     assert np.array_equal(bits(a), bits(b))
+
+
+def test_large_combined_oracle_equals_reference(oracle, reference):
+    """The large combined run's instance shape (288 customers around 12
+    cluster centres, m = 4, H = 1000) with initial populations of two GP seeds:
+    the oracle and the reference agree bit for bit."""
+    mw = workload.large_combined(K=1, seeds=2, rules_per_seed=4, S=2)
+    sd = mw.sds[0]
+    assert sd.n == 288 and sd.m == 4 and sd.tmax == 1000.0 and mw.rules[0].P == 8
+    zp = oracle.zstats(sd)
+    assert np.array_equal(bits(zp), bits(reference.zp_of(sd)))
+    a = oracle.eval_pairs(sd, zp, mw.rules[0], mw.sampled[0], mw.S, mw.masks[0])
+    b = reference.eval_pairs(sd, zp, mw.rules[0], mw.sampled[0], mw.S, mw.masks[0])
+    assert np.array_equal(bits(a), bits(b))

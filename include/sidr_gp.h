@@ -81,6 +81,25 @@ sidr_status sidr_gp_run_batched(sidr_ctx* ctx, const sidr_instance_desc* inst,
                                 int64_t test_seed, double* best_test, double* best_train,
                                 char* best_rules, int64_t rules_cap, sidr_gp_result* result);
 
+/* Many instances x many seeds (no single reference call: the reference runs
+ * exhaust_batched, engine/gp_engine.cu:131-203, once per instance).  For each
+ * of the K instances (zps [K][10], masks [K][61]) the seed-batched run of
+ * sidr_gp_run_batched with seeds first_seed .. first_seed + n_seeds - 1; all
+ * K * n_seeds populations are evaluated together in ONE multi-instance launch
+ * per generation (sidr_multi_*), each on its own instance and train block.
+ * Per instance the results equal sidr_gp_run_batched's on that instance
+ * alone.  shape: the launch's block shape (0 .. SIDR_MULTI_SHAPES-1), or -1 to
+ * autotune on the first launch and keep the choice.  Each generation builds
+ * its batch anew (instance tables included, on the host).
+ *   best_test[K*n_seeds]           held-out mean of each population's best rule
+ *   best_train[gens*K*n_seeds]     index (gen*K + k)*n_seeds + s
+ *   best_rules                     K*n_seeds prefix lines in (k, s) order */
+sidr_status sidr_gp_run_multi(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                              const sidr_gp_config* cfg, const char* terminals_csv, const int64_t* masks,
+                              int32_t n_seeds, int64_t first_seed, int64_t test_seed, int32_t shape,
+                              int32_t device, double* best_test, double* best_train, char* best_rules,
+                              int64_t rules_cap, sidr_gp_result* result);
+
 /* gen_durations (engine/sim_host.hpp:43-58) on the host: [S][n]. */
 sidr_status sidr_gen_durations(int32_t n, const double* durations, double sigma, int32_t S,
                                int64_t base_seed, double* out);

@@ -198,4 +198,147 @@ sidr_status sidr_gp_run_batched(sidr_ctx* ctx, const sidr_instance_desc* inst,
     return SIDR_OK;
 }
 
+sidr_status sidr_gp_run_multi(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                              const sidr_gp_config* cfg, const char* terminals_csv, const int64_t* masks,
+                              int32_t n_seeds, int64_t first_seed, int64_t test_seed, int32_t shape,
+                              int32_t device, double* best_test, double* best_train, char* best_rules,
+                              int64_t rules_cap, sidr_gp_result* result) {
+    using clock = std::chrono::steady_clock;
+    std::string err;
+    if (!insts || !zps || !masks) return gp_fail(SIDR_ERR_INVALID, "null argument");
+    if (K < 1 || n_seeds < 1) return gp_fail(SIDR_ERR_INVALID, "K < 1 or n_seeds < 1");
+    if ((int64_t)K * n_seeds > 32767) return gp_fail(SIDR_ERR_INVALID, "K * n_seeds > 32767");
+    if (shape < -1 || shape >= SIDR_MULTI_SHAPES) return gp_fail(SIDR_ERR_INVALID, "shape out of range");
+    if (!valid_config(cfg, err)) return gp_fail(SIDR_ERR_INVALID, err);
+    for (int k = 0; k < K; k++)
+        if (insts[k].n < 1 || !insts[k].durations)
+            return gp_fail(SIDR_ERR_INVALID, "instance " + std::to_string(k) + ": no customers or no durations");
+    std::vector<std::string> terms;
+    if (!parse_terminals(terminals_csv, terms, err)) return gp_fail(SIDR_ERR_INVALID, err);
+    const int ps = cfg->population, T = cfg->train_samples, E = K * n_seeds;
+    double t_eval = 0.0;
+    int64_t evals = 0;
+    int chosen = shape;
+    const auto t0 = clock::now();
+    // population e = k * n_seeds + s: instance k, seed first_seed + s
+    std::vector<Gp> gps;
+    gps.reserve(E);
+    for (int e = 0; e < E; e++) {
+        gps.emplace_back(*cfg, (uint64_t)(first_seed + e % n_seeds));
+        gps.back().vocab.terminals = terms;
+        gps.back().vocab.n_funcs = cfg->with_rmod ? 7 : 6;
+        gps.back().init();
+    }
+    // One multi-instance launch: entry q is instance ek[q] with the scenario
+    // block blocks[q] ([Tn][n]); rule p belongs to entry owner[p]; out [P][Tn].
+    auto launch = [&](const std::vector<int>& ek, const std::vector<std::vector<double>>& blocks, int Tn,
+                      std::vector<int32_t>& ops, std::vector<int32_t>& args, std::vector<int32_t>& off,
+                      std::vector<int32_t>& len, const std::vector<int32_t>& owner,
+                      std::vector<double>& out) -> sidr_status {
+        const int Q = (int)ek.size();
+        std::vector<sidr_instance_desc> d(Q);
+        std::vector<double> z((size_t)Q * 10), flat;
+        std::vector<int64_t> mk((size_t)Q * 61), offs(Q);
+        for (int q = 0; q < Q; q++) {
+            d[q] = insts[ek[q]];
+            std::copy(zps + 10 * (size_t)ek[q], zps + 10 * (size_t)ek[q] + 10, z.begin() + 10 * (size_t)q);
+            std::copy(masks + 61 * (size_t)ek[q], masks + 61 * (size_t)ek[q] + 61, mk.begin() + 61 * (size_t)q);
+            offs[q] = (int64_t)flat.size();
+            flat.insert(flat.end(), blocks[q].begin(), blocks[q].end());
+        }
+        sidr_rules_desc r{ops.data(), args.data(), off.data(), len.data(), (int32_t)off.size(),
+                          (int64_t)ops.size()};
+        out.assign((size_t)r.P * Tn, 0.0);
+        const auto e0 = clock::now();
+        sidr_multi* m = nullptr;
+        sidr_status st = sidr_multi_create(d.data(), z.data(), Q, &r, owner.data(), flat.data(),
+                                           (int64_t)flat.size(), offs.data(), Tn, mk.data(), device, &m);
+        if (st == SIDR_OK) st = chosen < 0 ? sidr_multi_autotune(m, 1, &chosen, nullptr) : sidr_multi_set_shape(m, chosen);
+        if (st == SIDR_OK) st = sidr_multi_run(m, nullptr);
+        if (st == SIDR_OK) st = sidr_multi_read(m, out.data());
+        const std::string why = st == SIDR_OK ? std::string() : std::string(sidr_last_error());
+        sidr_multi_destroy(m);
+        t_eval += std::chrono::duration<double>(clock::now() - e0).count();
+        evals += (int64_t)r.P * Tn;
+        if (st != SIDR_OK) return gp_fail(st, "evaluation: " + why);
+        return SIDR_OK;
+    };
+    // every population on its own train block (base seed seed*10000 + gen) of its instance
+    std::vector<std::vector<double>> fits(E, std::vector<double>(ps));
+    auto train_fit = [&](int gen) -> sidr_status {
+        std::vector<int32_t> ops, args, off, len, owner;
+        std::vector<std::vector<double>> blocks(E);
+        std::vector<int> ek(E);
+        for (int e = 0; e < E; e++) {
+            const int k = e / n_seeds, sd = e % n_seeds, n = insts[k].n;
+            gps[e].packed(ops, args, off, len);
+            owner.insert(owner.end(), ps, e);
+            ek[e] = k;
+            blocks[e].resize((size_t)T * n);
+            sidr_gen_durations(n, insts[k].durations, 0.2, T, (first_seed + sd) * 10000 + gen, blocks[e].data());
+        }
+        std::vector<double> out;
+        const sidr_status st = launch(ek, blocks, T, ops, args, off, len, owner, out);
+        if (st != SIDR_OK) return st;
+        for (int e = 0; e < E; e++)
+            for (int p = 0; p < ps; p++) {
+                double acc = 0.0;
+                for (int t = 0; t < T; t++) acc += out[((size_t)e * ps + p) * T + t];
+                fits[e][p] = acc / T;
+            }
+        return SIDR_OK;
+    };
+    for (int gen = 0; gen < cfg->generations; gen++) {
+        const sidr_status st = train_fit(gen);
+        if (st != SIDR_OK) return st;
+        for (int e = 0; e < E; e++) {
+            double b = fits[e][0];
+            for (int p = 1; p < ps; p++) b = fits[e][p] > b ? fits[e][p] : b;
+            if (best_train) best_train[(size_t)gen * E + e] = b;
+        }
+        if (gen < cfg->generations - 1)
+            for (int e = 0; e < E; e++) gps[e].step(fits[e]);
+    }
+    // final train block, best rule per population, held-out scoring on each instance's test block
+    sidr_status st = train_fit(cfg->generations);
+    if (st != SIDR_OK) return st;
+    std::string rules_text;
+    std::vector<int32_t> ops, args, off, len, owner;
+    for (int e = 0; e < E; e++) {
+        int bi = 0;
+        for (int p = 1; p < ps; p++)
+            if (fits[e][p] > fits[e][bi]) bi = p;
+        gps[e].packed(ops, args, off, len, (size_t)bi, 1);
+        owner.push_back(e / n_seeds);
+        size_t k = 0;
+        prefix_at(gps[e].pop[bi], k, gps[e].vocab, rules_text);
+        rules_text += '\n';
+    }
+    if (cfg->test_samples > 0) {
+        const int TS = cfg->test_samples;
+        std::vector<std::vector<double>> blocks(K);
+        std::vector<int> ek(K);
+        for (int k = 0; k < K; k++) {
+            ek[k] = k;
+            blocks[k].resize((size_t)TS * insts[k].n);
+            sidr_gen_durations(insts[k].n, insts[k].durations, 0.2, TS, test_seed, blocks[k].data());
+        }
+        std::vector<double> out;
+        if ((st = launch(ek, blocks, TS, ops, args, off, len, owner, out)) != SIDR_OK) return st;
+        for (int e = 0; e < E; e++) {
+            double acc = 0.0;
+            for (int t = 0; t < TS; t++) acc += out[(size_t)e * TS + t];
+            if (best_test) best_test[e] = acc / TS;
+        }
+    }
+    if (best_rules && rules_cap > (int64_t)rules_text.size())
+        std::memcpy(best_rules, rules_text.c_str(), rules_text.size() + 1);
+    if (result) {
+        result->eval_seconds = t_eval;
+        result->host_seconds = std::chrono::duration<double>(clock::now() - t0).count() - t_eval;
+        result->evaluations = evals;
+    }
+    return SIDR_OK;
+}
+
 }  // extern "C"

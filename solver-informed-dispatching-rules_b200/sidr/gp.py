@@ -43,6 +43,10 @@ def _lib():
         L.sidr_gp_run_batched.argtypes = [C.c_void_p, C.POINTER(_Inst), C.POINTER(_Cfg), C.c_char_p,
                                           C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
                                           dp, dp, C.c_char_p, C.c_int64, C.POINTER(_Result)]
+        L.sidr_gp_run_multi.argtypes = [C.POINTER(_Inst), dp, C.c_int32, C.POINTER(_Cfg), C.c_char_p,
+                                        C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
+                                        C.c_int32, C.c_int32, dp, dp, C.c_char_p, C.c_int64,
+                                        C.POINTER(_Result)]
         L._gp_ready = True
     return L
 
@@ -138,5 +142,31 @@ def run_batched(ctx, terminals: Sequence[str], mask, n_seeds: int, first_seed: i
                                       ",".join(terminals).encode(), k.i64(mask), n_seeds,
                                       first_seed, test_seed, bt.ctypes.data_as(dp),
                                       btr.ctypes.data_as(dp), buf, 1 << 22, C.byref(res)))
+    return RunResult(bt, btr, buf.value.decode().splitlines(), res.eval_seconds,
+                     res.host_seconds, res.evaluations)
+
+
+def run_multi(sds, zps, terminals: Sequence[str], masks, n_seeds: int, first_seed: int = 0,
+              test_seed: int = 1000000, shape: int = 1, device: int = 0, **cfg) -> RunResult:
+    """Seed-batched GP runs on many instances at once, one multi-instance launch
+    per generation (sidr_gp_run_multi): best_test [K, n_seeds], best_train
+    [generations, K, n_seeds], best_rules in (instance, seed) order."""
+    c = config(**cfg)
+    k = _Keep()
+    K = len(sds)
+    from . import _Inst
+    insts = (_Inst * K)(*[k.inst(sd) for sd in sds])
+    z = np.ascontiguousarray(np.stack([np.asarray(v, dtype=np.float64) for v in zps]))
+    m = np.ascontiguousarray(np.stack([np.asarray(v, dtype=np.int64) for v in masks]))
+    bt = np.zeros((K, n_seeds))
+    btr = np.zeros((c.generations, K, n_seeds))
+    buf = C.create_string_buffer(1 << 22)
+    res = _Result()
+    dp = C.POINTER(C.c_double)
+    _check(_lib().sidr_gp_run_multi(insts, z.ctypes.data_as(dp), K, C.byref(c),
+                                    ",".join(terminals).encode(),
+                                    m.ctypes.data_as(C.POINTER(C.c_int64)), n_seeds, first_seed,
+                                    test_seed, shape, device, bt.ctypes.data_as(dp),
+                                    btr.ctypes.data_as(dp), buf, 1 << 22, C.byref(res)))
     return RunResult(bt, btr, buf.value.decode().splitlines(), res.eval_seconds,
                      res.host_seconds, res.evaluations)

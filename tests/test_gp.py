@@ -61,3 +61,18 @@ def test_gp_rejects_bad_config():
         gp.Session(["SCORE", "NOPE"], 0)
     with pytest.raises(sidr.SidrError):
         gp.Session(["SCORE"], 0, max_depth=9)
+
+
+def test_run_multi_rejects_bad_arguments():
+    """Argument checks of the many-instance driver come before any device work."""
+    import sidr
+    from sidr import workload
+    w = workload.plain_eval(P=1, S=1)
+    zp = sidr.zstats(w.sd)
+    for kw in (dict(shape=7), dict(shape=-2)):
+        with pytest.raises(sidr.SidrError):
+            gp.run_multi([w.sd], [zp], workload.MENU29, [w.mask], 2, **kw)
+    with pytest.raises(sidr.SidrError):
+        gp.run_multi([w.sd], [zp], ["SCORE", "NOPE"], [w.mask], 2)
+    with pytest.raises(sidr.SidrError):
+        gp.run_multi([w.sd], [zp], workload.MENU29, [w.mask], 0)

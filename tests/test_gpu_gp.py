@@ -55,3 +55,30 @@ def test_run_batched_matches_cpu_replica(oracle):
         held = oracle.eval_pairs(w.sd, zp, rule, test, test_n, w.mask)[0]
         assert bits(res.best_test[s]) == bits(sum(float(v) for v in held) / test_n)
     assert res.evaluations == gens * n_seeds * pop * T + n_seeds * pop * T + n_seeds * test_n
+
+
+def test_run_multi_equals_run_batched_per_instance():
+    """Three instances of uneven size (25, 50 and 288 customers), two seeds
+    each, evolved through one multi-instance launch per generation: every
+    instance's best train fitness per generation, best rules and held-out
+    scores equal the seed-batched driver's on that instance alone."""
+    mw = workload.batched_uneven(K=4, rules_per_instance=1, S=1)
+    sds = [mw.sds[0], mw.sds[1], mw.sds[3]]
+    assert [sd.n for sd in sds] == [25, 50, 288]
+    zps = [sidr.zstats(sd) for sd in sds]
+    masks = [mw.masks[0]] * 3
+    terms = workload.MENU29
+    cfg = dict(population=32, generations=3, train_samples=3, test_samples=8)
+    multi = gp.run_multi(sds, zps, terms, masks, 2, first_seed=11, test_seed=4321, shape=1, **cfg)
+    auto = gp.run_multi(sds[:2], zps[:2], terms, masks[:2], 2, first_seed=11, test_seed=4321,
+                        shape=-1, **cfg)
+    for k, (sd, zp) in enumerate(zip(sds, zps)):
+        ctx = sidr.Context(sd, zp)
+        one = gp.run_batched(ctx, terms, masks[k], 2, first_seed=11, test_seed=4321, **cfg)
+        ctx.close()
+        assert np.array_equal(bits(multi.best_train[:, k, :]), bits(one.best_train)), k
+        assert np.array_equal(bits(multi.best_test[k]), bits(one.best_test)), k
+        assert multi.best_rules[2 * k:2 * k + 2] == one.best_rules, k
+        if k < 2:
+            assert np.array_equal(bits(auto.best_test[k]), bits(one.best_test)), k
+    assert multi.evaluations == 3 * 2 * 32 * 3 * (3 + 1) + 3 * 2 * 8

@@ -59,6 +59,20 @@ sidr_status sidr_gp_population_packed(const sidr_gp_session* s, int32_t* ops, in
 /* gp_step (engine/gp.hpp:170-194) with the given per-rule fitness. */
 sidr_status sidr_gp_step(sidr_gp_session* s, const double* fitness);
 
+/* Number of sidr_gp_step calls the session has made (-1 for NULL). */
+int64_t sidr_gp_generation(const sidr_gp_session* s);
+
+/* Checkpoint / resume (the reference resumes only its vocabulary GA, through
+ * the evaluation cache of s4_selection/ga.cu:301-346; the GP itself restarts).
+ * sidr_gp_checkpoint writes the session's whole state as text -- config,
+ * step count, terminal set, leaf-label table (ERC constants included), the
+ * MT19937 state and the population -- and returns the bytes needed (call
+ * with cap 0 to size the buffer; -1 for NULL).  sidr_gp_restore makes a new
+ * session from it that continues exactly as the checkpointed one would;
+ * malformed or inconsistent text is refused with SIDR_ERR_INVALID. */
+int64_t sidr_gp_checkpoint(const sidr_gp_session* s, char* buf, int64_t cap);
+sidr_status sidr_gp_restore(const char* checkpoint, sidr_gp_session** out);
+
 /* The seed-batched GP run of engine/gp_engine.cu:131-203 (exhaust_batched):
  * n_seeds populations (seeds first_seed .. first_seed+n_seeds-1) evolve
  * together, each generation evaluated in one grouped call on the evaluator with

@@ -1,5 +1,7 @@
 // sidr_gp.cpp -- the host GP loop driving the evaluator (include/sidr_gp.h).
 #include <chrono>
+#include <memory>
+#include <sstream>
 
 #include "sidr_gp_core.hpp"
 
@@ -7,8 +9,40 @@ using namespace sidr::gp;
 
 struct sidr_gp_session {
     Gp gp;
+    int64_t generation = 0;  // gp_step calls so far
     sidr_gp_session(const sidr_gp_config& c, uint64_t seed) : gp(c, seed) {}
 };
+
+namespace {
+
+constexpr const char* kCheckpointHeader = "sidr-gp-checkpoint 1";
+
+std::string hexf(double v) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%a", v);
+    return buf;
+}
+
+// A rule in prefix codes is well formed when it is one complete tree of
+// known functions and leaf labels.
+bool rule_ok(const Rule& r, int n_funcs, size_t n_labels) {
+    if (r.empty()) return false;
+    long need = 1;
+    for (size_t k = 0; k < r.size(); k++) {
+        if (need <= 0) return false;
+        const int32_t c = r[k];
+        if (c >= 0) {
+            if (c >= n_funcs) return false;
+            need += 1;
+        } else {
+            if ((size_t)(-(int64_t)c - 1) >= n_labels) return false;
+            need -= 1;
+        }
+    }
+    return need == 0;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -72,6 +106,108 @@ sidr_status sidr_gp_step(sidr_gp_session* s, const double* fitness) {
     if (!s || !fitness) return gp_fail(SIDR_ERR_INVALID, "null argument");
     std::vector<double> f(fitness, fitness + s->gp.pop.size());
     s->gp.step(f);
+    s->generation++;
+    return SIDR_OK;
+}
+
+int64_t sidr_gp_generation(const sidr_gp_session* s) { return s ? s->generation : -1; }
+
+int64_t sidr_gp_checkpoint(const sidr_gp_session* s, char* buf, int64_t cap) {
+    if (!s) return -1;
+    const Gp& g = s->gp;
+    const sidr_gp_config& c = g.cfg;
+    std::string t = std::string(kCheckpointHeader) + "\n";
+    t += "config " + std::to_string(c.population) + " " + std::to_string(c.generations) + " " +
+         std::to_string(c.max_depth) + " " + std::to_string(c.min_depth) + " " + std::to_string(c.tournament) +
+         " " + std::to_string(c.elitism) + " " + hexf(c.crossover_rate) + " " + hexf(c.mutation_rate) + " " +
+         hexf(c.reproduction_rate) + " " + std::to_string(c.train_samples) + " " +
+         std::to_string(c.test_samples) + " " + std::to_string(c.with_rmod) + "\n";
+    t += "generation " + std::to_string(s->generation) + "\n";
+    t += "terminals " + std::to_string(g.vocab.terminals.size()) + "\n";
+    for (const std::string& x : g.vocab.terminals) t += x + "\n";
+    t += "labels " + std::to_string(g.vocab.labels.size()) + "\n";
+    for (const std::string& x : g.vocab.labels) t += x + "\n";
+    t += "rng " + g.rng.state() + "\n";
+    t += "population " + std::to_string(g.pop.size()) + "\n";
+    for (const Rule& r : g.pop) {
+        t += std::to_string(r.size());
+        for (int32_t v : r) t += " " + std::to_string(v);
+        t += "\n";
+    }
+    if (buf && cap > (int64_t)t.size()) std::memcpy(buf, t.c_str(), t.size() + 1);
+    return (int64_t)t.size() + 1;
+}
+
+sidr_status sidr_gp_restore(const char* checkpoint, sidr_gp_session** out) {
+    if (!out || !checkpoint) return gp_fail(SIDR_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::istringstream in(checkpoint);
+    std::string line, word;
+    auto bad = [](const std::string& what) { return gp_fail(SIDR_ERR_INVALID, "checkpoint: " + what); };
+    if (!std::getline(in, line) || line != kCheckpointHeader) return bad("not a GP checkpoint of version 1");
+    sidr_gp_config c;
+    std::string cx, mu, rp;
+    if (!std::getline(in, line)) return bad("no config line");
+    {
+        std::istringstream ls(line);
+        if (!(ls >> word) || word != "config" ||
+            !(ls >> c.population >> c.generations >> c.max_depth >> c.min_depth >> c.tournament >> c.elitism >>
+              cx >> mu >> rp >> c.train_samples >> c.test_samples >> c.with_rmod))
+            return bad("malformed config line");
+        c.crossover_rate = std::strtod(cx.c_str(), nullptr);
+        c.mutation_rate = std::strtod(mu.c_str(), nullptr);
+        c.reproduction_rate = std::strtod(rp.c_str(), nullptr);
+    }
+    std::string err;
+    if (!valid_config(&c, err)) return bad(err);
+    int64_t generation = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "generation %lld", (long long*)&generation) != 1 ||
+        generation < 0)
+        return bad("malformed generation line");
+    auto read_list = [&](const char* key, std::vector<std::string>& items) -> bool {
+        long long cnt = -1;
+        if (!std::getline(in, line)) return false;
+        std::istringstream ls(line);
+        if (!(ls >> word) || word != key || !(ls >> cnt) || cnt < 0 || cnt > (1 << 24)) return false;
+        items.clear();
+        for (long long i = 0; i < cnt; i++) {
+            if (!std::getline(in, line) || line.empty()) return false;
+            items.push_back(line);
+        }
+        return true;
+    };
+    std::vector<std::string> terms, labels;
+    if (!read_list("terminals", terms)) return bad("malformed terminals");
+    std::string csv;
+    for (size_t i = 0; i < terms.size(); i++) csv += (i ? "," : "") + terms[i];
+    std::vector<std::string> parsed;
+    if (!parse_terminals(csv.c_str(), parsed, err) || parsed != terms) return bad("terminals: " + err);
+    if (!read_list("labels", labels)) return bad("malformed labels");
+    std::unique_ptr<sidr_gp_session> s(new sidr_gp_session(c, 0));
+    s->generation = generation;
+    s->gp.vocab.terminals = terms;
+    s->gp.vocab.n_funcs = c.with_rmod ? 7 : 6;
+    for (const std::string& l : labels)
+        if (s->gp.vocab.leaf(l) != (int)s->gp.vocab.labels.size() - 1) return bad("repeated label " + l);
+    if (!std::getline(in, line) || line.compare(0, 4, "rng ") != 0 || !s->gp.rng.set_state(line.substr(4)))
+        return bad("malformed generator state");
+    long long np = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "population %lld", &np) != 1 ||
+        np != c.population)
+        return bad("population size differs from the config");
+    for (long long i = 0; i < np; i++) {
+        if (!std::getline(in, line)) return bad("population truncated");
+        std::istringstream ls(line);
+        long long len = -1;
+        if (!(ls >> len) || len < 1 || len > (1 << 20)) return bad("malformed rule");
+        Rule r((size_t)len);
+        for (long long k = 0; k < len; k++)
+            if (!(ls >> r[(size_t)k])) return bad("malformed rule");
+        if (ls >> word) return bad("rule " + std::to_string(i) + ": more codes than its length");
+        if (!rule_ok(r, s->gp.vocab.n_funcs, labels.size())) return bad("rule " + std::to_string(i) + " is not a tree");
+        s->gp.pop.push_back(std::move(r));
+    }
+    *out = s.release();
     return SIDR_OK;
 }
 

@@ -133,6 +133,44 @@ class Mt19937 {
         return mu + z * sigma;
     }
 
+    // The generator's whole state as text (624 words, position, cached
+    // Box-Muller value as a hexadecimal float), and back.
+    std::string state() const {
+        std::string out = std::to_string(mti_) + " " + (has_spare_ ? "1 " : "0 ");
+        char buf[64];
+        std::snprintf(buf, sizeof buf, "%a", spare_);
+        out += buf;
+        for (int k = 0; k < kN; k++) out += " " + std::to_string(mt_[k]);
+        return out;
+    }
+    bool set_state(const std::string& text) {
+        const char* p = text.c_str();
+        char* e = nullptr;
+        const long mti = std::strtol(p, &e, 10);
+        if (e == p || mti < 0 || mti > kN + 1) return false;
+        p = e;
+        const long hs = std::strtol(p, &e, 10);
+        if (e == p || (hs != 0 && hs != 1)) return false;
+        p = e;
+        const double sp = std::strtod(p, &e);
+        if (e == p) return false;
+        p = e;
+        uint32_t mt[kN];
+        for (int k = 0; k < kN; k++) {
+            const unsigned long long v = std::strtoull(p, &e, 10);
+            if (e == p || v > 0xffffffffull) return false;
+            mt[k] = (uint32_t)v;
+            p = e;
+        }
+        while (*p == ' ') p++;
+        if (*p) return false;
+        std::memcpy(mt_, mt, sizeof mt);
+        mti_ = (int)mti;
+        has_spare_ = hs == 1;
+        spare_ = sp;
+        return true;
+    }
+
   private:
     static constexpr int kN = 624, kM = 397;
     uint32_t mt_[kN];

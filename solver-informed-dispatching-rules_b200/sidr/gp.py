@@ -37,6 +37,11 @@ def _lib():
         ip = C.POINTER(C.c_int32)
         L.sidr_gp_population_packed.argtypes = [C.c_void_p, ip, ip, ip, ip, C.POINTER(C.c_int64)]
         L.sidr_gp_step.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.sidr_gp_generation.argtypes = [C.c_void_p]
+        L.sidr_gp_generation.restype = C.c_int64
+        L.sidr_gp_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_int64]
+        L.sidr_gp_checkpoint.restype = C.c_int64
+        L.sidr_gp_restore.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
         dp = C.POINTER(C.c_double)
         L.sidr_gen_durations.argtypes = [C.c_int32, dp, C.c_double, C.c_int32, C.c_int64, dp]
         from . import _Inst
@@ -95,6 +100,34 @@ class Session:
     def step(self, fitness) -> None:
         f = np.ascontiguousarray(fitness, dtype=np.float64)
         _check(_lib().sidr_gp_step(self.h, f.ctypes.data_as(C.POINTER(C.c_double))))
+
+    @property
+    def generation(self) -> int:
+        """gp_step calls so far."""
+        return int(_lib().sidr_gp_generation(self.h))
+
+    def checkpoint(self) -> str:
+        """The session's whole state as text (sidr_gp_checkpoint)."""
+        L = _lib()
+        n = L.sidr_gp_checkpoint(self.h, None, 0)
+        buf = C.create_string_buffer(int(n))
+        L.sidr_gp_checkpoint(self.h, buf, n)
+        return buf.value.decode()
+
+    @classmethod
+    def restore(cls, text: str) -> "Session":
+        """A session that continues exactly as the checkpointed one would."""
+        h = C.c_void_p()
+        _check(_lib().sidr_gp_restore(text.encode(), C.byref(h)))
+        s = cls.__new__(cls)
+        s.h = h.value
+        v = text.splitlines()[1].split()[1:]
+        s.cfg = config(population=int(v[0]), generations=int(v[1]), max_depth=int(v[2]),
+                       min_depth=int(v[3]), tournament=int(v[4]), elitism=int(v[5]),
+                       crossover_rate=float.fromhex(v[6]), mutation_rate=float.fromhex(v[7]),
+                       reproduction_rate=float.fromhex(v[8]), train_samples=int(v[9]),
+                       test_samples=int(v[10]), with_rmod=int(v[11]))
+        return s
 
     def close(self):
         if getattr(self, "h", None):

@@ -76,3 +76,54 @@ def test_run_multi_rejects_bad_arguments():
         gp.run_multi([w.sd], [zp], ["SCORE", "NOPE"], [w.mask], 2)
     with pytest.raises(sidr.SidrError):
         gp.run_multi([w.sd], [zp], workload.MENU29, [w.mask], 0)
+
+
+def _fitness_of(sess):
+    """A deterministic stand-in fitness: a hash of each rule's text."""
+    import zlib
+    return np.array([zlib.crc32(t.encode()) % 1000 / 7.0 for t in sess.text()])
+
+
+@pytest.mark.parametrize("terms,rmod", [(["SCORE", "TA", "NS", "ATRISK", "ERC"], 1),
+                                        (["SCORE", "DUR", "TC", "REACH2"], 0)])
+def test_checkpoint_resume_continues_identically(terms, rmod):
+    """Three steps, a checkpoint, three more steps; a session restored from the
+    checkpoint takes the same three steps to the same populations, with ERC
+    constants and the generator state carried over."""
+    cfg = dict(population=40, max_depth=6, with_rmod=rmod)
+    a = gp.Session(terms, 9, **cfg)
+    for _ in range(3):
+        a.step(_fitness_of(a))
+    text = a.checkpoint()
+    b = gp.Session.restore(text)
+    assert b.generation == a.generation == 3
+    assert b.text() == a.text() and b.checkpoint() == text
+    for _ in range(3):
+        fa, fb = _fitness_of(a), _fitness_of(b)
+        a.step(fa)
+        b.step(fb)
+        assert b.text() == a.text()
+    pa, pb = a.packed(), b.packed()
+    assert np.array_equal(pa.ops, pb.ops) and np.array_equal(pa.args, pb.args)
+    assert b.generation == 6 and b.checkpoint() == a.checkpoint()
+
+
+def test_restore_refuses_malformed_checkpoints():
+    import sidr
+    a = gp.Session(["SCORE", "TA", "ERC"], 1, population=12, max_depth=4)
+    text = a.checkpoint()
+    lines = text.splitlines()
+    bad = [
+        "not a checkpoint",
+        text.replace("sidr-gp-checkpoint 1", "sidr-gp-checkpoint 2"),
+        "\n".join(lines[:-3]) + "\n",                                   # truncated population
+        "\n".join(lines[:-1] + ["2 0 -1"]) + "\n",                      # not one tree
+        "\n".join(lines[:-1] + ["3 0 -1 -1 -1"]) + "\n",                # codes beyond its length
+        "\n".join(lines[:-1] + ["1 -999"]) + "\n",                      # unknown leaf label
+        "\n".join(l if not l.startswith("rng ") else "rng 5 0 0x0p+0 1 2" for l in lines) + "\n",
+        "\n".join(l if not l.startswith("config ") else l.replace("config 12", "config 13", 1)
+                  for l in lines) + "\n",                               # population count differs
+    ]
+    for t in bad:
+        with pytest.raises(sidr.SidrError):
+            gp.Session.restore(t)

@@ -61,6 +61,16 @@ sidr_status sidr_phenotype(const sidr_rules_desc* rules, const double* terms, co
 sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int32_t N, int32_t K,
                            int32_t splits, int device, float* C);
 
+/* Failure-detection check of the GEMM kernel's bounded waits (diagnostic; no
+ * reference counterpart).  One launch of the kernel on a 128 x 48 x 32 zero
+ * problem in which the elected thread issues no MMA and no commit, so the
+ * mbarrier phase every thread waits on never completes: each wait gives up
+ * after wait_limit polls (1 .. 2^20), the kernel frees its tensor memory and
+ * raises its error flag, and the host reads the flag.  Returns
+ * SIDR_ERR_KERNEL when the flag was raised (the expected outcome); the device
+ * context stays usable. */
+sidr_status sidr_gemm_wait_check(int device, uint32_t wait_limit);
+
 /* The model: parameters 0 W1 [256 x 48] (input columns 40..47 are zero
  * padding), 1 b1 [256], 2 W2 [256 x 256], 3 b2 [256], 4 w3 [256], 5 b3 [1],
  * FP32 masters with BF16 copies for the GEMMs; He-uniform initialisation

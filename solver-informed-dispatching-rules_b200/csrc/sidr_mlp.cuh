@@ -39,6 +39,9 @@ struct GemmArgs {
     __nv_bfloat16* Hb;
     int ldh;
     int* error;          // set to 1 when an MMA wait runs out
+    uint32_t wait_limit; // polls of the mbarrier before a wait gives up (0: kWaitLimit)
+    int withhold;        // failure-detection check: issue no MMA and no commit, so
+                         // every wait runs out (nothing is left in flight)
 };
 
 constexpr int kTileM = 128;
@@ -129,7 +132,7 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
         // generic-proxy shared-memory writes become visible to the MMA's async proxy
         asm volatile("fence.proxy.async.shared::cta;");
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !g.withhold) {
             asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
             for (int ks = 0; ks < kChunkK / 16; ks++) {
@@ -146,6 +149,7 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
                          : "memory");
         }
         // every thread waits for the MMAs (they read the staged tiles)
+        const uint32_t limit = g.wait_limit ? g.wait_limit : kWaitLimit;
         uint32_t done = 0, spins = 0;
         while (!done) {
             asm volatile(
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
                 "selp.u32 %0, 1, 0, p;\n\t}\n"
                 : "=r"(done)
                 : "r"(bar), "r"(phase));
-            if (!done && ++spins > kWaitLimit) {
+            if (!done && ++spins > limit) {
                 failed = 1;
                 break;
             }

@@ -442,6 +442,46 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
     return SIDR_OK;
 }
 
+sidr_status sidr_gemm_wait_check(int device, uint32_t wait_limit) {
+    if (wait_limit < 1 || wait_limit > (1u << 20))
+        return fail_s(SIDR_ERR_INVALID, "wait check: wait_limit out of 1..2^20");
+    SIDR_SCHECK(cudaSetDevice(device));
+    constexpr int M = 128, N = 48, K = 32;
+    __nv_bfloat16 *dA = nullptr, *dB = nullptr;
+    float* dC = nullptr;
+    int* err = nullptr;
+    cudaError_t e = cudaMalloc(&dA, (size_t)M * K * 2);
+    if (!e) e = cudaMalloc(&dB, (size_t)N * K * 2);
+    if (!e) e = cudaMalloc(&dC, (size_t)M * N * 4);
+    if (!e) e = cudaMalloc(&err, sizeof(int));
+    if (!e) e = cudaMemset(dA, 0, (size_t)M * K * 2);
+    if (!e) e = cudaMemset(dB, 0, (size_t)N * K * 2);
+    if (!e) e = cudaMemset(err, 0, sizeof(int));
+    sidr_status s = SIDR_OK;
+    if (!e) {
+        GemmArgs g{};
+        g.A = dA; g.sam = K; g.sak = 1;
+        g.B = dB; g.sbn = K; g.sbk = 1;
+        g.M = M; g.N = N; g.K = K;
+        g.epilogue = kStoreF32;
+        g.C = dC; g.ldc = N; g.error = err;
+        g.wait_limit = wait_limit;
+        g.withhold = 1;
+        s = launch_gemm(g, 1, 0);
+        if (!s) e = cudaDeviceSynchronize();
+    }
+    int h = 0;
+    if (!e && !s) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaFree(err);
+    if (s) return s;
+    if (e) return fail_s(SIDR_ERR_CUDA, std::string("wait check: ") + cudaGetErrorString(e));
+    if (h) return fail_s(SIDR_ERR_KERNEL, "wait check: the MMA waits ran out and the kernel reported it");
+    return SIDR_OK;
+}
+
 sidr_status sidr_phenotype(const sidr_rules_desc* r, const double* terms, const int32_t* ncand,
                            const int32_t* ref, int32_t n_sit, int32_t max_cand, int device,
                            float* features) {

@@ -33,6 +33,7 @@ def _lib():
         L.sidr_mlp_gradients.argtypes = [C.c_void_p, _fp, _fp, C.c_int32, _fp]
         L.sidr_mlp_train.argtypes = [C.c_void_p, _fp, _fp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                      C.c_uint64, _fp]
+        L.sidr_gemm_wait_check.argtypes = [C.c_int, C.c_uint32]
         L._surrogate_ready = True
     return L
 
@@ -46,6 +47,12 @@ def to_bf16_bits(x) -> np.ndarray:
 
 def from_bf16_bits(b) -> np.ndarray:
     return (np.asarray(b, dtype=np.uint32) << 16).view(np.float32)
+
+
+def gemm_wait_check(device: int = 0, wait_limit: int = 1000) -> int:
+    """sidr_gemm_wait_check's status: SIDR_ERR_KERNEL (6) when the GEMM kernel,
+    with its MMAs withheld, gave up its bounded waits and said so."""
+    return int(_lib().sidr_gemm_wait_check(device, wait_limit))
 
 
 def gemm_bf16(A_bits, B_bits, splits: int = 1, device: int = 0) -> np.ndarray:

@@ -26,6 +26,17 @@ def test_gemm_matches_float64(M, N, K, splits):
     assert np.max(np.abs(got - ref)) <= 1e-5 * np.sqrt(K) * max(1.0, np.max(np.abs(ref)))
 
 
+def test_bounded_wait_is_reported_and_the_context_survives():
+    """The GEMM's MMA waits are bounded: with the MMAs and their commit
+    withheld, every wait runs out, the kernel frees its tensor memory and
+    raises its error flag, the host reads SIDR_ERR_KERNEL, and GEMMs on the
+    same context afterwards are still correct."""
+    for _ in range(2):
+        assert SG.gemm_wait_check(0, 1000) == 6
+    test_gemm_matches_float64(200, 48, 40, 1)
+    test_gemm_matches_float64(256, 256, 1024, 8)
+
+
 def params_of(m):
     return {k: m.param(k)[0].astype(np.float64) for k in SG.PARAM_NAMES}
 

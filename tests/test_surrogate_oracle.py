@@ -41,3 +41,9 @@ def test_bf16_rounding_is_nearest_even():
     # 1 + 2^-8 is halfway between 1 and 1 + 2^-7: ties to even (1.0)
     assert got[0] == 1.0 and got[1] == 1.0 and got[2] == 1.0078125
     assert got[3] == -3.0
+
+
+def test_gemm_wait_check_rejects_limits_before_any_device_work():
+    from sidr import surrogate as SG
+    assert SG.gemm_wait_check(0, 0) == 1
+    assert SG.gemm_wait_check(0, (1 << 20) + 1) == 1

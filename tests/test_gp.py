@@ -76,6 +76,8 @@ def test_run_multi_rejects_bad_arguments():
         gp.run_multi([w.sd], [zp], ["SCORE", "NOPE"], [w.mask], 2)
     with pytest.raises(sidr.SidrError):
         gp.run_multi([w.sd], [zp], workload.MENU29, [w.mask], 0)
+    with pytest.raises(sidr.SidrError):  # more populations than one launch's entries
+        gp.run_multi([w.sd] * 2, [zp] * 2, workload.MENU29, [w.mask] * 2, 20000, generations=1)
 
 
 def _fitness_of(sess):

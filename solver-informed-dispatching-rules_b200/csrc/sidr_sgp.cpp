@@ -9,8 +9,13 @@
 
 #include "../../include/sidr_surrogate.h"
 #include "sidr_gp_core.hpp"
+#include "sidr_sgp_select.hpp"
 
 using namespace sidr::gp;
+using sidr::sgp::best_distinct;
+using sidr::sgp::preselect;
+using sidr::sgp::spearman;
+using sidr::sgp::training_targets;
 
 namespace {
 
@@ -34,44 +39,6 @@ void pack_rules(const std::vector<Rule>& rules, const Vocab& v, Packed& pk) {
         compile_at(r, k, v, pk.ops, pk.args, pk.ops.size());
         pk.len.push_back((int32_t)pk.ops.size() - pk.off.back());
     }
-}
-
-// Ranks with ties sharing their average rank.
-std::vector<double> ranks_of(const std::vector<double>& x) {
-    const size_t n = x.size();
-    std::vector<size_t> o(n);
-    std::iota(o.begin(), o.end(), 0);
-    std::stable_sort(o.begin(), o.end(), [&](size_t a, size_t b) { return x[a] < x[b]; });
-    std::vector<double> r(n);
-    for (size_t i = 0; i < n;) {
-        size_t j = i;
-        while (j + 1 < n && x[o[j + 1]] == x[o[i]]) j++;
-        const double avg = 0.5 * (double)(i + j);
-        for (size_t k = i; k <= j; k++) r[o[k]] = avg;
-        i = j + 1;
-    }
-    return r;
-}
-
-// Spearman's rank correlation (Pearson correlation of the ranks).
-double spearman(const std::vector<double>& a, const std::vector<double>& b) {
-    const std::vector<double> ra = ranks_of(a), rb = ranks_of(b);
-    const double n = (double)a.size();
-    double ma = 0, mb = 0;
-    for (size_t i = 0; i < a.size(); i++) {
-        ma += ra[i];
-        mb += rb[i];
-    }
-    ma /= n;
-    mb /= n;
-    double sab = 0, saa = 0, sbb = 0;
-    for (size_t i = 0; i < a.size(); i++) {
-        sab += (ra[i] - ma) * (rb[i] - mb);
-        saa += (ra[i] - ma) * (ra[i] - ma);
-        sbb += (rb[i] - mb) * (rb[i] - mb);
-    }
-    if (saa <= 0 || sbb <= 0) return 0.0;
-    return sab / std::sqrt(saa * sbb);
 }
 
 }  // namespace
@@ -239,24 +206,13 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                 }
                 // train on the recent simulated fitness: standardised, or as
                 // uniform scores of its ranks over the whole history
-                std::vector<float> X, Y;
+                std::vector<float> X;
                 std::vector<double> all;
                 for (size_t h = 0; h < hist_x.size(); h++) {
                     X.insert(X.end(), hist_x[h].begin(), hist_x[h].end());
                     all.insert(all.end(), hist_t[h].begin(), hist_t[h].end());
                 }
-                const double cnt = (double)all.size();
-                if (sc->target == 1) {
-                    const std::vector<double> rk = ranks_of(all);
-                    for (double r : rk) Y.push_back((float)(((r + 0.5) / cnt - 0.5) * std::sqrt(12.0)));
-                } else {
-                    double mu = 0, sd = 0;
-                    for (double v : all) mu += v;
-                    mu /= cnt;
-                    for (double v : all) sd += (v - mu) * (v - mu);
-                    sd = std::sqrt(sd / cnt) + 1e-9;
-                    for (double v : all) Y.push_back((float)((v - mu) / sd));
-                }
+                std::vector<float> Y = training_targets(all, sc->target);
                 float loss = 0.0f;
                 double t0 = now_s();
                 st = sidr_mlp_train(model, X.data(), Y.data(), (int32_t)Y.size(), sc->train_steps, sc->batch,
@@ -296,42 +252,21 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                     for (int e = 0; e < cfg->elitism && e < ps; e++) next.push_back(gp.pop[order[e]]);
                     const int slots = ps - (int)next.size();
                     const int need = (int)std::lround(sc->screen_fraction * slots);
+                    std::vector<int> pick;
                     if (sc->selection == 1) {
                         // pre-selection: the best-predicted child of each group of
                         // screen/need consecutive (independently bred) children
-                        const int per = std::max(1, (int)cand.size() / std::max(need, 1));
-                        for (int q = 0; q < need; q++) {
-                            int b = q * per;
-                            for (int c = q * per + 1; c < (q + 1) * per && c < (int)cand.size(); c++)
-                                if (pred[c] > pred[b]) b = c;
-                            next.push_back(cand[b]);
-                        }
+                        pick = preselect(pred, need);
+                    } else if (sc->distinct == 1) {
+                        // the best-predicted children, one per ranking of the decision situations
+                        pick = best_distinct<std::vector<float>>(pred, (size_t)need, [&](int c) {
+                            return std::vector<float>(cf.begin() + (size_t)c * NF, cf.begin() + (size_t)c * NF + NS);
+                        });
                     } else {
-                        // global: the best-predicted distinct children (distinct
-                        // rules, or distinct rankings of the decision situations)
-                        std::vector<int> co(cand.size());
-                        std::iota(co.begin(), co.end(), 0);
-                        std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return pred[a] > pred[b]; });
-                        std::set<Rule> seen;
-                        std::set<std::vector<float>> seen_ph;
-                        std::vector<char> taken(cand.size(), 0);
-                        const size_t upto = next.size() + (size_t)need;
-                        for (size_t k = 0; next.size() < upto && k < co.size(); k++) {
-                            const int c = co[k];
-                            const bool fresh =
-                                sc->distinct == 1
-                                    ? seen_ph.insert(std::vector<float>(cf.begin() + (size_t)c * NF,
-                                                                        cf.begin() + (size_t)c * NF + NS))
-                                          .second
-                                    : seen.insert(cand[c]).second;
-                            if (fresh) {
-                                next.push_back(cand[c]);
-                                taken[c] = 1;
-                            }
-                        }
-                        for (size_t k = 0; next.size() < upto && k < co.size(); k++)
-                            if (!taken[co[k]]) next.push_back(cand[co[k]]);  // fewer distinct children than slots
+                        // the best-predicted distinct children
+                        pick = best_distinct<Rule>(pred, (size_t)need, [&](int c) { return cand[c]; });
                     }
+                    for (int c : pick) next.push_back(cand[c]);
                     if ((int)next.size() < ps) {
                         // the slots left to plain breeding
                         std::vector<Rule> plain = gp.breed(fit, (size_t)(ps - (int)next.size()));

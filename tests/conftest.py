@@ -15,7 +15,23 @@ for p in (PKG, os.path.join(REPO, "oracle"), REPO):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(REPO, "tests", "golden")
-REFERENCE_TREE = "/root/reference"
+
+
+def _reference_tree():
+    """The reference source tree: SIDR_REF, else the tree oracle/Makefile built
+    oracle/_ref from (it records the path in oracle/_ref/reference_tree.txt);
+    None when neither is known (on a machine without the tree the tests that
+    read it are skipped)."""
+    if os.environ.get("SIDR_REF"):
+        return os.environ["SIDR_REF"]
+    rec = os.path.join(REPO, "oracle", "_ref", "reference_tree.txt")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            return f.read().strip() or None
+    return None
+
+
+REFERENCE_TREE = _reference_tree()
 
 
 def pytest_configure(config):
@@ -46,6 +62,6 @@ def reference():
 
 @pytest.fixture(scope="session")
 def reference_tree():
-    if not os.path.isdir(os.path.join(REFERENCE_TREE, "instances")):
+    if not REFERENCE_TREE or not os.path.isdir(os.path.join(REFERENCE_TREE, "instances")):
         pytest.skip("reference tree not present")
     return REFERENCE_TREE

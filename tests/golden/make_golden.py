@@ -1,7 +1,10 @@
 """Regenerates the committed parity fixtures under tests/golden/ from the
 reference's own golden files and benchmark instances.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref REFERENCE_TREE]
+
+The reference tree comes from --ref, else the SIDR_REF environment variable, else
+the tree oracle/Makefile compiled oracle/_ref from (oracle/_ref/reference_tree.txt).
 
 Reads (never copies) the reference tree:
   verify/golden/sim.txt        12 cases (c101/r101/rc101/pr01 x ns11/ext29/full61):
@@ -210,15 +213,31 @@ def make_campaign(ref: str) -> dict:
     return out
 
 
+def recorded_reference_tree():
+    """SIDR_REF, else the tree oracle/Makefile built oracle/_ref from."""
+    if os.environ.get("SIDR_REF"):
+        return os.environ["SIDR_REF"]
+    rec = os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle", "_ref",
+                       "reference_tree.txt")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            return f.read().strip() or None
+    return None
+
+
 MAKERS = {"sim_cases": make_sim, "gp_cases": make_gp, "durations": make_durations,
           "compile": make_compile, "campaign": make_campaign}
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="the reference source tree")
     ap.add_argument("--only", nargs="*", choices=sorted(MAKERS), help="regenerate these only")
     a = ap.parse_args()
+    if a.ref is None:
+        a.ref = recorded_reference_tree()
+    if not a.ref or not os.path.isdir(a.ref):
+        raise SystemExit("reference tree unknown: pass --ref or set SIDR_REF")
     for name in a.only or list(MAKERS):
         fn = MAKERS[name]
         data = fn(a.ref)

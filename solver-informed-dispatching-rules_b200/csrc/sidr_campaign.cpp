@@ -4,6 +4,8 @@
 // and the train-side score of the cross-validatory choice
 // (s4_selection/choice.cu), on the host GP of sidr_gp_core.hpp and the B200
 // evaluator.
+#include <algorithm>
+#include <array>
 #include <atomic>
 #include <cctype>
 #include <charconv>
@@ -637,6 +639,372 @@ sidr_status copy_text(const std::string& s, char* buf, int64_t cap, int64_t* len
     return SIDR_OK;
 }
 
+// ------------------------------------------------------ vocabulary search
+//
+// The search over terminal subsets of s4_selection/ga.cu:288-523 in three
+// parts: a score store holding every evaluated genome's per-seed scores at the
+// two budgets (proxy and confirmation) and mirroring them in the resumable
+// cache file; a ranked hierarchy of 13 genomes; and the search, which breeds
+// one offspring along every parent/supporter link of the hierarchy per
+// generation.  Genomes are bit sets over the universe (bit b = universe[b]).
+// The search's generator draws in the reference's order (pool padding, then
+// per link: nb crossover draws and nb mutation draws), and its log lines and
+// cache file have the reference's text, so runs are comparable line for line.
+
+// Per-seed scores of genomes at the two evaluation budgets.
+class ScoreStore {
+public:
+    enum Budget { kProxy = 0, kConfirm = 1 };
+
+    explicit ScoreStore(std::string header) : header_(std::move(header)) {}
+    ~ScoreStore() {
+        if (file_) std::fclose(file_);
+    }
+    ScoreStore(const ScoreStore&) = delete;
+    ScoreStore& operator=(const ScoreStore&) = delete;
+
+    // Loads the entries of a cache file written under the same header (lines
+    // cut short are dropped: those genomes are evaluated again), then keeps
+    // the file open for appending; a file under another header is rewritten.
+    // Returns the number of entries loaded.
+    long attach(const char* path) {
+        long loaded = 0;
+        if (std::FILE* in = std::fopen(path, "r")) {
+            std::string row;
+            bool first = true, same_header = false;
+            while (read_row(in, row)) {
+                if (first) {
+                    same_header = row == header_;
+                    first = false;
+                    if (!same_header) break;
+                    continue;
+                }
+                loaded += parse_row(row) ? 1 : 0;
+            }
+            std::fclose(in);
+        }
+        file_ = std::fopen(path, loaded > 0 ? "a" : "w");
+        if (file_ && loaded == 0) std::fprintf(file_, "%s\n", header_.c_str());
+        return loaded;
+    }
+
+    bool has(Budget b, uint32_t g) const { return tab_[b].count(g) != 0; }
+    const std::vector<double>& at(Budget b, uint32_t g) const { return tab_[b].at(g); }
+    double mean(Budget b, uint32_t g) const { return mean_of(tab_[b].at(g)); }
+
+    void put(Budget b, uint32_t g, std::vector<double> v) {
+        if (file_) {
+            std::fprintf(file_, "%c %x %d", b == kProxy ? 'P' : 'C', g, (int)v.size());
+            for (double x : v) std::fprintf(file_, " %a", x);
+            std::fputc('\n', file_);
+        }
+        tab_[b][g] = std::move(v);
+    }
+    void sync() {
+        if (file_) std::fflush(file_);
+    }
+
+private:
+    static bool read_row(std::FILE* in, std::string& row) {
+        row.clear();
+        int c;
+        while ((c = std::fgetc(in)) != EOF && c != '\n') row += (char)c;
+        return !(c == EOF && row.empty());
+    }
+    // "<P|C> <genome hex> <count> <hexfloat> ..."
+    bool parse_row(const std::string& row) {
+        const char* p = row.c_str();
+        if ((p[0] != 'P' && p[0] != 'C') || p[1] != ' ') return false;
+        const Budget b = p[0] == 'P' ? kProxy : kConfirm;
+        char* end = nullptr;
+        const unsigned long g = std::strtoul(p + 2, &end, 16);
+        if (end == p + 2) return false;
+        const char* q = end;
+        const long count = std::strtol(q, &end, 10);
+        if (end == q || count < 0) return false;
+        std::vector<double> v;
+        for (q = end; (long)v.size() < count; q = end) {
+            const double x = std::strtod(q, &end);
+            if (end == q) return false;
+            v.push_back(x);
+        }
+        tab_[b][(uint32_t)g] = std::move(v);
+        return true;
+    }
+
+    std::string header_;
+    std::map<uint32_t, std::vector<double>> tab_[2];
+    std::FILE* file_ = nullptr;
+};
+
+// Thirteen genomes as a ternary heap of depth two: parent slot i (i = 0..3)
+// has the supporters 3i+1 .. 3i+3, so the root leads slots 1-3 and each of
+// those leads three leaves.  settle() restores the heap's order by passes
+// over the parents from the bottom (3, 2, 1, then the root): a parent swaps
+// places with its best supporter when that one scores strictly higher (of
+// equal bests, the first), and passes repeat until one moves nothing, at most
+// 13 times.
+struct RankedHierarchy {
+    static constexpr int kSlots = 13;
+    static constexpr int kParents = 4;
+    std::array<uint32_t, kSlots> g{};
+
+    static int supporter(int parent, int k) { return 3 * parent + 1 + k; }
+
+    template <class Score>
+    void settle(Score&& score) {
+        for (int pass = 0; pass < kSlots; pass++) {
+            bool moved = false;
+            for (int parent = kParents - 1; parent >= 0; parent--) {
+                int top = -1;
+                for (int k = 0; k < 3; k++) {
+                    const int s = supporter(parent, k);
+                    if (score(g[s]) > score(g[parent]) && (top < 0 || score(g[s]) > score(g[top]))) top = s;
+                }
+                if (top >= 0) {
+                    std::swap(g[parent], g[top]);
+                    moved = true;
+                }
+            }
+            if (!moved) return;
+        }
+    }
+    size_t distinct() const { return std::set<uint32_t>(g.begin(), g.end()).size(); }
+};
+
+// Scores lists of genomes at n seeds x ng inner generations, in chunks of at
+// most `bmax` genomes: through the caller's callback, or on the evaluator
+// (batch_score, Scorer::chunk).  Each chunk's size and time go to the log.
+struct ChunkedScoring {
+    sidr_ctx* ctx;
+    const sidr_instance_desc* inst;
+    const sidr_gp_config* cfg;
+    const Universe& uni;
+    int bmax;
+    sidr_vocab_fitness_fn callback;
+    void* user;
+    Log& log;
+    long evaluated = 0;
+    double seconds = 0.0;
+
+    sidr_status operator()(const std::vector<uint32_t>& gs, int n, int ng,
+                           std::vector<std::vector<double>>& res) {
+        res.assign(gs.size(), std::vector<double>(n));
+        for (size_t at = 0; at < gs.size(); at += bmax) {
+            const int kb = (int)std::min<size_t>(bmax, gs.size() - at);
+            std::vector<double> flat((size_t)kb * n);
+            const double t0 = now_s();
+            if (callback) {
+                if (callback(user, gs.data() + at, kb, n, ng, flat.data()) != 0)
+                    return gp_fail(SIDR_ERR_INVALID, "fitness callback failed");
+            } else {
+                Scorer sc{ctx, inst, *cfg, uni, SIDR_TRAIN_SEED, SIDR_TRAIN_N};
+                const sidr_status s = sc.chunk(gs.data() + at, kb, n, ng, flat.data());
+                if (s != SIDR_OK) return s;
+            }
+            const double dt = now_s() - t0;
+            for (int k = 0; k < kb; k++)
+                std::copy(flat.begin() + (size_t)k * n, flat.begin() + (size_t)(k + 1) * n, res[at + k].begin());
+            evaluated += kb;
+            seconds += dt;
+            log("  batch %d genomes @%d seeds | %.1fs | %.2fs/eval\n", kb, n, dt, dt / kb);
+        }
+        return SIDR_OK;
+    }
+};
+
+class VocabSearch {
+public:
+    VocabSearch(const sidr_vocab_ga_config& s, int cgens, const Universe& u, ScoreStore& store,
+                ChunkedScoring& scoring, Log& log)
+        : set_(s), cgens_(cgens), uni_(u), store_(store), scoring_(scoring), log_(log),
+          rng_((uint64_t)s.ga_seed) {}
+
+    struct Outcome {
+        uint32_t champion = 0;
+        double confirmed_mean = 0.0;
+    };
+
+    sidr_status run(const std::string& instance, Outcome& res) {
+        sidr_status st = seed_hierarchy(instance);
+        if (st != SIDR_OK) return st;
+        double record = proxy(h_.g[0]);
+        int flat_gens = 0;
+        for (int gen = 0; gen < set_.gens; gen++) {
+            report(("gen " + std::to_string(gen)).c_str(), true);
+            if ((st = breed_generation()) != SIDR_OK) return st;
+            if (proxy(h_.g[0]) > record) {
+                record = proxy(h_.g[0]);
+                flat_gens = 0;
+            } else if (++flat_gens >= set_.stag) {
+                log_("stop: stagnant %d gens\n", flat_gens);
+                break;
+            }
+        }
+        report("gen end", false);
+        return confirm_finalists(res);
+    }
+
+private:
+    double proxy(uint32_t g) const { return store_.mean(ScoreStore::kProxy, g); }
+    // ranking of the pool and the finalists: higher proxy mean, then fewer terminals
+    bool ranks_above(uint32_t a, uint32_t b) const {
+        const double fa = proxy(a), fb = proxy(b);
+        return fa != fb ? fa > fb : __builtin_popcount(a) < __builtin_popcount(b);
+    }
+
+    // Each universe bit on with probability 0.35.
+    uint32_t draw_genome() {
+        uint32_t g = 0;
+        for (int b = 0; b < uni_.nb; b++)
+            if (rng_.random() < 0.35) g |= 1u << b;
+        return g;
+    }
+    // Uniform crossover (bit b from x when the draw is < 0.5), then every bit
+    // flipped with probability pm / nb.
+    uint32_t offspring(uint32_t x, uint32_t y) {
+        uint32_t c = 0;
+        for (int b = 0; b < uni_.nb; b++) c |= (rng_.random() < 0.5 ? x : y) & (1u << b);
+        for (int b = 0; b < uni_.nb; b++)
+            if (rng_.random() < set_.pm / uni_.nb) c ^= 1u << b;
+        return c;
+    }
+
+    // Proxy scores for every genome of `gs` not scored yet (distinct, in
+    // ascending order).
+    sidr_status score_proxy(std::vector<uint32_t> gs) {
+        std::sort(gs.begin(), gs.end());
+        gs.erase(std::unique(gs.begin(), gs.end()), gs.end());
+        gs.erase(std::remove_if(gs.begin(), gs.end(), [&](uint32_t g) { return store_.has(ScoreStore::kProxy, g); }),
+                 gs.end());
+        if (gs.empty()) return SIDR_OK;
+        std::vector<std::vector<double>> res;
+        const sidr_status st = scoring_(gs, set_.proxy, set_.pgens, res);
+        if (st != SIDR_OK) return st;
+        for (size_t i = 0; i < gs.size(); i++) store_.put(ScoreStore::kProxy, gs[i], std::move(res[i]));
+        store_.sync();
+        return SIDR_OK;
+    }
+
+    // The starting pool: the neutral seeds when asked for (the empty set, the
+    // whole universe unless left out, every singleton), padded with random
+    // genomes to 13; scored, ranked, the best 13 placed in the hierarchy.
+    sidr_status seed_hierarchy(const std::string& instance) {
+        std::vector<uint32_t> pool;
+        if (set_.seeds_neutral) {
+            pool.push_back(0);
+            if (!set_.nofull) pool.push_back(uni_.nb >= 32 ? 0xffffffffu : (1u << uni_.nb) - 1u);
+            for (int b = 0; b < uni_.nb; b++) pool.push_back(1u << b);
+        }
+        std::sort(pool.begin(), pool.end());
+        pool.erase(std::unique(pool.begin(), pool.end()), pool.end());
+        const size_t n_seeded = pool.size();
+        while (pool.size() < (size_t)RankedHierarchy::kSlots) pool.push_back(draw_genome());
+        log_("# ga %s | universe %d | seeds %s (%zu)%s | tree-13 uniform-x pm %.2f | gens %d stag %d\n",
+             instance.c_str(), uni_.nb, set_.seeds_neutral ? "neutral" : "random", n_seeded,
+             set_.nofull ? " nofull" : "", set_.pm, set_.gens, set_.stag);
+        const sidr_status st = score_proxy(pool);
+        if (st != SIDR_OK) return st;
+        std::stable_sort(pool.begin(), pool.end(), [&](uint32_t a, uint32_t b) { return ranks_above(a, b); });
+        std::copy(pool.begin(), pool.begin() + RankedHierarchy::kSlots, h_.g.begin());
+        settle();
+        return SIDR_OK;
+    }
+
+    void settle() {
+        h_.settle([&](uint32_t g) { return proxy(g); });
+    }
+
+    void report(const char* label, bool with_distinct) {
+        double avg = 0.0;
+        for (uint32_t g : h_.g) avg += proxy(g);
+        avg /= RankedHierarchy::kSlots;
+        if (with_distinct)
+            log_("%s | best %.2f [%s] | mean %.2f | unique %zu | evals %ld\n", label, proxy(h_.g[0]),
+                 uni_.name_of(h_.g[0]).c_str(), avg, h_.distinct(), scoring_.evaluated);
+        else
+            log_("%s | best %.2f [%s] | mean %.2f | evals %ld\n", label, proxy(h_.g[0]),
+                 uni_.name_of(h_.g[0]).c_str(), avg, scoring_.evaluated);
+    }
+
+    // One generation: fresh genomes in the two last leaves when at most six
+    // of the 13 are distinct; one offspring per parent/supporter link (links
+    // in slot order), which takes the place of the link's weaker end (the
+    // supporter when they tie) if it scores strictly higher; then settle.
+    sidr_status breed_generation() {
+        sidr_status st;
+        if (h_.distinct() <= 6) {
+            const uint32_t a = draw_genome(), b = draw_genome();
+            h_.g[RankedHierarchy::kSlots - 1] = a;
+            h_.g[RankedHierarchy::kSlots - 2] = b;
+            if ((st = score_proxy({a, b})) != SIDR_OK) return st;
+            log_("  reinject 2\n");
+        }
+        struct Link {
+            int parent, sup;
+            uint32_t child;
+        };
+        std::vector<Link> links;
+        for (int parent = 0; parent < RankedHierarchy::kParents; parent++)
+            for (int k = 0; k < 3; k++) {
+                const int s = RankedHierarchy::supporter(parent, k);
+                links.push_back({parent, s, offspring(h_.g[parent], h_.g[s])});
+            }
+        std::vector<uint32_t> kids;
+        for (const Link& l : links) kids.push_back(l.child);
+        if ((st = score_proxy(kids)) != SIDR_OK) return st;
+        for (const Link& l : links) {
+            const int weaker = proxy(h_.g[l.sup]) <= proxy(h_.g[l.parent]) ? l.sup : l.parent;
+            if (proxy(l.child) > proxy(h_.g[weaker])) h_.g[weaker] = l.child;
+        }
+        settle();
+        return SIDR_OK;
+    }
+
+    // The hierarchy's distinct genomes, best-ranked first (ascending genome
+    // order among equals), the first `top` confirmed at `confirm` seeds with
+    // cgens inner generations; the champion has the highest confirmed mean
+    // (ties: fewer terminals, then rank).
+    sidr_status confirm_finalists(Outcome& res) {
+        const std::set<uint32_t> distinct(h_.g.begin(), h_.g.end());
+        std::vector<uint32_t> fin(distinct.begin(), distinct.end());
+        std::stable_sort(fin.begin(), fin.end(), [&](uint32_t a, uint32_t b) { return ranks_above(a, b); });
+        if ((int)fin.size() > set_.top) fin.resize(set_.top);
+        log_("\nconfirming top-%zu at %d seeds:\n", fin.size(), set_.confirm);
+        std::vector<uint32_t> todo;
+        for (uint32_t g : fin)
+            if (!store_.has(ScoreStore::kConfirm, g)) todo.push_back(g);
+        if (!todo.empty()) {
+            std::vector<std::vector<double>> scores;
+            const sidr_status st = scoring_(todo, set_.confirm, cgens_, scores);
+            if (st != SIDR_OK) return st;
+            for (size_t i = 0; i < todo.size(); i++) store_.put(ScoreStore::kConfirm, todo[i], std::move(scores[i]));
+            store_.sync();
+        }
+        size_t win = 0;
+        for (size_t i = 1; i < fin.size(); i++) {
+            const double m = store_.mean(ScoreStore::kConfirm, fin[i]);
+            const double mw = store_.mean(ScoreStore::kConfirm, fin[win]);
+            if (m > mw || (m == mw && __builtin_popcount(fin[i]) < __builtin_popcount(fin[win]))) win = i;
+        }
+        for (uint32_t g : fin)
+            log_("  %.2f (proxy %.2f) [%s]\n", store_.mean(ScoreStore::kConfirm, g), proxy(g),
+                 uni_.name_of(g).c_str());
+        res.champion = fin[win];
+        res.confirmed_mean = store_.mean(ScoreStore::kConfirm, fin[win]);
+        return SIDR_OK;
+    }
+
+    const sidr_vocab_ga_config& set_;
+    const int cgens_;
+    const Universe& uni_;
+    ScoreStore& store_;
+    ChunkedScoring& scoring_;
+    Log& log_;
+    Mt19937 rng_;
+    RankedHierarchy h_;
+};
+
 }  // namespace
 
 extern "C" {
@@ -750,276 +1118,33 @@ sidr_status sidr_vocab_ga(sidr_ctx* ctx, const sidr_instance_desc* inst,
     Universe u;
     sidr_status st = load_universe(base_csv, universe_csv, u);
     if (st != SIDR_OK) return st;
-    const int nb = u.nb;
-    Log out;
-    const std::string inst_s = instance_name;
+    Log text;
 
-    // batch_score with its per-chunk report (s4_selection/ga.cu:116-205)
-    long evals = 0;
-    double gpu_s = 0.0;
-    auto batch_score = [&](const std::vector<uint32_t>& gs, int n, int ng,
-                           std::vector<std::vector<double>>& res) -> sidr_status {
-        const int K = (int)gs.size();
-        res.assign(K, std::vector<double>(n));
-        for (int k0 = 0; k0 < K; k0 += ga->bmax) {
-            const int kb = std::min(ga->bmax, K - k0);
-            const double t0 = now_s();
-            std::vector<double> flat((size_t)kb * n);
-            if (fitness) {
-                if (fitness(user, gs.data() + k0, kb, n, ng, flat.data()) != 0)
-                    return gp_fail(SIDR_ERR_INVALID, "fitness callback failed");
-            } else {
-                Scorer sc{ctx, inst, *cfg, u, SIDR_TRAIN_SEED, SIDR_TRAIN_N};
-                const sidr_status s2 = sc.chunk(gs.data() + k0, kb, n, ng, flat.data());
-                if (s2 != SIDR_OK) return s2;
-            }
-            for (int k = 0; k < kb; k++)
-                res[k0 + k].assign(flat.begin() + (size_t)k * n, flat.begin() + (size_t)(k + 1) * n);
-            evals += kb;
-            const double dt = now_s() - t0;
-            gpu_s += dt;
-            out("  batch %d genomes @%d seeds | %.1fs | %.2fs/eval\n", kb, n, dt, dt / kb);
-        }
-        return SIDR_OK;
-    };
-
-    // evaluation cache (s4_selection/ga.cu:315-377)
-    std::map<uint32_t, std::vector<double>> cache, cache_conf;
-    std::string uni_join;
-    for (int b = 0; b < nb; b++) uni_join += (b ? "," : "") + u.uni[b];
-    char cache_hdr[512];
-    std::snprintf(cache_hdr, sizeof cache_hdr, "# gacache v1 %s uni=%s proxy=%d pgens=%d confirm=%d cgens=%d",
-                  inst_s.c_str(), uni_join.c_str(), ga->proxy, ga->pgens, ga->confirm, cfg->generations);
-    std::FILE* cache_fp = nullptr;
+    // the cache file's header names everything its scores depend on (s4_selection/ga.cu:315-377)
+    std::string names;
+    for (int b = 0; b < u.nb; b++) names += (b ? "," : "") + u.uni[b];
+    char header[512];
+    std::snprintf(header, sizeof header, "# gacache v1 %s uni=%s proxy=%d pgens=%d confirm=%d cgens=%d",
+                  instance_name, names.c_str(), ga->proxy, ga->pgens, ga->confirm, cfg->generations);
+    ScoreStore store(header);
     if (cache_path && *cache_path) {
-        long hits = 0;
-        if (std::FILE* in = std::fopen(cache_path, "r")) {
-            std::string line;
-            auto getline = [&](std::string& l) {
-                l.clear();
-                int c;
-                while ((c = std::fgetc(in)) != EOF && c != '\n') l += (char)c;
-                return !(c == EOF && l.empty());
-            };
-            if (getline(line) && line == cache_hdr) {
-                while (getline(line)) {
-                    const char* p = line.c_str();
-                    char kind[4] = {0};
-                    char hex[16] = {0};
-                    int n = 0, used = 0;
-                    if (std::sscanf(p, "%3s %15s %d%n", kind, hex, &n, &used) != 3) continue;
-                    if (std::strcmp(kind, "P") != 0 && std::strcmp(kind, "C") != 0) continue;
-                    const uint32_t g = (uint32_t)std::strtoul(hex, nullptr, 16);
-                    std::vector<double> v;
-                    const char* q = p + used;
-                    while ((int)v.size() < n) {
-                        char* endp = nullptr;
-                        const double x = std::strtod(q, &endp);
-                        if (endp == q) break;
-                        v.push_back(x);
-                        q = endp;
-                    }
-                    if ((int)v.size() != n) continue;  // a line cut short: recomputed
-                    (kind[0] == 'P' ? cache : cache_conf)[g] = v;
-                    hits++;
-                }
-            }
-            std::fclose(in);
-        }
-        cache_fp = std::fopen(cache_path, hits > 0 ? "a" : "w");
-        if (cache_fp && hits == 0) std::fprintf(cache_fp, "%s\n", cache_hdr);
-        if (hits > 0) out("# cache %s | %ld entries loaded\n", cache_path, hits);
+        const long loaded = store.attach(cache_path);
+        if (loaded > 0) text("# cache %s | %ld entries loaded\n", cache_path, loaded);
     }
-    auto cache_append = [&](const char* kind, uint32_t g, const std::vector<double>& v) {
-        if (!cache_fp) return;
-        std::fprintf(cache_fp, "%s %x %d", kind, g, (int)v.size());
-        for (double x : v) std::fprintf(cache_fp, " %a", x);
-        std::fprintf(cache_fp, "\n");
-    };
-    auto finish = [&](sidr_status s) {
-        if (cache_fp) std::fclose(cache_fp);
-        return s;
-    };
-
-    auto ensure = [&](std::vector<uint32_t> want) -> sidr_status {
-        std::sort(want.begin(), want.end());
-        want.erase(std::unique(want.begin(), want.end()), want.end());
-        std::vector<uint32_t> miss;
-        for (uint32_t g : want)
-            if (!cache.count(g)) miss.push_back(g);
-        if (miss.empty()) return SIDR_OK;
-        std::vector<std::vector<double>> res;
-        const sidr_status s2 = batch_score(miss, ga->proxy, ga->pgens, res);
-        if (s2 != SIDR_OK) return s2;
-        for (size_t i = 0; i < miss.size(); i++) {
-            cache[miss[i]] = res[i];
-            cache_append("P", miss[i], res[i]);
-        }
-        if (cache_fp) std::fflush(cache_fp);
-        return SIDR_OK;
-    };
-    auto mean_c = [&](uint32_t g) { return mean_of(cache[g]); };
-
-    // initial pool (:379-400)
-    Mt19937 rng((uint64_t)ga->ga_seed);
-    std::vector<uint32_t> seeds;
-    const uint32_t full = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
-    if (ga->seeds_neutral) {
-        seeds.push_back(0);
-        if (!ga->nofull) seeds.push_back(full);
-        for (int b = 0; b < nb; b++) seeds.push_back(1u << b);
-    }
-    std::sort(seeds.begin(), seeds.end());
-    seeds.erase(std::unique(seeds.begin(), seeds.end()), seeds.end());
-    const int NP = 13;
-    auto random_genome = [&]() {
-        uint32_t g = 0;
-        for (int b = 0; b < nb; b++)
-            if (rng.random() < 0.35) g |= 1u << b;
-        return g;
-    };
-    std::vector<uint32_t> pool = seeds;
-    while ((int)pool.size() < NP) pool.push_back(random_genome());
-    out("# ga %s | universe %d | seeds %s (%zu)%s | tree-13 uniform-x pm %.2f | gens %d stag %d\n",
-        inst_s.c_str(), nb, ga->seeds_neutral ? "neutral" : "random", seeds.size(),
-        ga->nofull ? " nofull" : "", ga->pm, ga->gens, ga->stag);
-    const double t_start = now_s();
-    if ((st = ensure(pool)) != SIDR_OK) return finish(st);
-    auto better = [&](uint32_t a, uint32_t b) {
-        const double fa = mean_c(a), fb = mean_c(b);
-        if (fa != fb) return fa > fb;
-        return nbits(a) < nbits(b);
-    };
-    std::stable_sort(pool.begin(), pool.end(), better);
-    pool.resize(NP);
-    std::vector<uint32_t> tree(pool.begin(), pool.end());
-
-    // ternary tree: slot 0 root, 1-3 mids, 4-12 leaves (:402-425)
-    auto restore = [&]() {
-        for (int pass = 0; pass < NP; pass++) {
-            bool moved = false;
-            for (int c = 3; c >= 0; c--) {
-                const int lead = c == 0 ? 0 : c;
-                const int base = c == 0 ? 1 : 4 + 3 * (c - 1);
-                int best = -1;
-                for (int j = 0; j < 3; j++) {
-                    const int idx = base + j;
-                    if (mean_c(tree[idx]) > mean_c(tree[lead]))
-                        if (best < 0 || mean_c(tree[idx]) > mean_c(tree[best])) best = idx;
-                }
-                if (best >= 0) {
-                    std::swap(tree[lead], tree[best]);
-                    moved = true;
-                }
-            }
-            if (!moved) break;
-        }
-    };
-    restore();
-
-    // uniform crossover, then per-gene mutation at pm/nb (:427-437)
-    auto cross_mut = [&](uint32_t a, uint32_t b) {
-        uint32_t child = 0;
-        for (int k = 0; k < nb; k++) child |= (rng.random() < 0.5 ? a : b) & (1u << k);
-        for (int k = 0; k < nb; k++)
-            if (rng.random() < ga->pm / nb) child ^= 1u << k;
-        return child;
-    };
-
-    double best_seen = mean_c(tree[0]);
-    int stag = 0;
-    for (int gen = 0; gen < ga->gens; gen++) {
-        const std::set<uint32_t> uniq(tree.begin(), tree.end());
-        double pmean = 0.0;
-        for (int i = 0; i < NP; i++) pmean += mean_c(tree[i]);
-        pmean /= NP;
-        out("gen %d | best %.2f [%s] | mean %.2f | unique %zu | evals %ld\n", gen, mean_c(tree[0]),
-            u.name_of(tree[0]).c_str(), pmean, uniq.size(), evals);
-        if ((int)uniq.size() <= 6) {
-            std::vector<uint32_t> fresh;
-            for (int r = 0; r < 2; r++) {
-                const uint32_t g = random_genome();
-                tree[12 - r] = g;
-                fresh.push_back(g);
-            }
-            if ((st = ensure(fresh)) != SIDR_OK) return finish(st);
-            out("  reinject 2\n");
-        }
-        std::vector<uint32_t> children;
-        std::vector<std::pair<int, int>> pairs;
-        for (int c = 0; c < 4; c++) {
-            const int lead = c == 0 ? 0 : c;
-            const int base = c == 0 ? 1 : 4 + 3 * (c - 1);
-            for (int j = 0; j < 3; j++) {
-                const int sup = base + j;
-                children.push_back(cross_mut(tree[lead], tree[sup]));
-                pairs.push_back({lead, sup});
-            }
-        }
-        if ((st = ensure(children)) != SIDR_OK) return finish(st);
-        for (size_t i = 0; i < children.size(); i++) {
-            const int lead = pairs[i].first, sup = pairs[i].second;
-            const int wp = mean_c(tree[sup]) <= mean_c(tree[lead]) ? sup : lead;
-            if (mean_c(children[i]) > mean_c(tree[wp])) tree[wp] = children[i];
-        }
-        restore();
-        const double cur = mean_c(tree[0]);
-        if (cur > best_seen) {
-            best_seen = cur;
-            stag = 0;
-        } else {
-            stag++;
-        }
-        if (stag >= ga->stag) {
-            out("stop: stagnant %d gens\n", stag);
-            break;
-        }
-    }
-    {
-        double pmean = 0.0;
-        for (int i = 0; i < NP; i++) pmean += mean_c(tree[i]);
-        pmean /= NP;
-        out("gen end | best %.2f [%s] | mean %.2f | evals %ld\n", mean_c(tree[0]), u.name_of(tree[0]).c_str(),
-            pmean, evals);
-    }
-
-    // finalists confirmed at `confirm` seeds (:482-516)
-    std::vector<uint32_t> fin_g(tree.begin(), tree.end());
-    std::sort(fin_g.begin(), fin_g.end());
-    fin_g.erase(std::unique(fin_g.begin(), fin_g.end()), fin_g.end());
-    std::stable_sort(fin_g.begin(), fin_g.end(), better);
-    if ((int)fin_g.size() > ga->top) fin_g.resize(ga->top);
-    out("\nconfirming top-%zu at %d seeds:\n", fin_g.size(), ga->confirm);
-    std::vector<uint32_t> cmiss;
-    for (uint32_t g : fin_g)
-        if (!cache_conf.count(g)) cmiss.push_back(g);
-    if (!cmiss.empty()) {
-        std::vector<std::vector<double>> cres;
-        if ((st = batch_score(cmiss, ga->confirm, cfg->generations, cres)) != SIDR_OK) return finish(st);
-        for (size_t i = 0; i < cmiss.size(); i++) {
-            cache_conf[cmiss[i]] = cres[i];
-            cache_append("C", cmiss[i], cres[i]);
-        }
-        if (cache_fp) std::fflush(cache_fp);
-    }
-    std::vector<std::vector<double>> conf;
-    for (uint32_t g : fin_g) conf.push_back(cache_conf[g]);
-    int bi = 0;
-    for (size_t i = 1; i < fin_g.size(); i++) {
-        const double a = mean_of(conf[i]), b = mean_of(conf[bi]);
-        if (a > b || (a == b && nbits(fin_g[i]) < nbits(fin_g[bi]))) bi = (int)i;
-    }
-    for (size_t i = 0; i < fin_g.size(); i++)
-        out("  %.2f (proxy %.2f) [%s]\n", mean_of(conf[i]), mean_c(fin_g[i]), u.name_of(fin_g[i]).c_str());
-    const double wall = now_s() - t_start;
-    out("\nCHAMPION train-%d %.2f | evals %ld | terms: %s\n", ga->confirm, mean_of(conf[bi]), evals,
-        u.name_of(fin_g[bi]).c_str());
-    out("PERF evals %ld | wall %.0fs | %.1fs/eval | batch-gpu %.0fs\n", evals, wall,
-        wall / std::max(1L, evals), gpu_s);
-    if (champion) *champion = fin_g[bi];
-    if (champion_mean) *champion_mean = mean_of(conf[bi]);
-    if (evals_out) *evals_out = evals;
-    return finish(copy_text(out.text, log, log_cap, log_len));
+    ChunkedScoring scoring{ctx, inst, cfg, u, ga->bmax, fitness, user, text};
+    VocabSearch search(*ga, cfg->generations, u, store, scoring, text);
+    const double t0 = now_s();
+    VocabSearch::Outcome res;
+    if ((st = search.run(instance_name, res)) != SIDR_OK) return st;
+    const double wall = now_s() - t0;
+    text("\nCHAMPION train-%d %.2f | evals %ld | terms: %s\n", ga->confirm, res.confirmed_mean,
+         scoring.evaluated, u.name_of(res.champion).c_str());
+    text("PERF evals %ld | wall %.0fs | %.1fs/eval | batch-gpu %.0fs\n", scoring.evaluated, wall,
+         wall / std::max(1L, scoring.evaluated), scoring.seconds);
+    if (champion) *champion = res.champion;
+    if (champion_mean) *champion_mean = res.confirmed_mean;
+    if (evals_out) *evals_out = scoring.evaluated;
+    return copy_text(text.text, log, log_cap, log_len);
 }
 
 sidr_status sidr_gen_trace(sidr_ctx* ctx, const sidr_instance_desc* inst,

@@ -204,13 +204,29 @@ sidr_status sidr_rules_check(const sidr_rules_desc* rules, const int64_t* masks,
  * which keeps the last call's contents; each call clears what must start at
  * zero.  Calls that overlapped on the GPU would race on the array, so each
  * call holds a process-wide lock from its first copy to its last and returns
- * only after the scores are in `out`. */
+ * only after the scores are in `out`.  The work runs on a non-blocking
+ * stream the library creates once per device (no implicit synchronisation
+ * with the caller's legacy-stream work), the caller's current device is
+ * restored on return, and the array's device address is kept for the life of
+ * the process: a cudaDeviceReset between calls is not supported.  A kernel
+ * error word raised during the call returns SIDR_ERR_KERNEL. */
 #define SIDR_STATIC_SCRATCH_BYTES (16u << 20)
 #define SIDR_STATIC_MAX_N 128
 sidr_status sidr_evaluate_static(const sidr_instance_desc* inst, const double zp[10],
                                  const sidr_rules_desc* rules, const double* grouped_sampled,
                                  int32_t G, int32_t T, int32_t group_size, int32_t mask_group,
                                  const int64_t* masks, int32_t device, double* out);
+
+/* Device-side guard check (diagnostic; no reference counterpart).  The
+ * evaluator kernel checks each rule record against the shared-memory slice
+ * its launch was sized for before staging it; a record that does not fit is
+ * refused (its scores become NaN) and the launch raises the kernel error
+ * word, which every host path reads back as SIDR_ERR_KERNEL.  Host
+ * validation makes that unreachable in normal calls; this entry launches the
+ * batch with its slice capacities set to zero, so every rule with at least
+ * one instruction is refused.  Expected result: SIDR_ERR_KERNEL, with the
+ * batch still usable by sidr_batch_run afterwards. */
+sidr_status sidr_batch_guard_check(sidr_batch* b);
 
 /* Number of kernel launches issued by this library since load (evaluator
  * and per-rule fitness kernels). */
@@ -231,6 +247,11 @@ sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s);
  * of CUDA's, on host arrays x[n] -> out[n] (diagnostic; no reference
  * counterpart).  They reproduce glibc 2.39's results bit for bit. */
 sidr_status sidr_libm_eval(int32_t fn, const double* x, int64_t n, int device, double* out);
+
+/* The device pow that the evaluator uses for rmod (engine/sim_core.hpp:30-35)
+ * in place of CUDA's: out[i] = x[i]^y[i] on host arrays (diagnostic; no
+ * reference counterpart).  It reproduces glibc 2.39's pow bit for bit. */
+sidr_status sidr_libm_pow(const double* x, const double* y, int64_t n, int device, double* out);
 
 #ifdef __cplusplus
 }

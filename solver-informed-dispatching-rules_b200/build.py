@@ -31,7 +31,7 @@ CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall"]
 CU_SOURCES = ["sidr_capi.cu", "sidr_surrogate.cu"]
 CPP_SOURCES = ["sidr_host.cpp", "sidr_gp.cpp", "sidr_campaign.cpp", "sidr_sgp.cpp"]
 HEADERS = ["sidr_internal.hpp", "sidr_kernel.cuh", "sidr_host.hpp", "sidr_libm.cuh", "sidr_exp_table.h",
-           "sidr_gp_core.hpp", "sidr_mlp.cuh", "sidr_sgp_select.hpp"]
+           "sidr_gp_core.hpp", "sidr_mlp.cuh", "sidr_sgp_select.hpp", "sidr_device.hpp"]
 PUBLIC_HEADERS = ["sidr.h", "sidr_gp.h", "sidr_campaign.h", "sidr_surrogate.h"]
 
 

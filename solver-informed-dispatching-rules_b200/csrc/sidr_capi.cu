@@ -22,6 +22,7 @@
 
 #include "../../include/sidr.h"
 #include "../../include/sidr_surrogate.h"
+#include "sidr_device.hpp"
 #include "sidr_host.hpp"
 #include "sidr_kernel.cuh"
 
@@ -227,6 +228,25 @@ cudaError_t upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t st) {
     return cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
 }
 
+const char* kernel_error_text(int code) {
+    switch (code) {
+    case kErrRuleRecord: return "a rule record exceeds the launch's shared-memory slice";
+    case kErrRuleIndex: return "a work item names a rule outside the batch";
+    case kErrInstance: return "a rule names an instance outside the batch";
+    }
+    return "unknown kernel error code";
+}
+
+// Reads the kernel error word once the stream's work is done (this syncs the
+// stream); SIDR_ERR_KERNEL when a launch raised it.
+sidr_status read_error_word(const int* dev_word, cudaStream_t st) {
+    int h = 0;
+    SIDR_CUDA(cudaMemcpyAsync(&h, dev_word, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SIDR_CUDA(cudaStreamSynchronize(st));
+    if (h) return fail(SIDR_ERR_KERNEL, std::string("evaluator kernel: ") + kernel_error_text(h));
+    return SIDR_OK;
+}
+
 // Launch geometry for a program set: warps per block bounded by the shared
 // memory each warp's slice takes; one persistent grid over all SMs.
 sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bool counting,
@@ -251,6 +271,7 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
 sidr_status launch(sidr_ctx* c, const DevBatch& b, bool counting, int grid, int block, size_t smem,
                    cudaStream_t st) {
     SIDR_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), st));
+    if (b.error) SIDR_CUDA(cudaMemsetAsync(b.error, 0, sizeof(int), st));
     if (counting && b.stats) SIDR_CUDA(cudaMemsetAsync(b.stats, 0, kStats * sizeof(unsigned long long), st));
     if ((long long)b.P * b.T == 0) return SIDR_OK;
     if (counting) eval_kernel<true><<<grid, block, smem, st>>>(c->inst, b);
@@ -314,6 +335,7 @@ sidr_status evaluate_common(sidr_ctx* c, const sidr_rules_desc* r, const double*
     g_h2d = (long long)(hp.prog.size() * 4 + hp.consts.size() * 8 + hp.slots.size() +
                         hp.meta.size() * sizeof(RuleMeta) + n_smp * 8);
     g_d2h = (long long)P * T * 8;
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     SIDR_CUDA(upload(c->prog, hp.prog, st));
@@ -350,8 +372,7 @@ sidr_status evaluate_common(sidr_ctx* c, const sidr_rules_desc* r, const double*
     s = launch(c, b, false, grid, block, smem, st);
     if (s) return s;
     SIDR_CUDA(cudaMemcpyAsync(out, c->out.p, (size_t)P * T * sizeof(double), cudaMemcpyDeviceToHost, st));
-    SIDR_CUDA(cudaStreamSynchronize(st));
-    return SIDR_OK;
+    return read_error_word(b.error, st);
 }
 
 }  // namespace
@@ -386,6 +407,7 @@ sidr_status sidr_last_transfer_bytes(int64_t* h2d, int64_t* d2h) {
 
 sidr_status sidr_fp64_peak(int device, int reps, double* ops_per_s) {
     if (!ops_per_s) return fail(SIDR_ERR_INVALID, "null argument");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(device));
     int sms = 0;
     SIDR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -429,6 +451,7 @@ sidr_status sidr_capture_situations(sidr_ctx* c, const sidr_rules_desc* r, const
     if ((s = compile_all(r, mask, 1, hp, nullptr, true))) return s;
     const int K = hp.meta[0].K;
     std::vector<int> slot_of(hp.slots.begin(), hp.slots.begin() + K);  // row -> slot
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     SIDR_CUDA(upload(c->prog, hp.prog, st));
@@ -491,6 +514,7 @@ sidr_status sidr_capture_situations(sidr_ctx* c, const sidr_rules_desc* r, const
     cudaFree(d_cust);
     cudaFree(d_info);
     if (e) return fail(SIDR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    if ((s = read_error_word(b.error, st))) return s;
     // rows -> 61-slot tables: captured slots, C1..C5 where active, zero elsewhere
     static const double kC[5] = {0.1, 0.2, 0.3, 0.4, 0.5};
     for (size_t q = 0; q < cand_n; q++) {
@@ -515,6 +539,7 @@ __global__ void libm_kernel(int fn, const double* x, long long n, double* out) {
 sidr_status sidr_libm_eval(int32_t fn, const double* x, int64_t n, int device, double* out) {
     if (fn < 0 || fn > 2 || n < 0 || (n > 0 && (!x || !out))) return fail(SIDR_ERR_INVALID, "bad argument");
     if (n == 0) return SIDR_OK;
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(device));
     double *dx = nullptr, *dout = nullptr;
     SIDR_CUDA(cudaMalloc(&dx, (size_t)n * sizeof(double)));
@@ -528,6 +553,31 @@ sidr_status sidr_libm_eval(int32_t fn, const double* x, int64_t n, int device, d
     cudaFree(dx);
     cudaFree(dout);
     if (e != cudaSuccess) return fail(SIDR_ERR_CUDA, std::string("libm eval: ") + cudaGetErrorString(e));
+    return SIDR_OK;
+}
+
+__global__ void libm_pow_kernel(const double* x, const double* y, long long n, double* out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = libm::pow_(x[i], y[i]);
+}
+
+sidr_status sidr_libm_pow(const double* x, const double* y, int64_t n, int device, double* out) {
+    if (n < 0 || (n > 0 && (!x || !y || !out))) return fail(SIDR_ERR_INVALID, "bad argument");
+    if (n == 0) return SIDR_OK;
+    DeviceGuard device_guard;
+    SIDR_CUDA(cudaSetDevice(device));
+    double* d = nullptr;  // x, y, out
+    SIDR_CUDA(cudaMalloc(&d, 3 * (size_t)n * sizeof(double)));
+    cudaError_t e = cudaMemcpy(d, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + n, y, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        libm_pow_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256>>>(d, d + n, n, d + 2 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 2 * n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(SIDR_ERR_CUDA, std::string("libm pow: ") + cudaGetErrorString(e));
     return SIDR_OK;
 }
 
@@ -583,6 +633,7 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         sidr_ctx_destroy(c);
         return fail(SIDR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
     };
+    DeviceGuard device_guard;
     cudaError_t err = cudaSetDevice(device);
     if (err != cudaSuccess) return bail(err, "cudaSetDevice");
     int v = 0;
@@ -646,6 +697,7 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
 
 void sidr_ctx_destroy(sidr_ctx* c) {
     if (!c) return;
+    DeviceGuard device_guard;
     cudaSetDevice(c->device);
     for (void* p : c->owned) cudaFree(p);
     for (DevBuf* b : {&c->prog, &c->consts, &c->slots, &c->meta, &c->sampled, &c->out, &c->counter,
@@ -701,6 +753,7 @@ sidr_status sidr_batch_create(sidr_ctx* c, const sidr_rules_desc* r, const doubl
         hp.consts.push_back(0.0);
         hp.slots.push_back(0);
     }
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(c->device));
     sidr_batch* bt = new sidr_batch();
     bt->ctx = c;
@@ -775,6 +828,7 @@ sidr_status sidr_batch_set_counting(sidr_batch* b, int enable) {
 sidr_status sidr_batch_run(sidr_batch* bt, void* stream) {
     NvtxRange range("sidr_batch_run");
     if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
     cudaStream_t st = (cudaStream_t)stream;  // 0 = the legacy default stream
     sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->grid, bt->block, bt->smem, st);
@@ -793,20 +847,36 @@ sidr_status sidr_batch_read(sidr_batch* bt, double* out) {
     if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
     if ((size_t)bt->P * bt->T == 0) return SIDR_OK;
     if (!out) return fail(SIDR_ERR_INVALID, "output buffer is null");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
     SIDR_CUDA(cudaDeviceSynchronize());
     SIDR_CUDA(cudaMemcpy(out, bt->out.p, (size_t)bt->P * bt->T * sizeof(double), cudaMemcpyDeviceToHost));
-    return SIDR_OK;
+    return read_error_word(bt->b.error, 0);
 }
 
 sidr_status sidr_batch_fitness(sidr_batch* bt, double* fitness) {
     if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
     if (bt->P == 0) return SIDR_OK;
     if (!fitness) return fail(SIDR_ERR_INVALID, "fitness buffer is null");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
     SIDR_CUDA(cudaDeviceSynchronize());
     SIDR_CUDA(cudaMemcpy(fitness, bt->fit.p, (size_t)bt->P * sizeof(double), cudaMemcpyDeviceToHost));
-    return SIDR_OK;
+    return read_error_word(bt->b.error, 0);
+}
+
+sidr_status sidr_batch_guard_check(sidr_batch* bt) {
+    if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
+    if ((long long)bt->P * bt->T == 0) return fail(SIDR_ERR_INVALID, "empty batch");
+    DeviceGuard device_guard;
+    SIDR_CUDA(cudaSetDevice(bt->ctx->device));
+    DevBatch b = bt->b;
+    b.prog_cap = 0;  // slices with room for no instruction and the minimum of rows
+    b.rows = 0;
+    cudaStream_t st = bt->ctx->stream;
+    sidr_status s = launch(bt->ctx, b, false, bt->grid, bt->block, bt->smem, st);
+    if (s) return s;
+    return read_error_word(b.error, st);
 }
 
 const double* sidr_batch_device_out(const sidr_batch* bt) { return bt ? (const double*)bt->out.p : nullptr; }
@@ -814,6 +884,7 @@ const double* sidr_batch_device_out(const sidr_batch* bt) { return bt ? (const d
 sidr_status sidr_batch_counts(sidr_batch* bt, sidr_counts* out) {
     if (!bt || !out) return fail(SIDR_ERR_INVALID, "null argument");
     unsigned long long v[kStats] = {};
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
     SIDR_CUDA(cudaDeviceSynchronize());
     SIDR_CUDA(cudaMemcpy(v, bt->stats.p, sizeof v, cudaMemcpyDeviceToHost));
@@ -828,6 +899,7 @@ sidr_status sidr_batch_counts(sidr_batch* bt, sidr_counts* out) {
 
 void sidr_batch_destroy(sidr_batch* bt) {
     if (!bt) return;
+    DeviceGuard device_guard;
     cudaSetDevice(bt->ctx->device);
     cudaDeviceSynchronize();
     for (DevBuf* b : {&bt->prog, &bt->consts, &bt->slots, &bt->meta, &bt->sampled, &bt->out,
@@ -859,7 +931,11 @@ extern "C" int sidr_section_cycles_take(unsigned long long* out16) {
 // library holds until the process exits.  In host code the name
 // sidr_static_scratch is only a host-side stand-in, not a device address: the
 // address comes from cudaGetSymbolAddress, looked up once per device with that
-// device current, and is passed to the kernel inside DevInst/DevBatch.
+// device current, and is passed to the kernel inside DevInst/DevBatch.  The
+// address is kept for the life of the process, so a cudaDeviceReset between
+// calls is not supported.  The copies, the launch and the wait run on a
+// non-blocking stream the library creates once per device, so a call does not
+// synchronise with work the caller has queued on the legacy default stream.
 
 namespace {
 
@@ -867,6 +943,7 @@ static __device__ __align__(256) unsigned char sidr_static_scratch[SIDR_STATIC_S
 
 std::mutex g_static_lock;                 // serialises every use of the array
 unsigned char* g_static_ptr[256] = {};    // device address per device index
+cudaStream_t g_static_stream[256] = {};   // the library's own non-blocking stream per device
 
 // Byte layout of one call inside the array.
 struct StaticLayout {
@@ -967,14 +1044,17 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
     }
     if (device < 0 || device >= ndev || device >= 256)
         return fail(SIDR_ERR_INVALID, "device index out of range");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(device));
     if (!g_static_ptr[device]) {  // once per device, with that device current
         void* ptr = nullptr;
         SIDR_CUDA(cudaGetSymbolAddress(&ptr, sidr_static_scratch));
         g_static_ptr[device] = static_cast<unsigned char*>(ptr);
     }
+    if (!g_static_stream[device])  // a non-blocking stream: no implicit sync with the legacy stream
+        SIDR_CUDA(cudaStreamCreateWithFlags(&g_static_stream[device], cudaStreamNonBlocking));
     unsigned char* base = g_static_ptr[device];
-    cudaStream_t st = 0;  // legacy default stream
+    cudaStream_t st = g_static_stream[device];
     for (const Piece& p : up) {
         *p.dst = base + p.at;
         SIDR_CUDA(cudaMemcpyAsync(base + p.at, p.src, p.bytes, cudaMemcpyHostToDevice, st));
@@ -996,7 +1076,6 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
     b.rows = hp.rows;
     b.prog_cap = hp.prog_cap;
     b.const_cap = hp.const_cap;
-    SIDR_CUDA(cudaMemsetAsync(base + at_error, 0, sizeof(int), st));  // launch() clears the counter
 
     // Launch geometry from the device's own attributes (no context here).
     sidr_ctx geo;
@@ -1014,7 +1093,8 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
     s = launch(&geo, b, false, grid, block, smem, st);
     if (s) return s;
     SIDR_CUDA(cudaMemcpyAsync(out, base + at_out, (size_t)P * T * 8, cudaMemcpyDeviceToHost, st));
-    SIDR_CUDA(cudaStreamSynchronize(st));
+    s = read_error_word(b.error, st);  // waits for the call's work; launch() cleared the word
+    if (s) return s;
     g_h2d = 0;
     for (const Piece& p : up) g_h2d += (long long)p.bytes;
     g_d2h = (long long)P * T * 8;
@@ -1061,6 +1141,7 @@ namespace {
 
 void multi_free(sidr_multi* m) {
     if (!m) return;
+    DeviceGuard device_guard;
     cudaSetDevice(m->device);
     cudaDeviceSynchronize();
     if (m->gexec) cudaGraphExecDestroy(m->gexec);
@@ -1082,6 +1163,7 @@ cudaError_t put_dev(sidr_multi* m, const void* src, size_t bytes, const void** d
 
 sidr_status multi_launch(sidr_multi* m, int shape, cudaStream_t st) {
     SIDR_CUDA(cudaMemsetAsync(m->b.counter, 0, sizeof(unsigned long long), st));
+    SIDR_CUDA(cudaMemsetAsync(m->b.error, 0, sizeof(int), st));
     void* args[] = {&m->b};
     SIDR_CUDA(cudaLaunchKernel(multi_kernel(shape), dim3(m->grid[shape]), dim3(m->block[shape]),
                                args, m->smem[shape], st));
@@ -1146,6 +1228,7 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return est[a] > est[b]; });
 
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(device));
     sidr_multi* m = new sidr_multi();
     m->device = device;
@@ -1217,8 +1300,10 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
         (e = put_dev(m, order.data(), order.size() * 4, (const void**)&b.order)) ||
         (e = put_dev(m, nullptr, out_n * 8, (const void**)&b.out)) ||
         (e = put_dev(m, nullptr, 8, (const void**)&b.counter)) ||
-        (e = put_dev(m, nullptr, 8, (const void**)&b.error)))
+        (e = put_dev(m, nullptr, 8, (const void**)&b.error)) ||
+        (e = cudaMemset((void*)b.error, 0, sizeof(int))))
         return bail(e, "batch upload");
+    b.n_inst = K;
     b.P = r->P;
     b.T = T;
     b.group_size = r->P > 0 ? r->P : 1;
@@ -1273,6 +1358,7 @@ sidr_status sidr_multi_set_shape(sidr_multi* m, int32_t shape) {
 sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, float* ms) {
     if (!m) return fail(SIDR_ERR_INVALID, "null batch");
     if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(m->device));
     if ((long long)m->P * m->T == 0) {
         if (chosen) *chosen = m->shape;
@@ -1315,6 +1401,7 @@ sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, fl
 sidr_status sidr_multi_capture(sidr_multi* m) {
     if (!m) return fail(SIDR_ERR_INVALID, "null batch");
     if (m->gexec) return SIDR_OK;
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(m->device));
     if (!m->gstream) SIDR_CUDA(cudaStreamCreateWithFlags(&m->gstream, cudaStreamNonBlocking));
     SIDR_CUDA(cudaStreamBeginCapture(m->gstream, cudaStreamCaptureModeThreadLocal));
@@ -1335,6 +1422,7 @@ sidr_status sidr_multi_capture(sidr_multi* m) {
 sidr_status sidr_multi_run(sidr_multi* m, void* stream) {
     NvtxRange range("sidr_multi_run");
     if (!m) return fail(SIDR_ERR_INVALID, "null batch");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(m->device));
     cudaStream_t st = (cudaStream_t)stream;
     if (m->gexec) {
@@ -1350,10 +1438,11 @@ sidr_status sidr_multi_read(sidr_multi* m, double* out) {
     if (!m) return fail(SIDR_ERR_INVALID, "null batch");
     if ((long long)m->P * m->T == 0) return SIDR_OK;
     if (!out) return fail(SIDR_ERR_INVALID, "output buffer is null");
+    DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(m->device));
     SIDR_CUDA(cudaDeviceSynchronize());
     SIDR_CUDA(cudaMemcpy(out, m->b.out, (size_t)m->P * m->T * 8, cudaMemcpyDeviceToHost));
-    return SIDR_OK;
+    return read_error_word(m->b.error, 0);
 }
 
 void sidr_multi_destroy(sidr_multi* m) { multi_free(m); }

@@ -149,7 +149,14 @@ struct DevBatch {
     const DevInst* insts;
     const int64_t* smp_off;
     const int32_t* order;
+    int n_inst;  // descriptors at insts
 };
+
+// Codes of the kernel error word (DevBatch::error); the host turns a nonzero
+// word into SIDR_ERR_KERNEL.  The first code raised in a launch is kept.
+constexpr int kErrRuleRecord = 1;  // a rule record exceeds the launch's shared-memory slice
+constexpr int kErrRuleIndex = 2;   // a work item names a rule outside the batch
+constexpr int kErrInstance = 3;    // a rule names an instance outside the batch
 
 // Decision-situation capture (capture_kernel only): for scenario s and its
 // d-th decision (d < dec), candidate c (< cand) -> its k terminal rows at

@@ -989,12 +989,12 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         case 3: r = fabs(b) < 1e-10 ? 1.0 : a / b; break;
         case 4: r = a < b ? a : b; break;
         case 5: r = a > b ? a : b; break;
-        default: {
+        default: {  // rmod: glibc's pow restated (libm::pow_), so the result is the CPU's
             const double base = a > 0.0 ? a : 0.0;
             double e = b;
             if (e < 0.0) e = 0.0;
             else if (e > 1.0) e = 1.0;
-            r = pow(base, 1.0 + e);
+            r = libm::pow_(base, 1.0 + e);
         }
         }
         S.rows[od * 32 + lane] = r;
@@ -1170,6 +1170,19 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
     return total;
 }
 
+// Why a rule record cannot run in a warp slice carved for B (0 = it can):
+// program, constants and rows beyond the slice's capacities, a result operand
+// outside them, or (multi-instance batches) an instance outside the batch.
+__device__ __forceinline__ int rule_record_error(const RuleMeta& m, const DevBatch& B, bool multi) {
+    const bool fits = m.n_ins >= 0 && m.n_ins <= B.prog_cap && m.n_const >= 0 &&
+                      m.n_const <= B.const_cap && m.K >= 0 && m.K <= 64 && m.D >= 0 &&
+                      m.K + m.D <= B.rows && m.res >= 0 &&
+                      ((m.res & kOpConst) ? (m.res & 511) < m.n_const : m.res < m.K + m.D);
+    if (!fits) return kErrRuleRecord;
+    if (multi && (m.inst < 0 || m.inst >= B.n_inst)) return kErrInstance;
+    return 0;
+}
+
 // The persistent work loop.  MULTI: every rule carries its instance; the
 // warp stages the instance descriptor with the rule's program.
 template <bool COUNT, bool MULTI, bool CAPTURE = false>
@@ -1194,6 +1207,20 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
         const int s = (int)(item % (unsigned long long)B.T);
         const int p = B.order ? B.order[r] : r;
         if (p != staged) {
+            // Guard of the warp's shared-memory slice: a rule record the launch
+            // was not sized for is refused (error word set, score NaN) before
+            // anything of it is staged.  Host validation makes this unreachable;
+            // the host reads the word back after every launch.
+            const int code = (p < 0 || p >= B.P) ? kErrRuleIndex : rule_record_error(B.meta[p], B, MULTI);
+            if (code) {
+                if (lane == 0) {
+                    atomicCAS(B.error, 0, code);
+                    if (p >= 0 && p < B.P) B.out[(size_t)p * B.T + s] = __longlong_as_double(0x7ff8000000000000LL);
+                }
+                staged = -1;
+                __syncwarp();
+                continue;
+            }
             rm = B.meta[p];
             for (int q = lane; q < rm.n_ins; q += 32) S.prog[q] = B.prog[rm.prog_off + q];
             for (int q = lane; q < rm.n_const; q += 32) S.cst[q] = B.consts[rm.const_off + q];

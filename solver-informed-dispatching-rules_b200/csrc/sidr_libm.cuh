@@ -21,6 +21,13 @@
 //              gen_exp_table.py), exp(r)-1 by a degree-5 polynomial, with the
 //              multiply-adds fused where glibc's FMA build (the one selected
 //              on every x86-64 CPU with FMA) fuses them.
+//   pow        glibc 2.28+'s power function from the same library (rmod,
+//              engine/sim_core.hpp:30-35): x^y = exp(y*log(x)) with log(x) in
+//              double-double from a 128-entry table of 1/c, log(c)
+//              (sidr_pow_table.h, gen_pow_table.py) and a degree-8
+//              polynomial of log1p(z/c - 1), the product y*log(x) split
+//              exactly with a fused multiply-add, and the exponential above
+//              taking the product's low part as a correction.
 //
 // Every other operation is a separately rounded IEEE operation (the device
 // code is compiled with -fmad=false, the host code with -ffp-contract=off).
@@ -32,6 +39,7 @@
 #include <string.h>
 
 #include "sidr_exp_table.h"
+#include "sidr_pow_table.h"
 
 #ifdef __CUDACC__
 #define SIDR_HD __host__ __device__ __forceinline__
@@ -51,6 +59,10 @@ namespace libm {
 __device__ const uint64_t kExpTableDev[256] = {SIDR_EXP_TABLE_ENTRIES};
 #endif
 static const uint64_t kExpTableHost[256] = {SIDR_EXP_TABLE_ENTRIES};
+#ifdef __CUDACC__
+__device__ const double kPowLogDev[384] = {SIDR_POW_LOG_TABLE_ENTRIES};
+#endif
+static const double kPowLogHost[384] = {SIDR_POW_LOG_TABLE_ENTRIES};
 
 SIDR_HD uint64_t bits_of(double x) {
 #ifdef __CUDA_ARCH__
@@ -77,6 +89,14 @@ SIDR_HD uint64_t exp_table(int i) {
     return kExpTableDev[i];
 #else
     return kExpTableHost[i];
+#endif
+}
+
+SIDR_HD double pow_log_table(int i) {
+#ifdef __CUDA_ARCH__
+    return kPowLogDev[i];
+#else
+    return kPowLogHost[i];
 #endif
 }
 
@@ -141,6 +161,159 @@ SIDR_HD double exp_(double x) {
         if (y == 0.0) y = 0.0;
     }
     return 0x1p-1022 * y;
+}
+
+// ------------------------------------------------------------------ pow
+
+// exp(x + xtail) * (sign_bias ? -1 : 1) for the power function: the
+// exponential above with the low part of y*log(x) added to the reduced
+// argument (|xtail| is far below ln2/128) and the result's sign carried in
+// the scale's exponent bits.
+SIDR_HD double exp_tail_(double x, double xtail, uint64_t sign_bias) {
+    const double kInvLn2N = 0x1.71547652b82fep0 * 128.0;
+    const double kNegLn2HiN = -0x1.62e42fefa0000p-8;
+    const double kNegLn2LoN = -0x1.cf79abc9e3b3ap-47;
+    const double kShift = 0x1.8p52;
+    const double kC2 = 0x1.ffffffffffdbdp-2, kC3 = 0x1.555555555543cp-3;
+    const double kC4 = 0x1.55555cf172b91p-5, kC5 = 0x1.1111167a4d017p-7;
+
+    const uint32_t top = (uint32_t)(bits_of(x) >> 52) & 0x7ffu;
+    bool scaled = false;
+    if (top - 0x3c9u >= 0x408u - 0x3c9u) {  // |x| < 2^-54 or |x| >= 512
+        if (top < 0x3c9u) {
+            const double one = 1.0 + x;
+            return sign_bias ? -one : one;
+        }
+        if (top >= 0x409u) {  // |x| >= 1024: overflow or underflow
+            const bool neg = (bits_of(x) >> 63) != 0;
+            const double v = neg ? 0.0 : HUGE_VAL;
+            return sign_bias ? -v : v;
+        }
+        scaled = true;
+    }
+    double kd = fused(kInvLn2N, x, kShift);
+    const uint64_t ki = bits_of(kd);
+    kd -= kShift;
+    double r = fused(kd, kNegLn2LoN, fused(kd, kNegLn2HiN, x));
+    r += xtail;
+    const int idx = (int)(2 * (ki % 128));
+    const double tail = double_of(exp_table(idx));
+    uint64_t sbits = exp_table(idx + 1) + ((ki + sign_bias) << 45);
+    const double r2 = r * r;
+    const double tmp = fused(r2 * r2, fused(r, kC5, kC4), fused(r2, fused(r, kC3, kC2), tail + r));
+    if (!scaled) {
+        const double scale = double_of(sbits);
+        return fused(scale, tmp, scale);
+    }
+    if ((ki & 0x80000000u) == 0) {
+        sbits -= 1009ull << 52;
+        const double scale = double_of(sbits);
+        return 0x1p1009 * fused(scale, tmp, scale);
+    }
+    sbits += 1022ull << 52;
+    const double scale = double_of(sbits);
+    const double st = scale * tmp;
+    double y = scale + st;
+    if (fabs(y) < 1.0) {  // round once at the subnormal precision
+        const double one = y < 0.0 ? -1.0 : 1.0;
+        double lo = scale - y + st;
+        const double hi = one + y;
+        lo = one - hi + y + lo;
+        y = (hi + lo) - one;
+        if (y == 0.0) y = double_of(sbits & 0x8000000000000000ull);
+    }
+    return 0x1p-1022 * y;
+}
+
+// log(x) for the bit pattern ix of a positive normal x (subnormals arrive
+// normalised with a negative exponent), as hi + *tail.  x = 2^k z with z in
+// [0x1.69555p-1, 0x1.69555p0); log(x) = k*ln2 + log(c) + log1p(z/c - 1),
+// with r = z/c - 1 exact (one fused multiply-add) and log1p(r) = r - r^2/2 +
+// r^3*q(r), q of degree 5.
+SIDR_HD double log_tail_(uint64_t ix, double* tail) {
+    const double kLn2Hi = 0x1.62e42fefa3800p-1, kLn2Lo = 0x1.ef35793c76730p-45;
+    // log1p(r) - r = a0 r^2 + a1 r^3 + ... + a6 r^8, scaled for the evaluation below
+    const double a0 = -0x1p-1, a1 = 0x1.555555555556p-2 * -2, a2 = -0x1.0000000000006p-2 * -2,
+                 a3 = 0x1.999999959554ep-3 * 4, a4 = -0x1.555555529a47ap-3 * 4,
+                 a5 = 0x1.2495b9b4845e9p-3 * -8, a6 = -0x1.0002b8b263fc3p-3 * -8;
+    const uint64_t tmp = ix - 0x3fe6955500000000ull;
+    const int i = (int)((tmp >> 45) % 128);
+    const int k = (int)((int64_t)tmp >> 52);
+    const double z = double_of(ix - (tmp & (0xfffull << 52)));
+    const double kd = (double)k;
+    const double invc = pow_log_table(3 * i), logc = pow_log_table(3 * i + 1);
+    const double logctail = pow_log_table(3 * i + 2);
+    const double r = fused(z, invc, -1.0);
+    const double t1 = fused(kd, kLn2Hi, logc);
+    const double t2 = t1 + r;
+    const double lo1 = fused(kd, kLn2Lo, logctail);
+    const double lo2 = t1 - t2 + r;
+    const double ar = a0 * r;
+    const double ar2 = r * ar;
+    const double ar3 = r * ar2;
+    const double hi = t2 + ar2;
+    const double lo3 = fused(ar, r, -ar2);
+    const double lo4 = t2 - hi + ar2;
+    const double q = fused(ar2, fused(ar2, fused(r, a6, a5), fused(r, a4, a3)), fused(r, a2, a1));
+    const double lo = fused(ar3, q, lo1 + lo2 + lo3 + lo4);
+    const double y = hi + lo;
+    *tail = hi - y + lo;
+    return y;
+}
+
+// 0: y not an integer, 1: odd integer, 2: even integer (y finite, nonzero).
+SIDR_HD int integer_kind(uint64_t iy) {
+    const int e = (int)(iy >> 52 & 0x7ff);
+    if (e < 0x3ff) return 0;
+    if (e > 0x3ff + 52) return 2;
+    if (iy & ((1ull << (0x3ff + 52 - e)) - 1)) return 0;
+    if (iy & (1ull << (0x3ff + 52 - e))) return 1;
+    return 2;
+}
+
+// x^y with the results of glibc's pow (round to nearest).
+SIDR_HD_CALL double pow_(double x, double y) {
+    const uint64_t kInf = 0x7ff0000000000000ull, kOne = 0x3ff0000000000000ull;
+    uint64_t ix = bits_of(x), sign_bias = 0;
+    const uint64_t iy = bits_of(y);
+    uint32_t topx = (uint32_t)(ix >> 52);
+    const uint32_t topy = (uint32_t)(iy >> 52);
+    if (topx - 0x001u >= 0x7ffu - 0x001u || (topy & 0x7ffu) - 0x3beu >= 0x43eu - 0x3beu) {
+        if (2 * iy - 1 >= 2 * kInf - 1) {  // y is 0, inf or nan
+            if (2 * iy == 0) return 1.0;
+            if (ix == kOne) return 1.0;
+            if (2 * ix > 2 * kInf || 2 * iy > 2 * kInf) return x + y;
+            if (2 * ix == 2 * kOne) return 1.0;
+            if ((2 * ix < 2 * kOne) == !(iy >> 63)) return 0.0;
+            return y * y;
+        }
+        if (2 * ix - 1 >= 2 * kInf - 1) {  // x is 0, inf or nan
+            double x2 = x * x;
+            if ((ix >> 63) && integer_kind(iy) == 1) x2 = -x2;
+            return (iy >> 63) ? 1.0 / x2 : x2;
+        }
+        if (ix >> 63) {  // finite x < 0
+            const int yk = integer_kind(iy);
+            if (yk == 0) return (x - x) / (x - x);
+            if (yk == 1) sign_bias = 0x800ull << 7;
+            ix &= 0x7fffffffffffffffull;
+            topx &= 0x7ffu;
+        }
+        if ((topy & 0x7ffu) - 0x3beu >= 0x43eu - 0x3beu) {  // |y| tiny or huge
+            if (ix == kOne) return 1.0;
+            if ((topy & 0x7ffu) < 0x3beu) return ix > kOne ? 1.0 + y : 1.0 - y;
+            return (ix > kOne) == (topy < 0x800u) ? HUGE_VAL : 0.0;
+        }
+        if (topx == 0) {  // subnormal x: normalise, exponent becomes negative
+            ix = bits_of(x * 0x1p52) & 0x7fffffffffffffffull;
+            ix -= 52ull << 52;
+        }
+    }
+    double lo;
+    const double hi = log_tail_(ix, &lo);
+    const double ehi = y * hi;
+    const double elo = fused(y, lo, fused(y, hi, -ehi));
+    return exp_tail_(ehi, elo, sign_bias);
 }
 
 // ------------------------------------------------------------- erf, erfc

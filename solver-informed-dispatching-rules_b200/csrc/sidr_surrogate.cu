@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/sidr_surrogate.h"
+#include "sidr_device.hpp"
 #include "sidr_host.hpp"
 #include "sidr_mlp.cuh"
 
@@ -406,6 +407,7 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
                            int32_t splits, int device, float* C) {
     if (!A || !B || !C || M < 1 || N < 1 || K < 1 || N > 256)
         return fail_s(SIDR_ERR_INVALID, "gemm: bad argument (1 <= N <= 256)");
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(device));
     __nv_bfloat16 *dA = nullptr, *dB = nullptr;
     float* dC = nullptr;
@@ -445,6 +447,7 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
 sidr_status sidr_gemm_wait_check(int device, uint32_t wait_limit) {
     if (wait_limit < 1 || wait_limit > (1u << 20))
         return fail_s(SIDR_ERR_INVALID, "wait check: wait_limit out of 1..2^20");
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(device));
     constexpr int M = 128, N = 48, K = 32;
     __nv_bfloat16 *dA = nullptr, *dB = nullptr;
@@ -543,6 +546,7 @@ sidr_status sidr_phenotype(const sidr_rules_desc* r, const double* terms, const 
         f[7] = (float)other / ops_n;
     }
     if (P == 0) return SIDR_OK;
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(device));
     const size_t nodes = (size_t)r->n_nodes;
     int32_t *d_ops = nullptr, *d_args = nullptr, *d_off = nullptr, *d_len = nullptr, *d_nc = nullptr,
@@ -589,6 +593,7 @@ sidr_status sidr_phenotype(const sidr_rules_desc* r, const double* terms, const 
 sidr_status sidr_mlp_create(int device, uint64_t seed, sidr_mlp** out) {
     if (!out) return fail_s(SIDR_ERR_INVALID, "out is null");
     *out = nullptr;
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(device));
     sidr_mlp* m = new sidr_mlp();
     m->device = device;
@@ -641,6 +646,7 @@ sidr_status sidr_mlp_param(sidr_mlp* m, int32_t which, int32_t write, float* val
     Param* p = param_by_index(m, which);
     if (!p) return fail_s(SIDR_ERR_INVALID, "parameter index 0..5");
     if (count) *count = p->n;
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(m->device));
     SIDR_SCHECK(cudaStreamSynchronize(m->st));
     if (values) {
@@ -659,6 +665,7 @@ sidr_status sidr_mlp_param(sidr_mlp* m, int32_t which, int32_t write, float* val
 sidr_status sidr_mlp_predict(sidr_mlp* m, const float* x, int32_t rows, float* y) {
     if (!m || (rows > 0 && (!x || !y)) || rows < 0) return fail_s(SIDR_ERR_INVALID, "bad argument");
     if (rows == 0) return SIDR_OK;
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(m->device));
     sidr_status s = ensure_rows(m, rows);
     if (s) return s;
@@ -670,6 +677,7 @@ sidr_status sidr_mlp_predict(sidr_mlp* m, const float* x, int32_t rows, float* y
 
 sidr_status sidr_mlp_gradients(sidr_mlp* m, const float* x, const float* t, int32_t rows, float* loss) {
     if (!m || !x || !t || rows < 1) return fail_s(SIDR_ERR_INVALID, "bad argument");
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(m->device));
     sidr_status s = ensure_rows(m, rows);
     if (s) return s;
@@ -684,6 +692,7 @@ sidr_status sidr_mlp_train(sidr_mlp* m, const float* x, const float* t, int32_t 
                            int32_t batch, float lr, uint64_t seed, float* final_loss) {
     if (!m || !x || !t || n < 1 || steps < 0 || batch < 1)
         return fail_s(SIDR_ERR_INVALID, "bad argument");
+    DeviceGuard device_guard;
     SIDR_SCHECK(cudaSetDevice(m->device));
     const int rows = std::min(batch, n);
     sidr_status s = ensure_rows(m, rows);

@@ -66,7 +66,7 @@ EXPORTS = [
     "sidr_kernel_launches", "sidr_rules_check", "sidr_last_transfer_bytes", "sidr_fp64_peak",
     "sidr_evaluate_static", "sidr_multi_create", "sidr_multi_autotune", "sidr_multi_set_shape",
     "sidr_multi_capture", "sidr_multi_run", "sidr_multi_read", "sidr_multi_destroy",
-    "sidr_libm_eval",
+    "sidr_libm_eval", "sidr_batch_guard_check", "sidr_libm_pow",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -102,6 +102,8 @@ def load() -> C.CDLL:
     L.sidr_batch_destroy.argtypes = [C.c_void_p]
     L.sidr_batch_set_counting.argtypes = [C.c_void_p, C.c_int]
     L.sidr_batch_counts.argtypes = [C.c_void_p, C.POINTER(_Counts)]
+    L.sidr_batch_guard_check.argtypes = [C.c_void_p]
+    L.sidr_libm_pow.argtypes = [_dp, _dp, C.c_int64, C.c_int, _dp]
     L.sidr_kernel_launches.restype = C.c_int64
     L.sidr_rules_check.argtypes = [C.POINTER(_Rules), _lp, C.c_int32, C.POINTER(C.c_int32)]
     L.sidr_last_transfer_bytes.argtypes = [_lp, _lp]
@@ -207,6 +209,17 @@ def libm_eval(fn: str, x, device: int = 0) -> np.ndarray:
     return out
 
 
+def libm_pow(x, y, device: int = 0) -> np.ndarray:
+    """The evaluator's device pow (glibc's, restated) on host arrays."""
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    b = np.ascontiguousarray(y, dtype=np.float64)
+    if a.shape != b.shape:
+        raise ValueError("x and y differ in shape")
+    out = np.zeros_like(a)
+    _check(load().sidr_libm_pow(_d(a), _d(b), a.size, device, _d(out)))
+    return out
+
+
 STATIC_SCRATCH_BYTES = 16 << 20  # SIDR_STATIC_SCRATCH_BYTES
 STATIC_MAX_N = 128               # SIDR_STATIC_MAX_N
 
@@ -250,6 +263,11 @@ class Batch:
 
     def set_counting(self, on: bool) -> None:
         _check(load().sidr_batch_set_counting(self.h, int(on)))
+
+    def guard_check(self) -> int:
+        """sidr_batch_guard_check: the kernel's rule-record guard, tripped on
+        purpose; returns the status (SIDR_ERR_KERNEL expected)."""
+        return int(load().sidr_batch_guard_check(self.h))
 
     def counts(self) -> dict:
         c = _Counts()

@@ -1,7 +1,8 @@
-// Compares sidr::libm::{erf_, erfc_, exp_} (csrc/sidr_libm.cuh) with the host
-// C library bit for bit over random arguments in every interval of the
+// Compares sidr::libm::{erf_, erfc_, exp_, pow_} (csrc/sidr_libm.cuh) with the
+// host C library bit for bit over random arguments in every interval of the
 // algorithms.  Usage: libm_check <samples per interval> <seed>; prints one line
 // per interval "name lo hi mismatches samples" and exits 1 on any mismatch.
+// For pow the interval is a family of (x, y) pairs, named by its number.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -74,6 +75,54 @@ int main(int argc, char** argv) {
         for (double x : special)
             if (bits(ours(r.fn, x)) != bits(theirs(r.fn, x))) bad++;
         std::printf("%s %a %a %ld %ld\n", r.fn, r.lo, r.hi, bad, n);
+        bad_total += bad != 0;
+    }
+    // pow: families of (x, y); the first ones cover rmod's arguments
+    // (x >= 0, y = 1 + clip(b, 0, 1))
+    auto pow_pair = [](int fam, double& x, double& y) {
+        switch (fam) {
+        case 0: x = std::exp2(uniform(-30.0, 30.0)); y = uniform(1.0, 2.0); break;
+        case 1: x = uniform(0.5, 2.0); y = uniform(1.0, 2.0); break;
+        case 2: x = std::exp2(uniform(-1074.0, 1023.9)); y = uniform(1.0, 2.0); break;
+        case 3: x = (double)(1 + next_u64() % 1000000) / (double)(1 + next_u64() % 1000);
+                y = 1.0 + (double)(next_u64() % 1001) / 1000.0; break;
+        case 4: x = std::exp2(uniform(-1022.0, 1023.9)); y = uniform(-8.0, 8.0); break;
+        case 5: { uint64_t u = next_u64() & 0x000fffffffffffffull; std::memcpy(&x, &u, 8); }
+                y = uniform(0.5, 2.0); break;
+        default: x = -std::exp2(uniform(-10.0, 10.0));
+                 y = (double)(long)uniform(-10.0, 10.0) + ((next_u64() & 1) ? 0.5 : 0.0); break;
+        }
+    };
+    for (int fam = 0; fam < 7; fam++) {
+        long bad = 0;
+        for (long k = 0; k < n; k++) {
+            double x, y;
+            pow_pair(fam, x, y);
+            const double a = sidr::libm::pow_(x, y), b = std::pow(x, y);
+            if (bits(a) != bits(b) && !(a != a && b != b)) {
+                if (bad < 2) std::printf("# pow(%a, %a): ours %a libc %a\n", x, y, a, b);
+                bad++;
+            }
+        }
+        std::printf("pow family%d - %ld %ld\n", fam, bad, n);
+        bad_total += bad != 0;
+    }
+    {  // special operands
+        const double xs[] = {0.0, -0.0, 1.0, -1.0, 2.0, 0.5, 0x1p-1074, 0x1p-1022, 1e308, INFINITY,
+                             -INFINITY, NAN, -2.0, 3.5};
+        const double ys[] = {0.0, -0.0, 1.0, 2.0, 1.5, -1.0, 0.5, 3.0, 1e-300, 1e300, INFINITY,
+                             -INFINITY, NAN, 1075.0, -1075.0};
+        long bad = 0, cnt = 0;
+        for (double x : xs)
+            for (double y : ys) {
+                const double a = sidr::libm::pow_(x, y), b = std::pow(x, y);
+                cnt++;
+                if (bits(a) != bits(b) && !(a != a && b != b)) {
+                    std::printf("# pow(%a, %a): ours %a libc %a\n", x, y, a, b);
+                    bad++;
+                }
+            }
+        std::printf("pow specials - %ld %ld\n", bad, cnt);
         bad_total += bad != 0;
     }
     return bad_total ? 1 : 0;

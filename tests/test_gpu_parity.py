@@ -262,3 +262,44 @@ def test_invalid_inputs_fail_without_launch():
         ctx.evaluate(r, w.sampled, w.S, w.mask)
     assert sidr.kernel_launches() == before
     ctx.close()
+
+
+def test_kernel_guard_raises_error_word(oracle):
+    """The kernel's rule-record guard, tripped on purpose by launching a batch
+    with slices too small for its rules (sidr_batch_guard_check): the launch
+    refuses every rule, raises the error word, and the host reports
+    SIDR_ERR_KERNEL; reading that launch's scores reports it too; the next
+    ordinary launch clears the word and gives the oracle's scores."""
+    w = workload.plain_eval(P=12, S=3)
+    zp = sidr.zstats(w.sd)
+    ctx = sidr.Context(w.sd, zp)
+    b = ctx.batch(w.rules, w.sampled, w.S, w.mask)
+    for _ in range(2):
+        assert b.guard_check() == 6  # SIDR_ERR_KERNEL
+        with pytest.raises(sidr.SidrError) as e:
+            b.read()
+        assert e.value.status == 6 and "shared-memory slice" in str(e.value)
+    b.run()
+    assert_bitexact(b.read(), oracle.eval_pairs(w.sd, zp, w.rules, w.sampled, w.S, w.mask), "after")
+    b.close()
+    ctx.close()
+
+
+def test_rmod_heavy_rules_match_oracle(oracle):
+    """rmod (opcode 6, pow(max(a, 0), 1 + clip(b, 0, 1)), engine/sim_core.hpp:
+    30-35) runs on glibc's pow restated for the device, so rules built from it
+    give the CPU simulator's scores by construction: 256 rules of depth 2-6
+    over the 29-terminal menu with ERC constants and rmod among the
+    functions, every one of which applies rmod, on 40 scenarios of the
+    GP-generation instance."""
+    w = workload.gp_generation(P=1, S=40)
+    pool = R.ramped_half_and_half(workload.MENU29 + ["ERC"], R.FUNCS_RMOD, 2, 6, 77, 1200)
+    trees = [t for t in pool if "rmod" in R.to_prefix(t)][:256]
+    assert len(trees) == 256
+    rules = R.pack(trees)
+    mask = R.term_mask_from(workload.MENU29 + ["ERC"])
+    zp = sidr.zstats(w.sd)
+    ctx = sidr.Context(w.sd, zp)
+    out = ctx.evaluate(rules, w.sampled, w.S, mask)
+    ctx.close()
+    assert_bitexact(out, oracle.eval_pairs(w.sd, zp, rules, w.sampled, w.S, mask), "rmod rules")

@@ -1,5 +1,5 @@
-"""The evaluator's erf, erfc and exp (csrc/sidr_libm.cuh) against the host C
-library, bit for bit: the host build of the same header over random
+"""The evaluator's erf, erfc, exp and pow (csrc/sidr_libm.cuh) against the host
+C library, bit for bit: the host build of the same header over random
 arguments in every interval of the algorithms (CPU), and the device build
 over the same kind of arguments (GPU)."""
 import ctypes
@@ -23,7 +23,7 @@ def test_host_build_matches_libc(tmp_path):
                    check=True)
     r = subprocess.run([str(exe), "200000", "3"], capture_output=True, text=True)
     rows = [ln.split() for ln in r.stdout.splitlines() if not ln.startswith("#")]
-    assert len(rows) == 27
+    assert len(rows) == 27 + 8  # 27 erf/erfc/exp intervals, 7 pow families, pow specials
     bad = [row for row in rows if row[3] != "0"]
     assert not bad and r.returncode == 0, r.stdout
 
@@ -55,3 +55,35 @@ def test_device_matches_libc(fn):
     bad = np.nonzero(got.view(np.uint64) != exp.view(np.uint64))[0]
     assert bad.size == 0, [(float(xs[i]).hex(), float(got[i]).hex(), float(exp[i]).hex())
                            for i in bad[:5]]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_device_pow_matches_libc():
+    """rmod's pow on the device: x >= 0, y in [1, 2] over many magnitudes,
+    rule-like ratios, the whole double range, other exponents, subnormal and
+    negative bases, and the special operands."""
+    rng = np.random.default_rng(12)
+    n = 200000
+    xs = [np.exp2(rng.uniform(-30, 30, n)), rng.uniform(0.5, 2.0, n),
+          np.exp2(rng.uniform(-1074, 1023.9, n)),
+          rng.integers(1, 1000001, n) / rng.integers(1, 1001, n),
+          np.exp2(rng.uniform(-1022, 1023.9, n)),
+          (rng.integers(0, 1 << 52, n, dtype=np.uint64)).view(np.float64),
+          -np.exp2(rng.uniform(-10, 10, n))]
+    ys = [rng.uniform(1, 2, n), rng.uniform(1, 2, n), rng.uniform(1, 2, n),
+          1.0 + rng.integers(0, 1001, n) / 1000.0, rng.uniform(-8, 8, n), rng.uniform(0.5, 2, n),
+          np.trunc(rng.uniform(-10, 10, n)) + 0.5 * rng.integers(0, 2, n)]
+    sx = np.array([0.0, -0.0, 1.0, -1.0, 2.0, 0.5, 5e-324, 1e308, np.inf, -np.inf, np.nan, -2.0])
+    sy = np.array([0.0, 1.0, 2.0, 1.5, -1.0, 0.5, 3.0, np.inf, -np.inf, np.nan, 1075.0])
+    gx, gy = np.meshgrid(sx, sy)
+    x = np.concatenate(xs + [gx.ravel()])
+    y = np.concatenate(ys + [gy.ravel()])
+    got = sidr.libm_pow(x, y)
+    LIBC.pow.restype = ctypes.c_double
+    LIBC.pow.argtypes = [ctypes.c_double, ctypes.c_double]
+    exp = np.array([LIBC.pow(float(a), float(b)) for a, b in zip(x, y)])
+    same = (got.view(np.uint64) == exp.view(np.uint64)) | (np.isnan(got) & np.isnan(exp))
+    bad = np.nonzero(~same)[0]
+    assert bad.size == 0, [(float(x[i]).hex(), float(y[i]).hex(), float(got[i]).hex(),
+                            float(exp[i]).hex()) for i in bad[:5]]

@@ -36,7 +36,7 @@ def _case(builder, P, S, G):
     return w, zp, grouped, masks
 
 
-def test_static_entry_matches_context_entry_twice():
+def test_static_entry_matches_context_entry_twice(oracle):
     for builder, P, S, G in ((workload.plain_eval, 48, 6, 2), (workload.gp_generation, 40, 5, 2)):
         w, zp, grouped, masks = _case(builder, P, S, G)
         gs = (P + G - 1) // G
@@ -46,9 +46,29 @@ def test_static_entry_matches_context_entry_twice():
         want = ctx.evaluate_grouped_masks(w.rules, grouped, G, S, gs, mg, masks)
         ctx.close()
         assert np.array_equal(bits(got), bits(want)), builder.__name__
+        cpu = oracle.eval_pairs(w.sd, zp, w.rules, grouped, S, masks, group_size=gs, mask_group=mg)
+        assert np.array_equal(bits(got), bits(cpu)), builder.__name__
         # the array keeps the previous call's contents; a repeat must not see them
         again = sidr.evaluate_static(w.sd, zp, w.rules, grouped, G, S, gs, mg, masks)
         assert np.array_equal(bits(again), bits(want)), builder.__name__
+
+
+def test_static_entry_allocates_nothing():
+    """After a first call (which looks up the array's device address and
+    creates the library's stream on this device), calls of different sizes
+    leave the device's free memory exactly where it was."""
+    import torch
+    cases = [_case(workload.plain_eval, P, S, 2) + (P, S) for P, S in ((16, 4), (48, 6), (8, 2))]
+    w, zp, grouped, masks, P, S = cases[0]
+    sidr.evaluate_static(w.sd, zp, w.rules, grouped, 2, S, (P + 1) // 2, P, masks)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(2):
+        for w, zp, grouped, masks, P, S in cases:
+            sidr.evaluate_static(w.sd, zp, w.rules, grouped, 2, S, (P + 1) // 2, P, masks)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
 
 
 def test_static_entry_rejects_oversized_calls():

@@ -18,10 +18,17 @@ e2e        : the same metric through the reference-shaped host call
 roofline   : the evaluator is bound by the FP64 pipe / issue rate, not HBM or
              tensor cores; achieved = op-model FP64 operations per launch
              (counted by the kernel's counting instantiation) / kernel time,
-             peak = the FP64 pipe throughput measured on this GPU.
+             peak = the FP64 pipe throughput measured on this GPU; traffic =
+             the launch's DRAM bytes from bench_traffic.json (an ncu capture of
+             this command), used only while the kernel sources hash to the
+             value recorded there.
+evolved    : the same measurements on generation 49 of the benchmark GP run
+             (same instance and scenarios): the populations a GP spends most of
+             its generations on, several times costlier per evaluation.
 cpu_baseline: the reference's CPU simulator (compiled from its own headers,
              oracle/_ref) or else the C oracle, on all host threads, on a
-             bounded sample of the same workload.
+             bounded sample of the same workload (--full-parity: all of it),
+             compared bit for bit with the GPU's scores.
 
 Multi-GPU: pairs are independent, so each rank evaluates its own generation
 (weak scaling, no collective on the data path); the timing is the maximum over
@@ -58,6 +65,13 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--evolved-steps", type=int, default=3,
+                    help="timed steps of the evolved-population leg (generation 49 of the "
+                         "benchmark GP run on the same instance and scenarios); 0 skips it")
+    ap.add_argument("--full-parity", action="store_true",
+                    help="compare every (rule, scenario) pair of the workload with the CPU "
+                         "simulator on all host threads, instead of a bounded sample: about "
+                         "five minutes per 512,000 pairs on 16 threads")
     ap.add_argument("--gp", action="store_true",
                     help="also run the GP loop of the workload (50 generations of 1024 rules x "
                          "500 scenarios + held-out evaluation) and report its wall time")
@@ -179,15 +193,19 @@ def cpu_checker():
     return O.Oracle(), "port"
 
 
-def cpu_baseline(w, zp, seconds, gpu_out=None):
+def cpu_baseline(w, zp, seconds, gpu_out=None, full=False):
     """The CPU simulator on all host threads over a bounded, strided sample of
-    the workload; returns the baseline record (and the parity of the sample
-    against the GPU's scores when given)."""
+    the workload (full: every rule and scenario); returns the baseline record
+    and, when the GPU's scores are given, their parity with the CPU's."""
     import numpy as np
     chk, kind = cpu_checker()
     threads = os.cpu_count() or 1
-    idx, chunks = cpu_sample(w.rules.P, w.S)
-    sub = w.rules.subset(idx)
+    if full:
+        idx, chunks = list(range(w.rules.P)), [(0, w.S)]
+        sub = w.rules
+    else:
+        idx, chunks = cpu_sample(w.rules.P, w.S)
+        sub = w.rules.subset(idx)
     evals, t_used, cmp, bad = 0, 0.0, 0, 0
     for s0, s1 in chunks:
         t0 = time.perf_counter()
@@ -198,11 +216,13 @@ def cpu_baseline(w, zp, seconds, gpu_out=None):
             g = gpu_out[idx][:, s0:s1]
             cmp += g.size
             bad += int(np.count_nonzero(g.view(np.uint64) != out.view(np.uint64)))
-        if t_used >= seconds:
+        if not full and t_used >= seconds:
             break
-    rec = {"value": evals / t_used, "unit": UNIT, "cores": threads, "kind": kind,
-           "sample": f"every 16th rule ({len(idx)} rules) x first {evals // len(idx)} scenarios "
-                     f"= {evals} evaluations in {t_used:.1f} s"}
+    sample = (f"all {len(idx)} rules x {w.S} scenarios = {evals} evaluations in {t_used:.1f} s"
+              if full else
+              f"every 16th rule ({len(idx)} rules) x first {evals // len(idx)} scenarios "
+              f"= {evals} evaluations in {t_used:.1f} s")
+    rec = {"value": evals / t_used, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample}
     if gpu_out is not None:
         rec["parity"] = {"pairs": cmp, "mismatches": bad}
     return rec
@@ -250,19 +270,34 @@ def run_reference(args, rank, world):
 
 # ------------------------------------------------------------------ ours
 
-def profile_traffic():
-    """Per-launch DRAM bytes (read + write) of the evaluator kernel on this
-    workload, from the committed ncu summary
-    profiles/eval_kernel_gp_generation_traffic.md (its "bytes_per_launch:"
-    line); None when absent."""
-    p = os.path.join(REPO, "profiles", "eval_kernel_gp_generation_traffic.md")
-    if not os.path.exists(p):
-        return None
-    with open(p) as f:
-        for line in f:
-            if line.startswith("bytes_per_launch:"):
-                return float(line.split(":", 1)[1])
-    return None
+def kernel_sources_sha():
+    """sha256 over the evaluator kernel's sources: the key under which a DRAM
+    traffic figure measured by ncu is valid."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in ("sidr_kernel.cuh", "sidr_internal.hpp", "sidr_libm.cuh", "sidr_capi.cu"):
+        with open(os.path.join(PKG, "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def recorded_traffic(workload_name):
+    """Per-launch DRAM bytes (read + write) of eval_kernel on this workload,
+    from bench_traffic.json beside this script (written from an ncu capture
+    of the same command); None when the record is absent or was measured on
+    other kernel sources than the ones built here."""
+    p = os.path.join(REPO, "bench_traffic.json")
+    try:
+        with open(p) as f:
+            rec = json.load(f)
+    except Exception:
+        return None, "no record"
+    ent = rec.get(workload_name)
+    if not ent:
+        return None, "no record for this workload"
+    if ent.get("kernel_sources_sha256") != kernel_sources_sha():
+        return None, "record measured on other kernel sources"
+    return float(ent["bytes_per_launch"]), ent.get("command", "")
 
 
 def measured_hbm_gbs():
@@ -275,8 +310,85 @@ def measured_hbm_gbs():
         return 6650.0, "fallback"
 
 
-def run_ours(args, rank, world, local):
+def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, world, e2e_on=True,
+            clocks=None):
+    """Device time of `steps` evaluations of workload w (resident batch, L2
+    flushed between steps), the end-to-end rate through sidr_evaluate with host
+    buffers, and the FP64 op-model roofline of the evaluator launch."""
     import numpy as np
+    import torch
+    import sidr
+    batch = ctx.batch(w.rules, w.sampled, w.S, w.mask)
+    sh = stream.cuda_stream
+    batch.set_counting(True)  # op-model counts: separate, untimed launch
+    batch.run(sh)
+    torch.cuda.synchronize()
+    counts = batch.counts()
+    batch.set_counting(False)
+    for _ in range(warmup):
+        flush.zero_()
+        batch.run(sh)
+    torch.cuda.synchronize()
+    ref_out = batch.read()
+    barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    launches0 = sidr.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        batch.run(sh)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = sidr.kernel_launches() - launches0
+    clk = clocks.stop() if clocks else None
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total_ms = allmax(sum(step_ms))
+    evals = w.rules.P * w.S
+    value = world * evals * steps / (total_ms / 1e3)
+    same = bool(np.array_equal(batch.read().view(np.uint64), ref_out.view(np.uint64)))
+    batch.close()
+    e2e = None
+    if e2e_on:
+        ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
+        barrier()
+        t_e2e = 0.0
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
+            t_e2e += time.perf_counter() - t0
+        t_e2e = allmax(t_e2e)
+        h2d, d2h = sidr.last_transfer_bytes()
+        same = same and bool(np.array_equal(out.view(np.uint64), ref_out.view(np.uint64)))
+        e2e = {"value": world * evals * steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": 1e3 * t_e2e / steps}
+    avg_s = (sum(step_ms) / len(step_ms)) / 1e3
+    achieved = counts["fp64_ops"] / avg_s
+    traffic, traffic_src = recorded_traffic(w.name)
+    roofline = {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_ops / 1e12,
+                "unit": "Tops/s (FP64 pipe, op model)", "frac": achieved / peak_ops,
+                "traffic": traffic, "traffic_source": traffic_src,
+                "peak_source": "measured on this GPU by sidr_fp64_peak (DFMA chains over all SMs)",
+                "op_model": "sidr_counts.fp64_ops (include/sidr.h)"}
+    hbm = None
+    if traffic is not None:
+        hbm_peak, hbm_src = measured_hbm_gbs()
+        hbm = {"achieved": traffic / avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+               "frac": traffic / avg_s / 1e9 / hbm_peak, "peak_source": hbm_src,
+               "traffic_bytes_per_launch": traffic}
+    return {"value": value, "total_ms": total_ms, "e2e": e2e, "launches": launches,
+            "roofline": roofline, "hbm": hbm, "clocks": clk, "counts": counts,
+            "repeat_runs_identical": same, "out": ref_out}
+
+
+def run_ours(args, rank, world, local):
     import torch
     import sidr
 
@@ -303,92 +415,41 @@ def run_ours(args, rank, world, local):
     w = workload_for(rank, args.P, args.S)
     zp = sidr.zstats(w.sd)
     ctx = sidr.Context(w.sd, zp, device=local)
-    batch = ctx.batch(w.rules, w.sampled, w.S, w.mask)
     stream = torch.cuda.Stream()  # the launching stream: events are recorded on it
     torch.cuda.set_stream(stream)
-    sh = stream.cuda_stream
-
-    # op-model counts (separate, untimed launch of the counting instantiation)
-    batch.set_counting(True)
-    batch.run(sh)
-    torch.cuda.synchronize()
-    counts = batch.counts()
-    batch.set_counting(False)
-
     peak_ops = sidr.fp64_peak(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    for _ in range(args.warmup):
-        flush.zero_()
-        batch.run(sh)
-    torch.cuda.synchronize()
-    ref_out = batch.read()
-
-    clocks = ClockSampler(gpu_uuid(local))
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    time.sleep(0.3)
-    launches0 = sidr.kernel_launches()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    for e0, e1 in ev:
-        flush.zero_()
-        e0.record(stream)
-        batch.run(sh)
-        e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    launches = sidr.kernel_launches() - launches0
-    clk = clocks.stop()
-    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
-    total_ms = allmax(sum(step_ms))
-    evals_per_rank = w.rules.P * w.S
-    value = world * evals_per_rank * args.steps / (total_ms / 1e3)
-    same = bool(np.array_equal(batch.read().view(np.uint64), ref_out.view(np.uint64)))
-
-    # end to end through the reference-shaped host call
-    e2e = None
-    if not args.no_e2e:
-        ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
-        barrier()
-        t_e2e = 0.0
-        for _ in range(args.steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            out = ctx.evaluate(w.rules, w.sampled, w.S, w.mask)
-            t_e2e += time.perf_counter() - t0
-        t_e2e = allmax(t_e2e)
-        h2d, d2h = sidr.last_transfer_bytes()
-        same = same and bool(np.array_equal(out.view(np.uint64), ref_out.view(np.uint64)))
-        e2e = {"value": world * evals_per_rank * args.steps / t_e2e, "unit": UNIT,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": 1e3 * t_e2e / args.steps}
-
-    avg_s = (sum(step_ms) / len(step_ms)) / 1e3
-    achieved = counts["fp64_ops"] / avg_s
-    traffic = profile_traffic()
-    roofline = {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_ops / 1e12,
-                "unit": "Tops/s (FP64 pipe, op model)", "frac": achieved / peak_ops,
-                "traffic": traffic,
-                "peak_source": "measured on this GPU by sidr_fp64_peak (DFMA chains over all SMs)",
-                "op_model": "sidr_counts.fp64_ops (include/sidr.h)"}
-
-    hbm_peak, hbm_src = measured_hbm_gbs()
-    hbm = None
-    if traffic is not None:
-        hbm = {"achieved": traffic / avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
-               "frac": traffic / avg_s / 1e9 / hbm_peak, "peak_source": hbm_src,
-               "traffic_bytes_per_launch": traffic}
-
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+    r = measure(ctx, w, args.steps, args.warmup, stream, flush, peak_ops, allmax, barrier, world,
+                e2e_on=not args.no_e2e, clocks=ClockSampler(gpu_uuid(local)))
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_of(args.P, args.S, world),
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "hbm": hbm, "clocks": clk,
-            "counts": counts, "repeat_runs_identical": same}
+            "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"],
+            "hbm": r["hbm"], "clocks": r["clocks"], "counts": r["counts"],
+            "repeat_runs_identical": r["repeat_runs_identical"]}
+    if args.evolved_steps > 0:
+        # the same instance and scenarios with generation 49 of the benchmark GP run: the
+        # populations a GP spends 49 of its 50 generations on
+        from sidr import workload as W
+        we = W.evolved(49, P=args.P, S=args.S)
+        re = measure(ctx, we, args.evolved_steps, 3, stream, flush, peak_ops, allmax, barrier,
+                     world, e2e_on=not args.no_e2e)
+        line["evolved"] = {"workload": f"evolved_gen49: generation 49 of the benchmark GP run "
+                                       f"(seed 0), {args.P} rules x {args.S} scenarios, same "
+                                       f"instance and scenarios", "value": re["value"],
+                           "unit": UNIT, "steps": args.evolved_steps, "warmup": 3,
+                           "ms_per_step": re["total_ms"] / args.evolved_steps, "e2e": re["e2e"],
+                           "roofline": re["roofline"], "counts": re["counts"],
+                           "repeat_runs_identical": re["repeat_runs_identical"]}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            # a bounded sample: the evolved rules cost the CPU simulator about 3x more per pair
+            line["evolved"]["cpu_baseline"] = cpu_baseline(we, zp, args.cpu_seconds / 2,
+                                                           gpu_out=re["out"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, zp, args.cpu_seconds, gpu_out=ref_out)
+        line["cpu_baseline"] = cpu_baseline(w, zp, args.cpu_seconds, gpu_out=r["out"],
+                                            full=args.full_parity)
     if args.gp and rank == 0:
         line["gp"] = gp_leg(ctx, w, args)
     if args.multi and rank == 0:
@@ -397,7 +458,6 @@ def run_ours(args, rank, world, local):
         line["sgp"] = sgp_leg(ctx, w, args)
     if args.campaign and rank == 0:
         line["campaign"] = campaign_leg()
-    batch.close()
     ctx.close()
     if dist:
         dist.destroy_process_group()

@@ -21,9 +21,13 @@ evaluation sizes the benchmark names, with the reference's own rule generator
                     uniform), m=4, H=1000, each with the initial populations of
                     30 GP seeds x 4096 rules and 2000 scenarios, for the
                     multi-instance launch (tests use reduced counts).
+  evolved           gp_generation's instance and scenarios with the population
+                    of generation 25 or 49 of the benchmark GP run
+                    (data/evolved_gp_generation.npz).
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -144,6 +148,25 @@ def large_combined(K: int = 10, seeds: int = 30, rules_per_seed: int = 4096, S: 
         sampled.append(gen_durations(sd.durations, sd.sigma, S, 1 + 1000 * k))
         masks.append(term_mask_from(MENU29))
     return MultiWorkload("large_combined", sds, rules, sampled, masks, S)
+
+
+EVOLVED_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                            "evolved_gp_generation.npz")
+
+
+def evolved(generation: int = 49, P: int = 1024, S: int = 500) -> Workload:
+    """gp_generation's instance and scenarios with an evolved population: the
+    population of the benchmark GP run (seed 0, 1024 rules, 500 training
+    scenarios per generation) at `generation` (25 or 49), saved by
+    data/make_evolved.py; the first P rules."""
+    z = np.load(EVOLVED_FILE)
+    key = f"gen{generation}"
+    if key not in z.files:
+        raise KeyError(f"{EVOLVED_FILE} holds {sorted(f for f in z.files if f.startswith('gen'))}")
+    trees = str(z[key]).split("\n")[:P]
+    base = gp_generation(P=1, S=S)
+    return Workload(f"evolved_gen{generation}", base.sd, pack(trees), base.sampled, base.mask,
+                    base.instance_text, trees)
 
 
 WORKLOADS = {"plain_eval": plain_eval, "gp_generation": gp_generation}

@@ -13,7 +13,10 @@
 //     using FactoryContext = sidr::FactoryContextT<SimData, PackedTrees>;
 //
 // and links libsidr_b200.so; gp_engine.cu, timing.cu, ga.cu, gen_trace.cu,
-// choice.cu, redeploy.cu and verify_cuda.cu then compile unchanged.
+// choice.cu, redeploy.cu and verify_cuda.cu then compile unchanged (and, with
+// no kernel left in the header, as plain C++).  tests/test_dropin.py builds the
+// reference's own verify_cuda.cu and gp_engine.cu this way and runs
+// verify_cuda's gate through the library.
 //
 // Method names, argument order and meaning, the `threads` argument (accepted
 // and ignored: the launch geometry is the library's) and the output layout

@@ -9,8 +9,10 @@
 // at a time; one elected thread issues the MMAs and commits them to an
 // mbarrier that the CTA waits on (bounded).  The epilogue reads the
 // accumulator back with tcgen05.ld (32 lanes x 32 bits per warp) and applies
-// one of: plain store, bias + ReLU with a BF16 copy, or atomic accumulation
-// (split-K over blockIdx.z for the weight gradients).
+// one of: plain store, bias + ReLU with a BF16 copy, or a store into the
+// partial-sum slice of its K range (split-K over blockIdx.z for the weight
+// gradients; the slices are then added in slice order by split_sum_kernel, so
+// the result does not depend on the order in which CTAs finish).
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -22,7 +24,7 @@ namespace mlp {
 enum Epilogue : int {
     kStoreF32 = 0,    // C[m*ldc + n] = acc
     kBiasRelu = 1,    // z = acc + bias[n]; Hb[m*ldh + n] = bf16(max(z, 0))
-    kAtomicF32 = 2,   // atomicAdd(C[m*ldc + n], acc)
+    kSplitF32 = 2,    // C[z*split_stride + m*ldc + n] = acc, z = blockIdx.z
 };
 
 struct GemmArgs {
@@ -35,6 +37,7 @@ struct GemmArgs {
     int epilogue;
     float* C;
     int ldc;
+    long long split_stride;  // floats between the partial-sum slices (kSplitF32)
     const float* bias;
     __nv_bfloat16* Hb;
     int ldh;
@@ -192,8 +195,8 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
                     const float acc = __uint_as_float(v[j]);
                     if (g.epilogue == kStoreF32) {
                         g.C[(long long)m * g.ldc + n] = acc;
-                    } else if (g.epilogue == kAtomicF32) {
-                        atomicAdd(&g.C[(long long)m * g.ldc + n], acc);
+                    } else if (g.epilogue == kSplitF32) {
+                        g.C[(long long)blockIdx.z * g.split_stride + (long long)m * g.ldc + n] = acc;
                     } else {
                         const float z = acc + g.bias[n];
                         g.Hb[(long long)m * g.ldh + n] = __float2bfloat16(z > 0.0f ? z : 0.0f);
@@ -209,6 +212,17 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
         asm volatile("tcgen05.fence::after_thread_sync;");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"((uint32_t)kCols));
+    }
+}
+
+// out[i] = parts[i] + parts[count + i] + ... over `splits` slices, added in
+// slice order.
+__global__ void split_sum_kernel(const float* parts, int splits, long long count, float* out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        float acc = parts[i];
+        for (int z = 1; z < splits; z++) acc += parts[(long long)z * count + i];
+        out[i] = acc;
     }
 }
 

@@ -220,14 +220,19 @@ int grid_for(long long n, int threads = 256) {
 
 // ------------------------------------------------------------- GEMM launch
 
-sidr_status launch_gemm(const GemmArgs& g0, int splits, cudaStream_t st) {
+// Launches C = A B^T.  With splits > 1 the K range is cut into slices of a
+// multiple of kChunkK; epilogue kSplitF32 then writes slice z at
+// C + z*split_stride and *slices receives the number of slices launched.
+sidr_status launch_gemm(const GemmArgs& g0, int splits, cudaStream_t st, int* slices = nullptr) {
     GemmArgs g = g0;
+    if (slices) *slices = 0;
     if (g.M <= 0 || g.N <= 0 || g.K <= 0) return SIDR_OK;
     if (splits < 1) splits = 1;
     int ks = (g.K + splits - 1) / splits;
     ks = (ks + kChunkK - 1) / kChunkK * kChunkK;
     g.k_split = ks;
-    const int gz = (g.K + ks - 1) / ks;
+    const int gz = (g.K + ks - 1) / ks;  // every slice holds at least one chunk
+    if (slices) *slices = gz;
     if (g.N > 64) {
         if (g.N > 256) return fail_s(SIDR_ERR_INVALID, "GEMM N tile above 256");
         dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + 255) / 256, gz);
@@ -236,6 +241,23 @@ sidr_status launch_gemm(const GemmArgs& g0, int splits, cudaStream_t st) {
         dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + 47) / 48, gz);
         umma_gemm_kernel<48><<<grid, 128, 0, st>>>(g);
     }
+    SIDR_SCHECK(cudaGetLastError());
+    return SIDR_OK;
+}
+
+// A split-K GEMM whose M x ldc result is the sum of its slices in slice order
+// (deterministic): the slices go to `parts` (room for kMaxSplits slices),
+// then split_sum_kernel adds them into C.
+constexpr int kMaxSplits = 16;
+sidr_status gemm_split_sum(GemmArgs g, int splits, float* parts, float* C, cudaStream_t st) {
+    const long long count = (long long)g.M * g.ldc;
+    g.epilogue = kSplitF32;
+    g.C = parts;
+    g.split_stride = count;
+    int gz = 0;
+    sidr_status s = launch_gemm(g, std::min(splits, kMaxSplits), st, &gz);
+    if (s || gz == 0) return s;
+    split_sum_kernel<<<(int)std::min<long long>((count + 255) / 256, 148 * 8), 256, 0, st>>>(parts, gz, count, C);
     SIDR_SCHECK(cudaGetLastError());
     return SIDR_OK;
 }
@@ -263,6 +285,7 @@ struct sidr_mlp {
     int all_cap = 0;
     __nv_bfloat16 *Xb = nullptr, *H1b = nullptr, *H2b = nullptr, *dZ2b = nullptr, *dZ1b = nullptr;
     float *y = nullptr, *dy = nullptr, *dZ2 = nullptr, *dH1 = nullptr, *dZ1 = nullptr, *loss = nullptr;
+    float* parts = nullptr;  // split-K partial sums of the weight gradients [kMaxSplits][kHid][kHid]
     int* err = nullptr;
     long long step = 0;
     std::vector<void*> owned;
@@ -345,17 +368,15 @@ sidr_status backward(sidr_mlp* m, int rows) {
     head_delta_kernel<<<grid_for((long long)rows * kHid), 256, 0, st>>>(m->H2b, m->dy, m->w3.p, m->dZ2,
                                                                          m->dZ2b, rows);
     col_sum_kernel<<<(kHid + 127) / 128, 128, 0, st>>>(m->dZ2, m->b2.g, rows, kHid);
-    SIDR_SCHECK(cudaMemsetAsync(m->W2.g, 0, m->W2.n * sizeof(float), st));
-    SIDR_SCHECK(cudaMemsetAsync(m->W1.g, 0, m->W1.n * sizeof(float), st));
-    const int splits = std::max(1, std::min(16, rows / 128));
+    const int splits = std::max(1, std::min(kMaxSplits, rows / 128));
     GemmArgs g{};
     g.error = m->err;
     // dW2[out][in] = sum_b dZ2[b][out] H1[b][in]: M = 256 (out), N = 256 (in), K = rows
     g.A = m->dZ2b; g.sam = 1; g.sak = kHid;
     g.B = m->H1b; g.sbn = 1; g.sbk = kHid;
     g.M = kHid; g.N = kHid; g.K = rows;
-    g.epilogue = kAtomicF32; g.C = m->W2.g; g.ldc = kHid;
-    if ((s = launch_gemm(g, splits, st))) return s;
+    g.ldc = kHid;
+    if ((s = gemm_split_sum(g, splits, m->parts, m->W2.g, st))) return s;
     // dH1[b][in] = sum_out dZ2[b][out] W2[out][in]: M = rows, N = 256, K = 256
     g.A = m->dZ2b; g.sam = kHid; g.sak = 1;
     g.B = m->W2b; g.sbn = 1; g.sbk = kHid;
@@ -369,8 +390,8 @@ sidr_status backward(sidr_mlp* m, int rows) {
     g.A = m->dZ1b; g.sam = 1; g.sak = kHid;
     g.B = m->Xb; g.sbn = 1; g.sbk = kInPad;
     g.M = kHid; g.N = kInPad; g.K = rows;
-    g.epilogue = kAtomicF32; g.C = m->W1.g; g.ldc = kInPad;
-    if ((s = launch_gemm(g, splits, st))) return s;
+    g.ldc = kInPad;
+    if ((s = gemm_split_sum(g, splits, m->parts, m->W1.g, st))) return s;
     SIDR_SCHECK(cudaGetLastError());
     return SIDR_OK;
 }
@@ -414,7 +435,9 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
     int* err = nullptr;
     cudaError_t e = cudaMalloc(&dA, (size_t)M * K * 2);
     if (!e) e = cudaMalloc(&dB, (size_t)N * K * 2);
+    float* parts = nullptr;
     if (!e) e = cudaMalloc(&dC, (size_t)M * N * 4);
+    if (!e && splits > 1) e = cudaMalloc(&parts, (size_t)kMaxSplits * M * N * 4);
     if (!e) e = cudaMalloc(&err, sizeof(int));
     if (!e) e = cudaMemcpy(dA, A, (size_t)M * K * 2, cudaMemcpyHostToDevice);
     if (!e) e = cudaMemcpy(dB, B, (size_t)N * K * 2, cudaMemcpyHostToDevice);
@@ -426,9 +449,9 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
         g.A = dA; g.sam = K; g.sak = 1;
         g.B = dB; g.sbn = K; g.sbk = 1;
         g.M = M; g.N = N; g.K = K;
-        g.epilogue = splits > 1 ? kAtomicF32 : kStoreF32;
+        g.epilogue = kStoreF32;
         g.C = dC; g.ldc = N; g.error = err;
-        s = launch_gemm(g, splits, 0);
+        s = splits > 1 ? gemm_split_sum(g, splits, parts, dC, 0) : launch_gemm(g, 1, 0);
         if (!s) e = cudaDeviceSynchronize();
     }
     int h = 0;
@@ -437,6 +460,7 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
     cudaFree(dA);
     cudaFree(dB);
     cudaFree(dC);
+    cudaFree(parts);
     cudaFree(err);
     if (s) return s;
     if (e) return fail_s(SIDR_ERR_CUDA, std::string("gemm: ") + cudaGetErrorString(e));
@@ -608,6 +632,7 @@ sidr_status sidr_mlp_create(int device, uint64_t seed, sidr_mlp** out) {
     if (!e) e = m->alloc(m->W2b, (size_t)kHid * kHid);
     if (!e) e = m->alloc(m->loss, 1);
     if (!e) e = m->alloc(m->err, 1);
+    if (!e) e = m->alloc(m->parts, (size_t)kMaxSplits * kHid * kHid);
     if (e) {
         delete m;
         return fail_s(SIDR_ERR_CUDA, std::string("surrogate create: ") + cudaGetErrorString(e));

@@ -89,3 +89,24 @@ def test_training_fits_a_smooth_target():
     after = m.gradients(x[:1024], t[:1024])
     assert after < 0.2 * first, (first, after)
     m.close()
+
+
+def test_training_is_deterministic():
+    """The split-K weight gradients are summed slice by slice in a fixed
+    order, so two models trained from the same seed on the same data end with
+    the same bits (and so do split-K GEMMs called twice)."""
+    rng = np.random.default_rng(9)
+    x = rng.normal(0, 1, (3000, 40)).astype(np.float32)
+    t = rng.normal(0, 1, 3000).astype(np.float32)
+    runs = []
+    for _ in range(2):
+        m = SG.MLP(seed=5)
+        m.train(x, t, steps=20, batch=1024, lr=1e-3, seed=7)
+        runs.append({k: m.param(k)[0].copy() for k in SG.PARAM_NAMES})
+        m.close()
+    for k in SG.PARAM_NAMES:
+        assert np.array_equal(runs[0][k].view(np.uint32), runs[1][k].view(np.uint32)), k
+    A = SG.to_bf16_bits(rng.normal(0, 1, (256, 2048)))
+    B = SG.to_bf16_bits(rng.normal(0, 1, (256, 2048)))
+    g1, g2 = SG.gemm_bf16(A, B, splits=16), SG.gemm_bf16(A, B, splits=16)
+    assert np.array_equal(g1.view(np.uint32), g2.view(np.uint32))

@@ -157,6 +157,32 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                          double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
                          sidr_sgp_result* result);
 
+/* The large combined run (no single reference call: the reference runs
+ * exhaust_batched, engine/gp_engine.cu:131-203, once per instance and seed
+ * set, without a surrogate): K instances (zps [K][10], masks [K][61]) x
+ * n_seeds GP runs each (GP seeds first_seed .. first_seed + n_seeds - 1),
+ * population e = k * n_seeds + s, evolved together with the pre-screening of
+ * sidr_sgp_run.  Per generation every population is simulated in ONE
+ * multi-instance launch (sidr_multi_*; shape as in sidr_gp_run_multi), each
+ * on its own train block (base seed seed*10000 + gen) of its instance; each
+ * instance has its own decision situations (from the first generation's best
+ * rule of its first seed) and its own model, trained on the window of all its
+ * seeds' simulated fitness; every population breeds and screens its own
+ * offspring, and all audits run in one more multi-instance launch.  Per
+ * generation g and population e: best_train[g*E + e], held_out[g*E + e] (the
+ * best rule on test_samples scenarios from test_seed of its instance),
+ * rho[g*E + e] (NaN when not audited); any of them may be NULL.  best_rules
+ * (may be NULL): the last generation's best rule of every population as prefix
+ * text, one line each in population order.  With K = 1 and n_seeds = 1 the
+ * run is sidr_sgp_run's, value for value.
+ * result->generations_screened / _fallback count population-generations. */
+sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                               const sidr_gp_config* cfg, const sidr_sgp_config* sc,
+                               const char* terminals_csv, const int64_t* masks, int32_t n_seeds,
+                               int64_t first_seed, int64_t test_seed, int32_t shape,
+                               double* best_train, double* held_out, double* rho,
+                               char* best_rules, int64_t rules_cap, sidr_sgp_result* result);
+
 #ifdef __cplusplus
 }
 #endif

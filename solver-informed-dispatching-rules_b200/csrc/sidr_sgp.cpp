@@ -4,6 +4,7 @@
 // every fitness and plain breeding whenever the model's audit rank
 // correlation is too low.
 #include <chrono>
+#include <cmath>
 #include <numeric>
 #include <set>
 
@@ -39,6 +40,60 @@ void pack_rules(const std::vector<Rule>& rules, const Vocab& v, Packed& pk) {
         compile_at(r, k, v, pk.ops, pk.args, pk.ops.size());
         pk.len.push_back((int32_t)pk.ops.size() - pk.off.back());
     }
+}
+
+
+// The surrogate state of one instance: its decision situations, its model
+// and the window of simulated fitness (all of its seeds) the model trains on.
+struct InstanceSurrogate {
+    std::vector<double> sit_terms;
+    std::vector<int32_t> sit_nc, sit_ref;
+    sidr_mlp* model = nullptr;
+    std::vector<std::vector<float>> hist_x;
+    std::vector<std::vector<double>> hist_t;
+    InstanceSurrogate() = default;
+    InstanceSurrogate(const InstanceSurrogate&) = delete;
+    InstanceSurrogate& operator=(const InstanceSurrogate&) = delete;
+    ~InstanceSurrogate() {
+        if (model) sidr_mlp_destroy(model);
+    }
+};
+
+// Decision situations of one instance: rollouts of `rule` on
+// capture_scenarios scenarios (base seed seed*10000 + 7777), NS decisions of 2
+// .. max_cand candidates drawn with Mt19937(seed*7919 + 17) -- the sampling of
+// sidr_sgp_run.
+sidr_status capture_for(sidr_ctx* ctx, const sidr_instance_desc* inst, const int64_t* mask,
+                        const sidr_sgp_config* sc, uint64_t seed, Packed& rule, InstanceSurrogate& out) {
+    const int n = inst->n, NS = sc->n_situations;
+    sidr_rules_desc r = rule.desc();
+    const int S = sc->capture_scenarios, D = 64, C = sc->max_cand;
+    std::vector<double> smp((size_t)S * n), cap_terms((size_t)S * D * C * 61);
+    std::vector<int32_t> cap_cust((size_t)S * D * C), cap_info((size_t)S * D * 2);
+    sidr_gen_durations(n, inst->durations, 0.2, S, (long long)seed * 10000 + 7777, smp.data());
+    sidr_status st = sidr_capture_situations(ctx, &r, smp.data(), S, mask, D, C, cap_terms.data(),
+                                             cap_cust.data(), cap_info.data());
+    if (st != SIDR_OK) return st;
+    std::vector<int> pool;
+    for (int q = 0; q < S * D; q++)
+        if (cap_info[2 * q] >= 2 && cap_info[2 * q] <= C && cap_info[2 * q + 1] >= 0) pool.push_back(q);
+    if ((int)pool.size() < NS) return gp_fail(SIDR_ERR_INVALID, "too few decision situations captured");
+    Mt19937 srng(seed * 7919 + 17);
+    const std::vector<size_t> pick = srng.sample(pool.size(), (size_t)NS);
+    out.sit_terms.assign((size_t)NS * C * 61, 0.0);
+    for (int j = 0; j < NS; j++) {
+        const int q = pool[pick[j]];
+        const int nc = cap_info[2 * q], chosen = cap_info[2 * q + 1];
+        int ref = -1;
+        for (int c = 0; c < nc; c++)
+            if (cap_cust[(size_t)q * C + c] == chosen) ref = c;
+        if (ref < 0) return gp_fail(SIDR_ERR_KERNEL, "captured choice not among the candidates");
+        std::copy(cap_terms.begin() + (size_t)q * C * 61, cap_terms.begin() + (size_t)(q + 1) * C * 61,
+                  out.sit_terms.begin() + (size_t)j * C * 61);
+        out.sit_nc.push_back(nc);
+        out.sit_ref.push_back(ref);
+    }
+    return SIDR_OK;
 }
 
 }  // namespace
@@ -160,35 +215,14 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
             // situations from the first generation's best rule
             Packed pk;
             pack_rules({gp.pop[bi]}, gp.vocab, pk);
-            sidr_rules_desc r = pk.desc();
-            const int S = sc->capture_scenarios, D = 64, C = sc->max_cand;
-            std::vector<double> smp((size_t)S * n), cap_terms((size_t)S * D * C * 61);
-            std::vector<int32_t> cap_cust((size_t)S * D * C), cap_info((size_t)S * D * 2);
-            sidr_gen_durations(n, inst->durations, 0.2, S, (long long)seed * 10000 + 7777, smp.data());
+            InstanceSurrogate cap;
             const double t0 = now_s();
-            st = sidr_capture_situations(ctx, &r, smp.data(), S, mask, D, C, cap_terms.data(),
-                                         cap_cust.data(), cap_info.data());
+            st = capture_for(ctx, inst, mask, sc, seed, pk, cap);
             t_eval += now_s() - t0;
             if (st != SIDR_OK) return st;
-            std::vector<int> pool;  // decisions with 2..C candidates and a choice
-            for (int q = 0; q < S * D; q++)
-                if (cap_info[2 * q] >= 2 && cap_info[2 * q] <= C && cap_info[2 * q + 1] >= 0) pool.push_back(q);
-            if ((int)pool.size() < NS) return gp_fail(SIDR_ERR_INVALID, "too few decision situations captured");
-            Mt19937 srng(seed * 7919 + 17);
-            const std::vector<size_t> pick = srng.sample(pool.size(), (size_t)NS);
-            sit_terms.assign((size_t)NS * C * 61, 0.0);
-            for (int j = 0; j < NS; j++) {
-                const int q = pool[pick[j]];
-                const int nc = cap_info[2 * q], chosen = cap_info[2 * q + 1];
-                int ref = -1;
-                for (int c = 0; c < nc; c++)
-                    if (cap_cust[(size_t)q * C + c] == chosen) ref = c;
-                if (ref < 0) return gp_fail(SIDR_ERR_KERNEL, "captured choice not among the candidates");
-                std::copy(cap_terms.begin() + (size_t)q * C * 61, cap_terms.begin() + (size_t)(q + 1) * C * 61,
-                          sit_terms.begin() + (size_t)j * C * 61);
-                sit_nc.push_back(nc);
-                sit_ref.push_back(ref);
-            }
+            sit_terms.swap(cap.sit_terms);
+            sit_nc.swap(cap.sit_nc);
+            sit_ref.swap(cap.sit_ref);
             if ((st = sidr_mlp_create(sc->device, sc->model_seed, &model)) != SIDR_OK) return st;
         }
         if (sc->use_surrogate) {
@@ -303,3 +337,297 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
 }
 
 }  // extern "C"
+
+
+// ----------------------------------------------------------------------------
+// Many instances x many seeds (sidr_sgp_run_multi).
+
+extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                                          const sidr_gp_config* cfg, const sidr_sgp_config* sc,
+                                          const char* terminals_csv, const int64_t* masks, int32_t n_seeds,
+                                          int64_t first_seed, int64_t test_seed, int32_t shape,
+                                          double* best_train, double* held_out, double* rho,
+                                          char* best_rules, int64_t rules_cap, sidr_sgp_result* result) {
+    std::string err;
+    if (!insts || !zps || !masks || !sc) return gp_fail(SIDR_ERR_INVALID, "null argument");
+    if (K < 1 || n_seeds < 1) return gp_fail(SIDR_ERR_INVALID, "K < 1 or n_seeds < 1");
+    if ((int64_t)K * n_seeds > 16383) return gp_fail(SIDR_ERR_INVALID, "K * n_seeds > 16383");
+    if (shape < -1 || shape >= SIDR_MULTI_SHAPES) return gp_fail(SIDR_ERR_INVALID, "shape out of range");
+    if (!valid_config(cfg, err)) return gp_fail(SIDR_ERR_INVALID, err);
+    if (sc->n_situations + 8 != SIDR_MLP_INPUTS)
+        return gp_fail(SIDR_ERR_INVALID, "n_situations + 8 must equal the model's 40 inputs");
+    if (sc->screen < cfg->population || sc->audit < 3 || sc->history < 1 || sc->batch < 1 ||
+        sc->capture_scenarios < 1 || sc->max_cand < 2 || cfg->test_samples < 1)
+        return gp_fail(SIDR_ERR_INVALID, "surrogate settings out of range");
+    if (sc->selection < 0 || sc->selection > 1 || sc->target < 0 || sc->target > 1 ||
+        !(sc->screen_fraction >= 0.0 && sc->screen_fraction <= 1.0) || sc->distinct < 0 || sc->distinct > 1)
+        return gp_fail(SIDR_ERR_INVALID, "selection, target, screen_fraction or distinct out of range");
+    for (int k = 0; k < K; k++)
+        if (insts[k].n < 1 || !insts[k].durations)
+            return gp_fail(SIDR_ERR_INVALID, "instance " + std::to_string(k) + ": no customers or no durations");
+    std::vector<std::string> terms;
+    if (!parse_terminals(terminals_csv, terms, err)) return gp_fail(SIDR_ERR_INVALID, err);
+    const int S = n_seeds, E = K * S, ps = cfg->population, T = cfg->train_samples, G = cfg->generations;
+    const int NS = sc->n_situations, NF = SIDR_MLP_INPUTS;
+    const double t_start = now_s();
+    double t_eval = 0.0, t_model = 0.0;
+    int64_t evals = 0;
+    int screened = 0, fallback = 0, chosen = shape;
+
+    // population e = k * S + s: instance k, GP seed first_seed + s
+    std::vector<Gp> gps;
+    gps.reserve(E);
+    for (int e = 0; e < E; e++) {
+        gps.emplace_back(*cfg, (uint64_t)(first_seed + e % S));
+        gps.back().vocab.terminals = terms;
+        gps.back().vocab.n_funcs = cfg->with_rmod ? 7 : 6;
+        gps.back().init();
+    }
+    auto seed_of = [&](int e) { return (long long)(first_seed + e % S); };
+
+    // One multi-instance launch: rule sets[q] (owner q) on instance inst_of[q]
+    // with the scenario block blocks[q] of Tn scenarios; per-rule means.
+    auto simulate = [&](const std::vector<const std::vector<Rule>*>& sets, const std::vector<int>& inst_of,
+                        const std::vector<std::vector<double>>& blocks, int Tn,
+                        std::vector<std::vector<double>>& fit) -> sidr_status {
+        const int Q = (int)sets.size();
+        Packed pk;
+        std::vector<int32_t> owner;
+        std::vector<sidr_instance_desc> d(Q);
+        std::vector<double> z((size_t)Q * 10), flat;
+        std::vector<int64_t> mk((size_t)Q * 61), offs(Q);
+        for (int q = 0; q < Q; q++) {
+            const int k = inst_of[q];
+            pack_rules(*sets[q], gps[0].vocab, pk);
+            owner.insert(owner.end(), sets[q]->size(), q);
+            d[q] = insts[k];
+            std::copy(zps + 10 * (size_t)k, zps + 10 * (size_t)k + 10, z.begin() + 10 * (size_t)q);
+            std::copy(masks + 61 * (size_t)k, masks + 61 * (size_t)k + 61, mk.begin() + 61 * (size_t)q);
+            offs[q] = (int64_t)flat.size();
+            flat.insert(flat.end(), blocks[q].begin(), blocks[q].end());
+        }
+        sidr_rules_desc r = pk.desc();
+        std::vector<double> out((size_t)r.P * Tn);
+        const double t0 = now_s();
+        sidr_multi* m = nullptr;
+        sidr_status st = sidr_multi_create(d.data(), z.data(), Q, &r, owner.data(), flat.data(),
+                                           (int64_t)flat.size(), offs.data(), Tn, mk.data(), sc->device, &m);
+        if (st == SIDR_OK) st = chosen < 0 ? sidr_multi_autotune(m, 1, &chosen, nullptr) : sidr_multi_set_shape(m, chosen);
+        if (st == SIDR_OK) st = sidr_multi_run(m, nullptr);
+        if (st == SIDR_OK) st = sidr_multi_read(m, out.data());
+        const std::string why = st == SIDR_OK ? std::string() : std::string(sidr_last_error());
+        sidr_multi_destroy(m);
+        t_eval += now_s() - t0;
+        evals += (int64_t)r.P * Tn;
+        if (st != SIDR_OK) return gp_fail(st, "evaluation: " + why);
+        fit.assign(Q, {});
+        size_t p = 0;
+        for (int q = 0; q < Q; q++) {
+            fit[q].assign(sets[q]->size(), 0.0);
+            for (size_t i = 0; i < sets[q]->size(); i++, p++) {
+                double acc = 0.0;
+                for (int s = 0; s < Tn; s++) acc += out[p * Tn + s];
+                fit[q][i] = acc / Tn;
+            }
+        }
+        return SIDR_OK;
+    };
+    auto train_blocks = [&](int g) {
+        std::vector<std::vector<double>> blocks(E);
+        for (int e = 0; e < E; e++) {
+            const int n = insts[e / S].n;
+            blocks[e].resize((size_t)T * n);
+            sidr_gen_durations(n, insts[e / S].durations, 0.2, T, seed_of(e) * 10000 + g, blocks[e].data());
+        }
+        return blocks;
+    };
+    std::vector<std::vector<double>> test_blocks(K);
+    for (int k = 0; k < K; k++) {
+        test_blocks[k].resize((size_t)cfg->test_samples * insts[k].n);
+        sidr_gen_durations(insts[k].n, insts[k].durations, 0.2, cfg->test_samples, test_seed,
+                           test_blocks[k].data());
+    }
+    std::vector<int> inst_of_e(E);
+    for (int e = 0; e < E; e++) inst_of_e[e] = e / S;
+
+    std::vector<InstanceSurrogate> sur(K);
+    auto features_of = [&](int k, const std::vector<Rule>& rules, std::vector<float>& f) -> sidr_status {
+        Packed pk;
+        pack_rules(rules, gps[0].vocab, pk);
+        sidr_rules_desc r = pk.desc();
+        f.assign((size_t)r.P * NF, 0.0f);
+        const double t0 = now_s();
+        const sidr_status st = sidr_phenotype(&r, sur[k].sit_terms.data(), sur[k].sit_nc.data(),
+                                              sur[k].sit_ref.data(), NS, sc->max_cand, sc->device, f.data());
+        t_model += now_s() - t0;
+        return st;
+    };
+
+    std::vector<std::vector<double>> fits;
+    for (int g = 0; g < G; g++) {
+        std::vector<const std::vector<Rule>*> sets(E);
+        for (int e = 0; e < E; e++) sets[e] = &gps[e].pop;
+        const std::vector<std::vector<double>> blocks = train_blocks(g);
+        sidr_status st = simulate(sets, inst_of_e, blocks, T, fits);
+        if (st != SIDR_OK) return st;
+        // each population's best rule: train fitness and the held-out block
+        std::vector<size_t> best(E, 0);
+        std::vector<std::vector<Rule>> champions(E);
+        for (int e = 0; e < E; e++) {
+            for (size_t p = 1; p < fits[e].size(); p++)
+                if (fits[e][p] > fits[e][best[e]]) best[e] = p;
+            if (best_train) best_train[(size_t)g * E + e] = fits[e][best[e]];
+            champions[e] = {gps[e].pop[best[e]]};
+            if (rho) rho[(size_t)g * E + e] = std::nan("");
+        }
+        if (g == G - 1 && best_rules) {  // the last generation's best rules as prefix text
+            std::string text;
+            for (int e = 0; e < E; e++) {
+                size_t k = 0;
+                prefix_at(champions[e][0], k, gps[e].vocab, text);
+                text += '\n';
+            }
+            if (rules_cap <= (int64_t)text.size())
+                return gp_fail(SIDR_ERR_INVALID, "best_rules buffer too small");
+            std::memcpy(best_rules, text.c_str(), text.size() + 1);
+        }
+        {
+            std::vector<const std::vector<Rule>*> bsets(E);
+            std::vector<std::vector<double>> tb(E);
+            for (int e = 0; e < E; e++) {
+                bsets[e] = &champions[e];
+                tb[e] = test_blocks[e / S];
+            }
+            std::vector<std::vector<double>> ho;
+            if ((st = simulate(bsets, inst_of_e, tb, cfg->test_samples, ho)) != SIDR_OK) return st;
+            if (held_out)
+                for (int e = 0; e < E; e++) held_out[(size_t)g * E + e] = ho[e][0];
+        }
+        if (!sc->use_surrogate) {
+            if (g < G - 1)
+                for (int e = 0; e < E; e++) gps[e].step(fits[e]);
+            continue;
+        }
+        if (g == 0) {
+            // per instance: situations from the best rule of its first seed, and a model
+            for (int k = 0; k < K; k++) {
+                const int e = k * S;
+                sidr_ctx* ctx = nullptr;
+                if ((st = sidr_ctx_create(&insts[k], zps + 10 * (size_t)k, sc->device, &ctx)) != SIDR_OK) return st;
+                Packed one;
+                pack_rules(champions[e], gps[e].vocab, one);
+                const double t0 = now_s();
+                st = capture_for(ctx, &insts[k], masks + 61 * (size_t)k, sc, (uint64_t)seed_of(e), one, sur[k]);
+                t_eval += now_s() - t0;
+                sidr_ctx_destroy(ctx);
+                if (st != SIDR_OK) return st;
+                if ((st = sidr_mlp_create(sc->device, sc->model_seed + (uint64_t)k, &sur[k].model)) != SIDR_OK)
+                    return st;
+            }
+        }
+        for (int e = 0; e < E; e++) {
+            std::vector<float> f;
+            if ((st = features_of(e / S, gps[e].pop, f)) != SIDR_OK) return st;
+            sur[e / S].hist_x.push_back(std::move(f));
+            sur[e / S].hist_t.push_back(fits[e]);
+        }
+        if (g == G - 1) break;
+        // per instance: train its model on the window of all its seeds' simulated fitness
+        for (int k = 0; k < K; k++) {
+            InstanceSurrogate& u = sur[k];
+            while ((int)u.hist_x.size() > sc->history * 2 * S) {  // population + audit entries per seed
+                u.hist_x.erase(u.hist_x.begin());
+                u.hist_t.erase(u.hist_t.begin());
+            }
+            std::vector<float> X;
+            std::vector<double> all;
+            for (size_t h = 0; h < u.hist_x.size(); h++) {
+                X.insert(X.end(), u.hist_x[h].begin(), u.hist_x[h].end());
+                all.insert(all.end(), u.hist_t[h].begin(), u.hist_t[h].end());
+            }
+            const std::vector<float> Y = training_targets(all, sc->target);
+            float loss = 0.0f;
+            const uint64_t tseed = ((uint64_t)first_seed * 131 + (uint64_t)g) ^ ((uint64_t)k * 0x9e3779b97f4a7c15ull);
+            const double t0 = now_s();
+            st = sidr_mlp_train(u.model, X.data(), Y.data(), (int32_t)Y.size(), sc->train_steps, sc->batch,
+                                sc->lr, tseed, &loss);
+            t_model += now_s() - t0;
+            if (st != SIDR_OK) return st;
+        }
+        // per population: breed, predict, and pick the audit sample
+        std::vector<std::vector<Rule>> cand(E), aud_rules(E);
+        std::vector<std::vector<float>> cf(E), pred(E);
+        std::vector<std::vector<size_t>> aud(E);
+        for (int e = 0; e < E; e++) {
+            const int k = e / S;
+            cand[e] = gps[e].breed(fits[e], (size_t)sc->screen);
+            if ((st = features_of(k, cand[e], cf[e])) != SIDR_OK) return st;
+            pred[e].resize(cand[e].size());
+            const double t0 = now_s();
+            st = sidr_mlp_predict(sur[k].model, cf[e].data(), (int32_t)cand[e].size(), pred[e].data());
+            t_model += now_s() - t0;
+            if (st != SIDR_OK) return st;
+            aud[e] = gps[e].rng.sample(cand[e].size(), (size_t)sc->audit);
+            for (size_t a : aud[e]) aud_rules[e].push_back(cand[e][a]);
+        }
+        // every audit in one launch, each on its population's train block
+        std::vector<const std::vector<Rule>*> asets(E);
+        for (int e = 0; e < E; e++) asets[e] = &aud_rules[e];
+        std::vector<std::vector<double>> aud_fit;
+        if ((st = simulate(asets, inst_of_e, blocks, T, aud_fit)) != SIDR_OK) return st;
+        for (int e = 0; e < E; e++) {
+            const int k = e / S;
+            std::vector<double> aud_pred;
+            std::vector<float> aud_x;
+            for (size_t a : aud[e]) {
+                aud_pred.push_back(pred[e][a]);
+                aud_x.insert(aud_x.end(), cf[e].begin() + a * NF, cf[e].begin() + (a + 1) * NF);
+            }
+            const double r_s = spearman(aud_pred, aud_fit[e]);
+            if (rho) rho[(size_t)g * E + e] = r_s;
+            sur[k].hist_x.push_back(std::move(aud_x));
+            sur[k].hist_t.push_back(aud_fit[e]);
+            if (!(r_s >= sc->rho_min)) {
+                fallback++;
+                gps[e].step(fits[e]);
+                continue;
+            }
+            // elites, then the screened offspring, then plain breeding for the slots left
+            std::vector<int> order(ps);
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return fits[e][a] > fits[e][b]; });
+            std::vector<Rule> next;
+            for (int i = 0; i < cfg->elitism && i < ps; i++) next.push_back(gps[e].pop[order[i]]);
+            const int slots = ps - (int)next.size();
+            const int need = (int)std::lround(sc->screen_fraction * slots);
+            std::vector<int> pick;
+            const std::vector<float>& pe = pred[e];
+            const std::vector<float>& fe = cf[e];
+            if (sc->selection == 1) {
+                pick = preselect(pe, need);
+            } else if (sc->distinct == 1) {
+                pick = best_distinct<std::vector<float>>(pe, (size_t)need, [&](int c) {
+                    return std::vector<float>(fe.begin() + (size_t)c * NF, fe.begin() + (size_t)c * NF + NS);
+                });
+            } else {
+                pick = best_distinct<Rule>(pe, (size_t)need, [&](int c) { return cand[e][c]; });
+            }
+            for (int c : pick) next.push_back(cand[e][c]);
+            if ((int)next.size() < ps) {
+                std::vector<Rule> plain = gps[e].breed(fits[e], (size_t)(ps - (int)next.size()));
+                for (Rule& r : plain) next.push_back(std::move(r));
+            }
+            gps[e].pop.swap(next);
+            screened++;
+        }
+    }
+    if (result) {
+        result->eval_seconds = t_eval;
+        result->model_seconds = t_model;
+        result->host_seconds = now_s() - t_start - t_eval - t_model;
+        result->evaluations = evals;
+        result->generations_screened = screened;
+        result->generations_fallback = fallback;
+    }
+    return SIDR_OK;
+}

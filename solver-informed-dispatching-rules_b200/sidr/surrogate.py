@@ -157,6 +157,10 @@ def _lib2():
         L.sidr_sgp_run.argtypes = [C.c_void_p, C.POINTER(_Inst), C.POINTER(_Cfg), C.POINTER(_SgpCfg),
                                    C.c_char_p, C.POINTER(C.c_int64), C.c_uint64, C.c_int64, _dp, _dp,
                                    _dp, _dp, C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
+        L.sidr_sgp_run_multi.argtypes = [C.POINTER(_Inst), _dp, C.c_int32, C.POINTER(_Cfg),
+                                         C.POINTER(_SgpCfg), C.c_char_p, C.POINTER(C.c_int64),
+                                         C.c_int32, C.c_int64, C.c_int64, C.c_int32, _dp, _dp, _dp,
+                                         C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
         L._sgp_ready = True
     return L
 
@@ -226,6 +230,40 @@ def sgp_run(ctx, terminals, mask, seed: int = 0, test_seed: int = 1000000,
                           secs.ctypes.data_as(_dp), buf, 1 << 16, C.byref(res)))
     return {"best_train": bt, "held_out": ho, "rho": rho, "seconds": secs,
             "best_rule": buf.value.decode(), "eval_seconds": res.eval_seconds,
+            "model_seconds": res.model_seconds, "host_seconds": res.host_seconds,
+            "evaluations": res.evaluations, "screened": res.generations_screened,
+            "fallback": res.generations_fallback}
+
+
+def sgp_run_multi(sds, zps, terminals, masks, n_seeds: int, first_seed: int = 0,
+                  test_seed: int = 1000000, shape: int = -1, gp: Optional[dict] = None,
+                  **sgp_kw) -> dict:
+    """sidr_sgp_run_multi: K instances x n_seeds surrogate-screened GP runs,
+    one multi-instance launch per generation; per generation and population
+    (e = k * n_seeds + s) the best train fitness, held-out score and audit
+    rho, shaped [G, K, n_seeds]."""
+    from . import _Inst, _Keep
+    from .gp import config
+    L = _lib2()
+    c = config(**(gp or {}))
+    s = sgp_config(**sgp_kw)
+    k = _Keep()
+    K = len(sds)
+    insts = (_Inst * K)(*[k.inst(sd) for sd in sds])
+    z = np.ascontiguousarray(np.stack([np.asarray(v, dtype=np.float64) for v in zps]))
+    m = np.ascontiguousarray(np.stack([np.asarray(v, dtype=np.int64) for v in masks]))
+    G = c.generations
+    bt, ho, rho = (np.zeros((G, K, n_seeds)) for _ in range(3))
+    res = _SgpResult()
+    cap = 1 << 24
+    buf = C.create_string_buffer(cap)
+    _check(L.sidr_sgp_run_multi(insts, z.ctypes.data_as(_dp), K, C.byref(c), C.byref(s),
+                                ",".join(terminals).encode(), m.ctypes.data_as(C.POINTER(C.c_int64)),
+                                n_seeds, first_seed, test_seed, shape, bt.ctypes.data_as(_dp),
+                                ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp), buf, cap,
+                                C.byref(res)))
+    return {"best_train": bt, "held_out": ho, "rho": rho,
+            "best_rules": buf.value.decode().splitlines(), "eval_seconds": res.eval_seconds,
             "model_seconds": res.model_seconds, "host_seconds": res.host_seconds,
             "evaluations": res.evaluations, "screened": res.generations_screened,
             "fallback": res.generations_fallback}

@@ -218,3 +218,53 @@ def test_screening_gain_over_random_offspring(setup):
     print("top-predicted mean", true[top].mean(), "random mean", true[rand].mean(), "rho", rho)
     assert true[top].mean() > true[rand].mean()
     m.close()
+
+
+def _small_cfg():
+    gp = dict(population=64, generations=4, train_samples=12, test_samples=20)
+    sg = dict(screen=256, audit=24, train_steps=12, batch=128, history=2)
+    return gp, sg
+
+
+def test_sgp_multi_single_population_is_sgp_run():
+    """With one instance and one seed the combined driver is sidr_sgp_run,
+    value for value (the model's training is deterministic, and the
+    multi-instance launch gives the single-instance scores)."""
+    w = workload.gp_generation(P=1, S=1)
+    zp = sidr.zstats(w.sd)
+    gp, sg = _small_cfg()
+    ctx = sidr.Context(w.sd, zp)
+    one = SG.sgp_run(ctx, workload.MENU29, w.mask, seed=3, test_seed=1000000, gp=gp, **sg)
+    ctx.close()
+    multi = SG.sgp_run_multi([w.sd], [zp], workload.MENU29, [w.mask], 1, first_seed=3,
+                             test_seed=1000000, shape=0, gp=gp, **sg)
+    assert np.array_equal(multi["best_train"][:, 0, 0], one["best_train"])
+    assert np.array_equal(multi["held_out"][:, 0, 0], one["held_out"])
+    r1, r2 = multi["rho"][:, 0, 0], one["rho"]
+    assert np.array_equal(np.isnan(r1), np.isnan(r2)) and np.array_equal(r1[~np.isnan(r1)], r2[~np.isnan(r2)])
+    assert (multi["screened"], multi["fallback"]) == (one["screened"], one["fallback"])
+
+
+def test_sgp_multi_matches_cpu_simulator(oracle):
+    """The large combined run's driver at reduced counts: two 288-customer
+    instances (12-cluster and uniform layouts, m = 4, H = 1000) x two GP seeds,
+    surrogate screening on; the final best rule of every population, scored by
+    the C oracle on its instance's held-out block, gives the driver's held-out
+    score bit for bit, and the run is the same when repeated."""
+    mw = workload.large_combined(K=2, seeds=1, rules_per_seed=1, S=1)
+    zps = [sidr.zstats(sd) for sd in mw.sds]
+    gp, sg = _small_cfg()
+    runs = [SG.sgp_run_multi(mw.sds, zps, workload.MENU29, mw.masks, 2, first_seed=5,
+                             test_seed=1000000, shape=-1, gp=gp, **sg) for _ in range(2)]
+    a, b = runs
+    for key in ("best_train", "held_out"):
+        assert np.array_equal(a[key], b[key]), key
+    assert a["best_rules"] == b["best_rules"]
+    assert a["screened"] + a["fallback"] == 2 * 2 * (gp["generations"] - 1)
+    for e, text in enumerate(a["best_rules"]):
+        k = e // 2
+        sd = mw.sds[k]
+        rules = R.pack([text])
+        test = R.gen_durations(sd.durations, sd.sigma, gp["test_samples"], 1000000)
+        cpu = oracle.eval_pairs(sd, zps[k], rules, test, gp["test_samples"], mw.masks[k])
+        assert cpu.sum() / gp["test_samples"] == a["held_out"][-1, k, e % 2], e

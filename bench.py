@@ -97,6 +97,10 @@ def parse_args():
                     help="with --multi: use this block shape (index into sidr.Multi.SHAPES) "
                          "instead of autotuning, e.g. at full size (--multi-rules 1000 --multi-S 500), "
                          "where each autotuning launch takes about a minute")
+    ap.add_argument("--sharded", action="store_true",
+                    help="instead of one independent generation per GPU, run the benchmark GP with "
+                         "every generation's rules sharded over the ranks (fitness all_gather, "
+                         "strong scaling): W untimed generations, then K timed ones")
     ap.add_argument("--multi-rules", type=int, default=100)
     ap.add_argument("--multi-S", type=int, default=100)
     return ap.parse_args()
@@ -631,11 +635,57 @@ def gp_leg(ctx, w, args):
             "best_train_last": float(res.best_train[-1, 0]), "best_rule": res.best_rules[0]}
 
 
+def run_sharded(args, rank, world, local):
+    """The benchmark GP (1024 rules, 500 training scenarios per generation),
+    its rules sharded over the ranks (sidr.dist.sharded_gp): each generation
+    evaluates this rank's block on its GPU, all_gathers the fitness and steps
+    the same GP on every rank.  A step is one generation, timed on the host
+    (evaluation, gather and GP step) and maximised over ranks."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    import sidr
+    from sidr import dist as D
+    from sidr import workload as W
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group("gloo", init_method="tcp://127.0.0.1:29533", rank=0, world_size=1)
+    w = W.gp_generation(P=1, S=1)
+    ctx = sidr.Context(w.sd, sidr.zstats(w.sd), device=local)
+    times = []
+    dev = torch.device("cuda", local) if world > 1 else None
+    D.sharded_gp(ctx, W.MENU29, w.mask, seed=0, generations=args.warmup + args.steps,
+                 population=args.P, train_samples=args.S, device=dev,
+                 on_generation=lambda g, sec: times.append(sec) if g >= args.warmup else None)
+    total = D.max_over_ranks(sum(times), device=dev)
+    ctx.close()
+    dist.destroy_process_group()
+    if rank == 0:
+        value = args.P * args.S * args.steps / total
+        print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic",
+                          "config": dict(config_of(args.P, args.S, world),
+                                         parallelism=f"rule shards over {world} GPUs, fitness "
+                                                     f"all_gather per generation",
+                                         step="one GP generation (host wall clock: evaluation, "
+                                              "gather and GP step), max over ranks")}),
+              flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.sharded:
+        run_sharded(args, rank, world, local)
         return
     run_ours(args, rank, world, local)
 

@@ -565,6 +565,7 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
         const uint32_t own = has ? bit_in_word(v.ci, w) : 0u;
         if (COUNT && has) heavy += __popc(word & ~own);
         __syncwarp();  // the previous word's queue reads are done
+        SIDR_SEC_MARK(t_p1)
         uint32_t addm = 0, ewm = 0, ebm = 0, pbm = 0;
         int qn = 0;
         for (uint32_t bits = word; bits;) {
@@ -604,15 +605,19 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
                 }
             }
         }
+        SIDR_SEC_ADD(11, t_p1);
         if (qn > v.cap) {  // warp-uniform
             eloss = at_risk_word_direct(v, w, word, eloss);
             continue;
         }
+        SIDR_SEC_MARK(t_q)
         if (qn) {
             __syncwarp();
             for (int k = lane; k < qn; k += 32) Q[2 * k] = norm_cdf_ratio(Q[2 * k], Q[2 * k + 1]);
             __syncwarp();
         }
+        SIDR_SEC_ADD(12, t_q);
+        SIDR_SEC_MARK(t_p2)
         const int jl = (w << 5) + lane;
         const double sw = jl < v.n ? v.scores[jl] : 0.0;
         const uint32_t anym = addm | ewm | ebm;
@@ -639,6 +644,7 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
                 }
             }
         }
+        SIDR_SEC_ADD(13, t_p2);
     }
     __syncwarp();
     if (COUNT) {
@@ -1090,8 +1096,10 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         const int k = base + lane;
         double pri = -1e300;
         int idx = 0x7fffffff;
+        SIDR_SEC_MARK(t_atr)
         const double eloss =
             need_atr ? at_risk<COUNT>(at_risk_view(I, S, d, k < ncand ? S.cand[k] : -1), wc) : 0.0;
+        SIDR_SEC_ADD(10, t_atr);
         if (k < ncand) {
             idx = S.cand[k];
             pri = score_candidate<COUNT>(I, S, rm, d, idx, eloss, wc);

@@ -58,3 +58,36 @@ def sharded_fitness(evaluate: Callable[[Sequence[int]], np.ndarray], P: int, gro
     lo, hi = shard_range(P, rank, world)
     local = np.asarray(evaluate(range(lo, hi)), dtype=np.float64) if hi > lo else np.zeros(0)
     return gather_fitness(local, P, group, device)
+
+
+def sharded_gp(ctx, terminals: Sequence[str], mask, seed: int = 0, generations: int = 50,
+               population: int = 1024, train_samples: int = 500, group=None, device=None,
+               on_generation=None, **cfg):
+    """The benchmark GP of gp.run_batched for one seed (engine/gp.hpp's GP,
+    train block of base seed seed*10000 + gen), with every generation's
+    fitness sharded over the ranks of `group`: each rank evaluates its block
+    of the population on its own GPU (ctx), the blocks are gathered, and every
+    rank steps the same GP.  Returns (session, best train fitness per
+    generation); on_generation(g, seconds) is called after each generation
+    with its wall clock on this rank."""
+    import time
+    from . import gp as G
+    sess = G.Session(terminals, seed, population=population, generations=generations,
+                     train_samples=train_samples, **cfg)
+    best = []
+    for g in range(generations):
+        t0 = time.perf_counter()
+        smp = G.gen_durations(ctx.sd.durations, ctx.sd.sigma, train_samples, seed * 10000 + g)
+        pk = sess.packed()
+
+        def evaluate(idx):
+            out = ctx.evaluate(pk.subset(list(idx)), smp, train_samples, mask)
+            return out.sum(axis=1) / train_samples  # integer-valued scores: exact in any order
+
+        f = sharded_fitness(evaluate, population, group, device)
+        best.append(float(f.max()))
+        if g < generations - 1:
+            sess.step(f)
+        if on_generation:
+            on_generation(g, time.perf_counter() - t0)
+    return sess, np.array(best)

@@ -75,3 +75,48 @@ def test_two_ranks_stay_in_lockstep(tmp_path):
         f = np.array([float(pk.lengths[i] * 3 + (pk.ops[pk.offsets[i]] % 5)) for i in range(37)])
         assert np.array_equal(f, a[37 * g:37 * (g + 1)])
         sess.step(f)
+
+
+def _gp_worker(rank, world, port, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import sidr
+        from sidr import workload
+        w = workload.gp_generation(P=1, S=1)
+        ctx = sidr.Context(w.sd, sidr.zstats(w.sd))
+        sess, best = D.sharded_gp(ctx, workload.MENU29, w.mask, seed=2, generations=3,
+                                  population=48, train_samples=8)
+        np.save(os.path.join(out_dir, f"best{rank}.npy"), best)
+        with open(os.path.join(out_dir, f"gp{rank}.txt"), "w") as fh:
+            fh.write("\n".join(sess.text()))
+        ctx.close()
+    finally:
+        dist.destroy_process_group()
+
+
+import pytest  # noqa: E402
+
+from conftest import cuda_available  # noqa: E402
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+def test_sharded_gp_matches_the_seed_batched_driver(tmp_path):
+    """The GP with rule shards over two ranks (both on this run's one GPU,
+    gloo between them) evolves exactly as the seed-batched driver does in one
+    process: same best train fitness every generation, same population."""
+    port = _free_port()
+    mp.spawn(_gp_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True)
+    b0, b1 = np.load(tmp_path / "best0.npy"), np.load(tmp_path / "best1.npy")
+    assert np.array_equal(b0, b1)
+    assert (tmp_path / "gp0.txt").read_text() == (tmp_path / "gp1.txt").read_text()
+    import sidr
+    from sidr import gp, workload
+    w = workload.gp_generation(P=1, S=1)
+    ctx = sidr.Context(w.sd, sidr.zstats(w.sd))
+    res = gp.run_batched(ctx, workload.MENU29, w.mask, 1, first_seed=2, population=48,
+                         generations=3, train_samples=8, test_samples=4)
+    ctx.close()
+    assert np.array_equal(res.best_train[:, 0], b0)

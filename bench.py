@@ -472,36 +472,48 @@ def run_ours(args, rank, world, local):
 def multi_leg(args, stream):
     """The uneven batch (40 instances: 25/50/100/288 customers, three layouts,
     m 2-4, H 230/1000, rules of log-uniform length 3-255) in one persistent
-    launch: autotuned block shape, CUDA-graph replay, device-timed."""
+    launch: block shape autotuned on a sample of the batch (every 16th rule of
+    the longest-first order) unless --multi-shape is given, CUDA-graph replay,
+    device-timed.  Then, per instance-size class, the same instances in a
+    launch of their own and one by one through the single-instance path, which
+    shows where the batch's time goes."""
+    import numpy as np
     import torch
     import sidr
     from sidr import workload
+
+    def timed(run, reps=2):
+        run()
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        return best
+
     t0 = time.perf_counter()
     mw = workload.batched_uneven(K=40, rules_per_instance=args.multi_rules, S=args.multi_S)
     zps = [sidr.zstats(sd) for sd in mw.sds]
     m = sidr.Multi(mw.sds, zps, mw.rules, mw.sampled, mw.S, mw.masks)
     prep = time.perf_counter() - t0
+    t_tune = time.perf_counter()
     if args.multi_shape >= 0:
         chosen, ms = args.multi_shape, None
         m.set_shape(chosen)
     else:
-        chosen, ms = m.autotune(reps=1)
+        chosen, ms = m.autotune_sampled(stride=16, reps=1)
+    t_tune = time.perf_counter() - t_tune
     m.capture()
-    m.run(stream.cuda_stream)
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(3)]
-    for e0, e1 in ev:
-        e0.record(stream)
-        m.run(stream.cuda_stream)
-        e1.record(stream)
-    torch.cuda.synchronize()
-    t = min(e0.elapsed_time(e1) for e0, e1 in ev) / 1e3
+    t = timed(lambda: m.run(stream.cuda_stream))
     P = sum(r.P for r in mw.rules)
     res = m.read()
     m.close()
     # spot check: every 125th rule of instances 3 (288 customers) and 38 by the single-instance path
-    import numpy as np
     mism, pairs = 0, 0
     for k in (3, 38):
         ctx = sidr.Context(mw.sds[k], zps[k])
@@ -510,10 +522,30 @@ def multi_leg(args, stream):
         mism += int((res[k][idx].view(np.uint64) != want.view(np.uint64)).sum())
         pairs += want.size
         ctx.close()
+    classes = {}
+    for n in sorted({sd.n for sd in mw.sds}):
+        ks = [k for k, sd in enumerate(mw.sds) if sd.n == n]
+        mc = sidr.Multi([mw.sds[k] for k in ks], [zps[k] for k in ks], [mw.rules[k] for k in ks],
+                        [mw.sampled[k] for k in ks], mw.S, [mw.masks[k] for k in ks])
+        mc.set_shape(chosen)
+        tc = timed(lambda: mc.run(stream.cuda_stream), reps=1)
+        mc.close()
+        t_one = 0.0
+        for k in ks:
+            ctx = sidr.Context(mw.sds[k], zps[k])
+            b = ctx.batch(mw.rules[k], mw.sampled[k], mw.S, mw.masks[k])
+            t_one += timed(lambda: b.run(stream.cuda_stream), reps=1)
+            b.close()
+            ctx.close()
+        ev = sum(mw.rules[k].P for k in ks) * mw.S
+        classes[str(n)] = {"instances": len(ks), "evaluations": ev, "own_launch_seconds": tc,
+                           "own_launch_evals_per_s": ev / tc, "one_by_one_seconds": t_one,
+                           "one_by_one_evals_per_s": ev / t_one}
     return {"workload": f"40 instances x {args.multi_rules} rules x {args.multi_S} scenarios",
             "evaluations": P * mw.S, "seconds": t, "evals_per_s": P * mw.S / t,
-            "shapes_ms": ms, "chosen_shape": list(sidr.Multi.SHAPES[chosen]),
-            "host_prep_seconds": prep, "spot_check_pairs": pairs, "spot_check_mismatches": mism}
+            "shapes_ms_on_sample": ms, "tuning_seconds": t_tune,
+            "chosen_shape": list(sidr.Multi.SHAPES[chosen]), "host_prep_seconds": prep,
+            "spot_check_pairs": pairs, "spot_check_mismatches": mism, "per_size_class": classes}
 
 
 def campaign_leg():

@@ -170,6 +170,12 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
                               const int64_t* sampled_offsets, int32_t T, const int64_t* masks,
                               int32_t device, sidr_multi** out);
 sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, float* ms);
+/* The same choice made on a sample of the batch: each shape is timed on every
+ * stride-th rule of the longest-first work order (all T scenarios), so that
+ * the sample keeps the batch's mix of instance sizes and rule costs and the
+ * tuning of a full-size batch takes about 1/stride of a launch per shape. */
+sidr_status sidr_multi_autotune_sampled(sidr_multi* m, int32_t reps, int32_t stride, int32_t* chosen,
+                                        float* ms);
 sidr_status sidr_multi_set_shape(sidr_multi* m, int32_t shape);
 sidr_status sidr_multi_capture(sidr_multi* m);
 sidr_status sidr_multi_run(sidr_multi* m, void* stream);

@@ -1132,6 +1132,7 @@ struct sidr_multi {
     int grid[SIDR_MULTI_SHAPES] = {}, block[SIDR_MULTI_SHAPES] = {};
     size_t smem[SIDR_MULTI_SHAPES] = {};
     std::string key;
+    std::vector<int32_t> order;  // the longest-first work order (host copy)
     cudaStream_t gstream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -1304,6 +1305,7 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
         (e = cudaMemset((void*)b.error, 0, sizeof(int))))
         return bail(e, "batch upload");
     b.n_inst = K;
+    m->order = order;
     b.P = r->P;
     b.T = T;
     b.group_size = r->P > 0 ? r->P : 1;
@@ -1389,6 +1391,64 @@ sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, fl
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    m->shape = best_sh;
+    {
+        std::lock_guard<std::mutex> g(g_tune_lock);
+        g_tune_cache[m->key] = best_sh;
+    }
+    if (chosen) *chosen = best_sh;
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_autotune_sampled(sidr_multi* m, int32_t reps, int32_t stride, int32_t* chosen,
+                                        float* ms) {
+    if (!m || stride < 1) return fail(SIDR_ERR_INVALID, "null batch or stride < 1");
+    if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
+    DeviceGuard device_guard;
+    SIDR_CUDA(cudaSetDevice(m->device));
+    if ((long long)m->P * m->T == 0) {
+        if (chosen) *chosen = m->shape;
+        return SIDR_OK;
+    }
+    // every stride-th rule of the longest-first order: the sample keeps the batch's mix of costs
+    std::vector<int32_t> sample;
+    for (size_t i = 0; i < m->order.size(); i += (size_t)stride) sample.push_back(m->order[i]);
+    int32_t* d_order = nullptr;
+    SIDR_CUDA(cudaMalloc(&d_order, sample.size() * sizeof(int32_t)));
+    cudaError_t e = cudaMemcpy(d_order, sample.data(), sample.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    const DevBatch full = m->b;
+    m->b.order = d_order;
+    m->b.P_items = (int)sample.size();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!e) e = cudaEventCreate(&e0);
+    if (!e) e = cudaEventCreate(&e1);
+    float best = 1e30f;
+    int best_sh = 0;
+    sidr_status s = SIDR_OK;
+    for (int sh = 0; sh < SIDR_MULTI_SHAPES && !e && !s; sh++) {
+        float t_best = 1e30f;
+        for (int k = 0; k < (reps < 1 ? 1 : reps) + 1 && !e && !s; k++) {  // first run warms up
+            e = cudaEventRecord(e0, 0);
+            if (!e) s = multi_launch(m, sh, 0);
+            if (!e && !s) e = cudaEventRecord(e1, 0);
+            if (!e && !s) e = cudaEventSynchronize(e1);
+            float t = 0.f;
+            if (!e && !s) e = cudaEventElapsedTime(&t, e0, e1);
+            if (k > 0 && t < t_best) t_best = t;
+        }
+        if (ms) ms[sh] = t_best;
+        if (t_best < best) {
+            best = t_best;
+            best_sh = sh;
+        }
+    }
+    m->b = full;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_order);
+    if (s) return s;
+    if (e) return fail(SIDR_ERR_CUDA, std::string("sampled autotune: ") + cudaGetErrorString(e));
+    if ((s = read_error_word(m->b.error, 0))) return s;
     m->shape = best_sh;
     {
         std::lock_guard<std::mutex> g(g_tune_lock);

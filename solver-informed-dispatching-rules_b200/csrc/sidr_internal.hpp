@@ -149,7 +149,8 @@ struct DevBatch {
     const DevInst* insts;
     const int64_t* smp_off;
     const int32_t* order;
-    int n_inst;  // descriptors at insts
+    int n_inst;   // descriptors at insts
+    int P_items;  // rules in the work queue (0: all P); with `order`, a sample of the batch
 };
 
 // Codes of the kernel error word (DevBatch::error); the host turns a nonzero

@@ -1202,7 +1202,8 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
     const size_t slice = warp_slice_bytes(B.rows, B.const_cap, B.prog_cap);
     const WarpSmem S = carve(smem_raw + (size_t)wib * slice, B.rows, B.const_cap, B.prog_cap);
 
-    const unsigned long long total = (unsigned long long)B.P * (unsigned long long)B.T;
+    const unsigned long long total =
+        (unsigned long long)(B.P_items > 0 ? B.P_items : B.P) * (unsigned long long)B.T;
     int staged = -1;
     RuleMeta rm;
     WarpCounts wc = {0, 0, 0, 0, 0, 0};

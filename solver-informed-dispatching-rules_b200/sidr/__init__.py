@@ -66,7 +66,7 @@ EXPORTS = [
     "sidr_kernel_launches", "sidr_rules_check", "sidr_last_transfer_bytes", "sidr_fp64_peak",
     "sidr_evaluate_static", "sidr_multi_create", "sidr_multi_autotune", "sidr_multi_set_shape",
     "sidr_multi_capture", "sidr_multi_run", "sidr_multi_read", "sidr_multi_destroy",
-    "sidr_libm_eval", "sidr_batch_guard_check", "sidr_libm_pow",
+    "sidr_libm_eval", "sidr_batch_guard_check", "sidr_libm_pow", "sidr_multi_autotune_sampled",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -364,6 +364,8 @@ class Multi:
                                             C.POINTER(vp)]
             L.sidr_multi_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32),
                                               C.POINTER(C.c_float)]
+            L.sidr_multi_autotune_sampled.argtypes = [vp, C.c_int32, C.c_int32,
+                                                      C.POINTER(C.c_int32), C.POINTER(C.c_float)]
             L.sidr_multi_set_shape.argtypes = [vp, C.c_int32]
             L.sidr_multi_capture.argtypes = [vp]
             L.sidr_multi_run.argtypes = [vp, vp]
@@ -402,6 +404,14 @@ class Multi:
         ch = C.c_int32()
         ms = (C.c_float * len(self.SHAPES))()
         _check(load().sidr_multi_autotune(self.h, reps, C.byref(ch), ms))
+        return ch.value, [float(x) for x in ms]
+
+    def autotune_sampled(self, stride: int = 16, reps: int = 1):
+        """sidr_multi_autotune_sampled: the block shape chosen on every
+        stride-th rule of the longest-first order."""
+        ch = C.c_int32()
+        ms = (C.c_float * len(self.SHAPES))()
+        _check(load().sidr_multi_autotune_sampled(self.h, reps, stride, C.byref(ch), ms))
         return ch.value, [float(x) for x in ms]
 
     def set_shape(self, shape: int):

@@ -39,6 +39,11 @@ def test_multi_matches_per_instance(oracle):
             assert np.array_equal(bits(got), bits(want[k])), (shape, k)
     chosen, ms = m.autotune(reps=1)
     assert 0 <= chosen < len(ms) and all(t > 0 for t in ms)
+    chosen, ms = m.autotune_sampled(stride=4, reps=1)  # timed on every 4th rule of the work order
+    assert 0 <= chosen < len(ms) and all(t > 0 for t in ms)
+    m.run()
+    for k, got in enumerate(m.read()):
+        assert np.array_equal(bits(got), bits(want[k])), ("after sampled tuning", k)
     m.capture()
     for _ in range(2):
         m.run()

@@ -46,7 +46,7 @@
 // erf and erfc stay out of line on the device: they run only for arguments
 // whose result is not exactly 0 or 1, and inlining them into the neighbour
 // scans would raise their register count
-#define SIDR_HD_CALL __host__ __device__ __noinline__
+#define SIDR_HD_CALL static __host__ __device__ __noinline__  // one copy per translation unit
 #else
 #define SIDR_HD inline
 #define SIDR_HD_CALL inline

@@ -1,9 +1,10 @@
 // sidr_surrogate.cu -- the surrogate fitness model of the surrogate-assisted
 // GP (include/sidr_surrogate.h): a 40 -> 256 -> 256 -> 1 ReLU MLP with BF16
 // weights and activations and FP32 accumulation, trained on the device with
-// Adam.  Its four GEMMs per step (two forward, two of the backward pass's
-// three) and the two weight-gradient GEMMs run on the tcgen05 kernel of
-// sidr_mlp.cuh; the 256 -> 1 layer, the ReLU masks, the bias gradients, the
+// Adam.  Its five GEMMs per training step (two forward, the backward pass's
+// input gradient and two weight gradients) run on the TMA-fed tcgen05 kernel
+// of sidr_mlp.cuh, the backward ones on K-major copies made by a transpose
+// kernel; the 256 -> 1 layer, the ReLU masks, the bias gradients, the
 // loss and Adam are small element-wise kernels.  Also here: the phenotype
 // kernel (each rule's priority ranking on fixed decision situations) and the
 // diagnostic GEMM entry point.
@@ -18,6 +19,7 @@
 #include "../../include/sidr_surrogate.h"
 #include "sidr_device.hpp"
 #include "sidr_host.hpp"
+#include "sidr_libm.cuh"
 #include "sidr_mlp.cuh"
 
 using namespace sidr;
@@ -182,7 +184,7 @@ __device__ double eval_rule(const int32_t* ops, const int32_t* args, int len, co
             else {
                 const double base = a > 0.0 ? a : 0.0;
                 const double e = b < 0.0 ? 0.0 : (b > 1.0 ? 1.0 : b);
-                r = pow(base, 1.0 + e);
+                r = libm::pow_(base, 1.0 + e);
             }
             st[sp++] = r;
         }
@@ -220,8 +222,50 @@ int grid_for(long long n, int threads = 256) {
 
 // ------------------------------------------------------------- GEMM launch
 
-// Launches C = A B^T.  With splits > 1 the K range is cut into slices of a
-// multiple of kChunkK; epilogue kSplitF32 then writes slice z at
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
+// (the library links no driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// The tensor map of a K-major BF16 operand [rows][K] with row stride ld
+// elements: boxes of kChunkK x box_rows with the 128-byte swizzle, zeros
+// outside the extent.
+sidr_status operand_map(CUtensorMap* map, const __nv_bfloat16* p, int rows, int K, long long ld, int box_rows) {
+    if (((uintptr_t)p & 15u) != 0 || (ld * 2) % 16 != 0)
+        return fail_s(SIDR_ERR_INVALID, "GEMM operand: base or row stride not a multiple of 16 bytes");
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return fail_s(SIDR_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kChunkK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail_s(SIDR_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return SIDR_OK;
+}
+
+bool smem_attr_set[256] = {};  // per device: the kernel's dynamic shared-memory limit raised
+std::mutex smem_attr_lock;
+
+// Launches C = A B^T (both K-major).  With splits > 1 the K range is cut into
+// slices of a multiple of kChunkK; epilogue kSplitF32 then writes slice z at
 // C + z*split_stride and *slices receives the number of slices launched.
 sidr_status launch_gemm(const GemmArgs& g0, int splits, cudaStream_t st, int* slices = nullptr) {
     GemmArgs g = g0;
@@ -233,17 +277,38 @@ sidr_status launch_gemm(const GemmArgs& g0, int splits, cudaStream_t st, int* sl
     g.k_split = ks;
     const int gz = (g.K + ks - 1) / ks;  // every slice holds at least one chunk
     if (slices) *slices = gz;
-    if (g.N > 64) {
-        if (g.N > 256) return fail_s(SIDR_ERR_INVALID, "GEMM N tile above 256");
-        dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + 255) / 256, gz);
-        umma_gemm_kernel<256><<<grid, 128, 0, st>>>(g);
-    } else {
-        dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + 47) / 48, gz);
-        umma_gemm_kernel<48><<<grid, 128, 0, st>>>(g);
+    CUtensorMap ma, mb;
+    sidr_status s = operand_map(&ma, g.A, g.M, g.K, g.lda, kTileM);
+    if (s) return s;
+    if ((s = operand_map(&mb, g.B, g.N, g.K, g.ldb, kTileN))) return s;
+    {
+        int dev = 0;
+        SIDR_SCHECK(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(smem_attr_lock);
+        if (dev < 0 || dev >= 256) return fail_s(SIDR_ERR_INVALID, "device index out of range");
+        if (!smem_attr_set[dev]) {
+            SIDR_SCHECK(cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kGemmSmem));
+            smem_attr_set[dev] = true;
+        }
     }
+    dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + kTileN - 1) / kTileN, gz);
+    umma_gemm_kernel<<<grid, 128, kGemmSmem, st>>>(ma, mb, g);
     SIDR_SCHECK(cudaGetLastError());
     return SIDR_OK;
 }
+
+// dst [cols][ldd] = src [rows][lds] transposed (an M- or N-contiguous operand
+// turned K-major); ldd is a multiple of 8 elements.
+sidr_status transpose(const __nv_bfloat16* src, int rows, int cols, long long lds, __nv_bfloat16* dst,
+                      long long ldd, cudaStream_t st) {
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    transpose_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(src, rows, cols, lds, dst, ldd);
+    SIDR_SCHECK(cudaGetLastError());
+    return SIDR_OK;
+}
+
+long long pad8(long long x) { return (x + 7) / 8 * 8; }
 
 // A split-K GEMM whose M x ldc result is the sum of its slices in slice order
 // (deterministic): the slices go to `parts` (room for kMaxSplits slices),
@@ -286,6 +351,9 @@ struct sidr_mlp {
     __nv_bfloat16 *Xb = nullptr, *H1b = nullptr, *H2b = nullptr, *dZ2b = nullptr, *dZ1b = nullptr;
     float *y = nullptr, *dy = nullptr, *dZ2 = nullptr, *dH1 = nullptr, *dZ1 = nullptr, *loss = nullptr;
     float* parts = nullptr;  // split-K partial sums of the weight gradients [kMaxSplits][kHid][kHid]
+    // K-major copies of the operands the backward pass reads M- or N-contiguous
+    __nv_bfloat16 *dZ2T = nullptr, *H1T = nullptr, *dZ1T = nullptr, *XbT = nullptr, *W2T = nullptr;
+    long long ldT = 0;  // row stride of dZ2T/H1T/dZ1T/XbT: cap rounded up to 8
     int* err = nullptr;
     long long step = 0;
     std::vector<void*> owned;
@@ -325,8 +393,11 @@ sidr_status ensure_rows(sidr_mlp* m, int rows) {
         (e = m->alloc(m->H2b, (size_t)cap * kHid)) || (e = m->alloc(m->dZ2b, (size_t)cap * kHid)) ||
         (e = m->alloc(m->dZ1b, (size_t)cap * kHid)) || (e = m->alloc(m->y, cap)) ||
         (e = m->alloc(m->dy, cap)) || (e = m->alloc(m->dZ2, (size_t)cap * kHid)) ||
-        (e = m->alloc(m->dH1, (size_t)cap * kHid)) || (e = m->alloc(m->dZ1, (size_t)cap * kHid)))
+        (e = m->alloc(m->dH1, (size_t)cap * kHid)) || (e = m->alloc(m->dZ1, (size_t)cap * kHid)) ||
+        (e = m->alloc(m->dZ2T, (size_t)kHid * pad8(cap))) || (e = m->alloc(m->H1T, (size_t)kHid * pad8(cap))) ||
+        (e = m->alloc(m->dZ1T, (size_t)kHid * pad8(cap))) || (e = m->alloc(m->XbT, (size_t)kInPad * pad8(cap))))
         return fail_s(SIDR_ERR_CUDA, std::string("surrogate buffers: ") + cudaGetErrorString(e));
+    m->ldT = pad8(cap);
     m->cap = cap;  // (older, smaller buffers stay owned until the model is destroyed)
     return SIDR_OK;
 }
@@ -342,15 +413,15 @@ sidr_status forward(sidr_mlp* m, int rows) {
     GemmArgs g{};
     g.error = m->err;
     // H1 = relu(Xb W1^T + b1): M = rows, N = 256, K = 48
-    g.A = m->Xb; g.sam = kInPad; g.sak = 1;
-    g.B = m->W1b; g.sbn = kInPad; g.sbk = 1;
+    g.A = m->Xb; g.lda = kInPad;
+    g.B = m->W1b; g.ldb = kInPad;
     g.M = rows; g.N = kHid; g.K = kInPad;
     g.epilogue = kBiasRelu; g.bias = m->b1.p; g.Hb = m->H1b; g.ldh = kHid;
     sidr_status s = launch_gemm(g, 1, m->st);
     if (s) return s;
     // H2 = relu(H1 W2^T + b2): K = 256
-    g.A = m->H1b; g.sam = kHid; g.sak = 1;
-    g.B = m->W2b; g.sbn = kHid; g.sbk = 1;
+    g.A = m->H1b; g.lda = kHid;
+    g.B = m->W2b; g.ldb = kHid;
     g.K = kHid; g.bias = m->b2.p; g.Hb = m->H2b;
     if ((s = launch_gemm(g, 1, m->st))) return s;
     head_forward_kernel<<<(rows + 127) / 128, 128, 0, m->st>>>(m->H2b, m->w3.p, m->b3.p, m->y, rows);
@@ -371,24 +442,30 @@ sidr_status backward(sidr_mlp* m, int rows) {
     const int splits = std::max(1, std::min(kMaxSplits, rows / 128));
     GemmArgs g{};
     g.error = m->err;
-    // dW2[out][in] = sum_b dZ2[b][out] H1[b][in]: M = 256 (out), N = 256 (in), K = rows
-    g.A = m->dZ2b; g.sam = 1; g.sak = kHid;
-    g.B = m->H1b; g.sbn = 1; g.sbk = kHid;
+    // dW2[out][in] = sum_b dZ2[b][out] H1[b][in]: M = 256 (out), N = 256 (in), K = rows,
+    // on K-major copies dZ2^T [out][b] and H1^T [in][b]
+    if ((s = transpose(m->dZ2b, rows, kHid, kHid, m->dZ2T, m->ldT, st))) return s;
+    if ((s = transpose(m->H1b, rows, kHid, kHid, m->H1T, m->ldT, st))) return s;
+    g.A = m->dZ2T; g.lda = m->ldT;
+    g.B = m->H1T; g.ldb = m->ldT;
     g.M = kHid; g.N = kHid; g.K = rows;
     g.ldc = kHid;
     if ((s = gemm_split_sum(g, splits, m->parts, m->W2.g, st))) return s;
-    // dH1[b][in] = sum_out dZ2[b][out] W2[out][in]: M = rows, N = 256, K = 256
-    g.A = m->dZ2b; g.sam = kHid; g.sak = 1;
-    g.B = m->W2b; g.sbn = 1; g.sbk = kHid;
+    // dH1[b][in] = sum_out dZ2[b][out] W2[out][in]: M = rows, N = 256, K = 256, B = W2^T [in][out]
+    if ((s = transpose(m->W2b, kHid, kHid, kHid, m->W2T, kHid, st))) return s;
+    g.A = m->dZ2b; g.lda = kHid;
+    g.B = m->W2T; g.ldb = kHid;
     g.M = rows; g.N = kHid; g.K = kHid;
     g.epilogue = kStoreF32; g.C = m->dH1; g.ldc = kHid;
     if ((s = launch_gemm(g, 1, st))) return s;
     relu_back_kernel<<<grid_for((long long)rows * kHid), 256, 0, st>>>(m->dH1, m->H1b, m->dZ1, m->dZ1b,
                                                                         (long long)rows * kHid);
     col_sum_kernel<<<(kHid + 127) / 128, 128, 0, st>>>(m->dZ1, m->b1.g, rows, kHid);
-    // dW1[out][in] = sum_b dZ1[b][out] Xb[b][in]: M = 256, N = 48, K = rows
-    g.A = m->dZ1b; g.sam = 1; g.sak = kHid;
-    g.B = m->Xb; g.sbn = 1; g.sbk = kInPad;
+    // dW1[out][in] = sum_b dZ1[b][out] Xb[b][in]: M = 256, N = 48, K = rows, on dZ1^T and Xb^T
+    if ((s = transpose(m->dZ1b, rows, kHid, kHid, m->dZ1T, m->ldT, st))) return s;
+    if ((s = transpose(m->Xb, rows, kInPad, kInPad, m->XbT, m->ldT, st))) return s;
+    g.A = m->dZ1T; g.lda = m->ldT;
+    g.B = m->XbT; g.ldb = m->ldT;
     g.M = kHid; g.N = kInPad; g.K = rows;
     g.ldc = kInPad;
     if ((s = gemm_split_sum(g, splits, m->parts, m->W1.g, st))) return s;
@@ -433,21 +510,22 @@ sidr_status sidr_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int3
     __nv_bfloat16 *dA = nullptr, *dB = nullptr;
     float* dC = nullptr;
     int* err = nullptr;
-    cudaError_t e = cudaMalloc(&dA, (size_t)M * K * 2);
-    if (!e) e = cudaMalloc(&dB, (size_t)N * K * 2);
+    const long long ld = pad8(K);  // rows padded to 16 bytes for the tensor maps
+    cudaError_t e = cudaMalloc(&dA, (size_t)M * ld * 2);
+    if (!e) e = cudaMalloc(&dB, (size_t)N * ld * 2);
     float* parts = nullptr;
     if (!e) e = cudaMalloc(&dC, (size_t)M * N * 4);
     if (!e && splits > 1) e = cudaMalloc(&parts, (size_t)kMaxSplits * M * N * 4);
     if (!e) e = cudaMalloc(&err, sizeof(int));
-    if (!e) e = cudaMemcpy(dA, A, (size_t)M * K * 2, cudaMemcpyHostToDevice);
-    if (!e) e = cudaMemcpy(dB, B, (size_t)N * K * 2, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy2D(dA, ld * 2, A, (size_t)K * 2, (size_t)K * 2, M, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy2D(dB, ld * 2, B, (size_t)K * 2, (size_t)K * 2, N, cudaMemcpyHostToDevice);
     if (!e) e = cudaMemset(dC, 0, (size_t)M * N * 4);
     if (!e) e = cudaMemset(err, 0, sizeof(int));
     sidr_status s = SIDR_OK;
     if (!e) {
         GemmArgs g{};
-        g.A = dA; g.sam = K; g.sak = 1;
-        g.B = dB; g.sbn = K; g.sbk = 1;
+        g.A = dA; g.lda = ld;
+        g.B = dB; g.ldb = ld;
         g.M = M; g.N = N; g.K = K;
         g.epilogue = kStoreF32;
         g.C = dC; g.ldc = N; g.error = err;
@@ -487,8 +565,8 @@ sidr_status sidr_gemm_wait_check(int device, uint32_t wait_limit) {
     sidr_status s = SIDR_OK;
     if (!e) {
         GemmArgs g{};
-        g.A = dA; g.sam = K; g.sak = 1;
-        g.B = dB; g.sbn = K; g.sbk = 1;
+        g.A = dA; g.lda = K;
+        g.B = dB; g.ldb = K;
         g.M = M; g.N = N; g.K = K;
         g.epilogue = kStoreF32;
         g.C = dC; g.ldc = N; g.error = err;
@@ -633,6 +711,7 @@ sidr_status sidr_mlp_create(int device, uint64_t seed, sidr_mlp** out) {
     if (!e) e = m->alloc(m->loss, 1);
     if (!e) e = m->alloc(m->err, 1);
     if (!e) e = m->alloc(m->parts, (size_t)kMaxSplits * kHid * kHid);
+    if (!e) e = m->alloc(m->W2T, (size_t)kHid * kHid);
     if (e) {
         delete m;
         return fail_s(SIDR_ERR_CUDA, std::string("surrogate create: ") + cudaGetErrorString(e));

@@ -101,6 +101,13 @@ def parse_args():
                     help="instead of one independent generation per GPU, run the benchmark GP with "
                          "every generation's rules sharded over the ranks (fitness all_gather, "
                          "strong scaling): W untimed generations, then K timed ones")
+    ap.add_argument("--large", action="store_true",
+                    help="also run the large combined run's driver (sidr_sgp_run_multi): 10 instances "
+                         "of 288 customers x 30 GP seeds x 4096 rules, surrogate screening 16384 "
+                         "offspring per seed-generation, for --large-generations generations of "
+                         "--large-S training scenarios")
+    ap.add_argument("--large-S", type=int, default=4)
+    ap.add_argument("--large-generations", type=int, default=2)
     ap.add_argument("--multi-rules", type=int, default=100)
     ap.add_argument("--multi-S", type=int, default=100)
     return ap.parse_args()
@@ -462,6 +469,8 @@ def run_ours(args, rank, world, local):
         line["sgp"] = sgp_leg(ctx, w, args)
     if args.campaign and rank == 0:
         line["campaign"] = campaign_leg()
+    if args.large and rank == 0:
+        line["large"] = large_leg(args)
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -546,6 +555,39 @@ def multi_leg(args, stream):
             "shapes_ms_on_sample": ms, "tuning_seconds": t_tune,
             "chosen_shape": list(sidr.Multi.SHAPES[chosen]), "host_prep_seconds": prep,
             "spot_check_pairs": pairs, "spot_check_mismatches": mism, "per_size_class": classes}
+
+
+def large_leg(args):
+    """The large combined run's driver (sidr_sgp_run_multi) at its full
+    population shape -- 10 instances of 288 customers (12-cluster and uniform
+    layouts, m = 4, H = 1000) x 30 GP seeds x 4096 rules, 16384 offspring
+    screened per seed-generation -- for a few generations with fewer training
+    scenarios than the benchmark's 2000.  Every generation simulates all
+    1.2 M rules of the populations in one multi-instance launch; the
+    evaluation time scales with the scenario count, the model and host time
+    do not."""
+    import sidr
+    from sidr import surrogate as SG
+    from sidr import workload as W
+    mw = W.large_combined(K=10, seeds=1, rules_per_seed=1, S=1)
+    zps = [sidr.zstats(sd) for sd in mw.sds]
+    G = args.large_generations
+    t0 = time.perf_counter()
+    r = SG.sgp_run_multi(mw.sds, zps, W.MENU29, mw.masks, 30, first_seed=0, test_seed=1000000,
+                         shape=-1, gp=dict(population=4096, generations=G,
+                                           train_samples=args.large_S, test_samples=500),
+                         screen=16384)
+    wall = time.perf_counter() - t0
+    pop_evals = 10 * 30 * 4096 * args.large_S
+    return {"workload": f"10 instances x 288 customers x 30 seeds x 4096 rules, {G} generations "
+                        f"of {args.large_S} training scenarios, screening 16384 per "
+                        f"seed-generation, held-out 500",
+            "wall_seconds": wall, "eval_seconds": r["eval_seconds"],
+            "model_seconds": r["model_seconds"], "host_seconds": r["host_seconds"],
+            "evaluations": r["evaluations"], "evals_per_s": r["evaluations"] / r["eval_seconds"],
+            "population_evaluations_per_generation": pop_evals,
+            "screened": r["screened"], "fallback": r["fallback"],
+            "best_held_out_mean": float(r["held_out"][-1].mean())}
 
 
 def campaign_leg():

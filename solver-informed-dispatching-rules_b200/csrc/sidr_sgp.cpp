@@ -385,7 +385,8 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
     }
     auto seed_of = [&](int e) { return (long long)(first_seed + e % S); };
 
-    // One multi-instance launch: rule sets[q] (owner q) on instance inst_of[q]
+    // One multi-instance launch: rule sets[q] of population q (its leaf labels
+    // are interned in that population's own vocabulary) on instance inst_of[q]
     // with the scenario block blocks[q] of Tn scenarios; per-rule means.
     auto simulate = [&](const std::vector<const std::vector<Rule>*>& sets, const std::vector<int>& inst_of,
                         const std::vector<std::vector<double>>& blocks, int Tn,
@@ -398,7 +399,7 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
         std::vector<int64_t> mk((size_t)Q * 61), offs(Q);
         for (int q = 0; q < Q; q++) {
             const int k = inst_of[q];
-            pack_rules(*sets[q], gps[0].vocab, pk);
+            pack_rules(*sets[q], gps[q].vocab, pk);
             owner.insert(owner.end(), sets[q]->size(), q);
             d[q] = insts[k];
             std::copy(zps + 10 * (size_t)k, zps + 10 * (size_t)k + 10, z.begin() + 10 * (size_t)q);
@@ -451,9 +452,11 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
     for (int e = 0; e < E; e++) inst_of_e[e] = e / S;
 
     std::vector<InstanceSurrogate> sur(K);
-    auto features_of = [&](int k, const std::vector<Rule>& rules, std::vector<float>& f) -> sidr_status {
+    // phenotypes of rules bred by population e, on its instance's situations
+    auto features_of = [&](int e, const std::vector<Rule>& rules, std::vector<float>& f) -> sidr_status {
+        const int k = e / S;
         Packed pk;
-        pack_rules(rules, gps[0].vocab, pk);
+        pack_rules(rules, gps[e].vocab, pk);
         sidr_rules_desc r = pk.desc();
         f.assign((size_t)r.P * NF, 0.0f);
         const double t0 = now_s();
@@ -527,7 +530,7 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
         }
         for (int e = 0; e < E; e++) {
             std::vector<float> f;
-            if ((st = features_of(e / S, gps[e].pop, f)) != SIDR_OK) return st;
+            if ((st = features_of(e, gps[e].pop, f)) != SIDR_OK) return st;
             sur[e / S].hist_x.push_back(std::move(f));
             sur[e / S].hist_t.push_back(fits[e]);
         }
@@ -561,7 +564,7 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
         for (int e = 0; e < E; e++) {
             const int k = e / S;
             cand[e] = gps[e].breed(fits[e], (size_t)sc->screen);
-            if ((st = features_of(k, cand[e], cf[e])) != SIDR_OK) return st;
+            if ((st = features_of(e, cand[e], cf[e])) != SIDR_OK) return st;
             pred[e].resize(cand[e].size());
             const double t0 = now_s();
             st = sidr_mlp_predict(sur[k].model, cf[e].data(), (int32_t)cand[e].size(), pred[e].data());

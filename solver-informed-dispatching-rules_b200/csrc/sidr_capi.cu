@@ -93,6 +93,7 @@ struct HostPrograms {
     std::vector<uint8_t> slots;
     std::vector<RuleMeta> meta;
     int rows = 1, prog_cap = 1, const_cap = 1;
+    bool rmod = false;  // some rule has rmod instructions: the launch needs the RMOD kernel
 };
 
 }  // namespace
@@ -116,6 +117,7 @@ struct sidr_batch {
     DevBatch b{};
     int P = 0, T = 0, G = 0, group_size = 1;
     bool counting = false;
+    bool rmod = false;  // the batch's rules use rmod
     int grid = 0, block = 0;
     size_t smem = 0;
     DevBuf prog, consts, slots, meta, sampled, out, counter, stats, error, fit;
@@ -192,6 +194,7 @@ sidr_status compile_all(const sidr_rules_desc* r, const int64_t* masks, int mask
         hp.consts.insert(hp.consts.end(), cr.consts.begin(), cr.consts.end());
         hp.slots.insert(hp.slots.end(), cr.slots.begin(), cr.slots.end());
         hp.rows = std::max(hp.rows, cr.K + cr.D);
+        hp.rmod = hp.rmod || (cr.need & kNeedRmod) != 0;
         hp.prog_cap = std::max(hp.prog_cap, (int)cr.prog.size());
         hp.const_cap = std::max(hp.const_cap, (int)cr.consts.size());
     }
@@ -249,6 +252,13 @@ sidr_status read_error_word(const int* dev_word, cudaStream_t st) {
 
 // Launch geometry for a program set: warps per block bounded by the shared
 // memory each warp's slice takes; one persistent grid over all SMs.
+// The single-instance kernel for a launch: counting instantiation or not, with
+// or without the rmod code (only batches that use rmod pay for it).
+const void* eval_kernel_fn(bool counting, bool rmod) {
+    if (counting) return rmod ? (const void*)eval_kernel<true, true> : (const void*)eval_kernel<true, false>;
+    return rmod ? (const void*)eval_kernel<false, true> : (const void*)eval_kernel<false, false>;
+}
+
 sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bool counting,
                         int& grid, int& block, size_t& smem) {
     const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
@@ -258,7 +268,7 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
     if (wpb < 1) wpb = 1;
     block = 32 * wpb;
     smem = slice * wpb;
-    const void* fn = counting ? (const void*)eval_kernel<true> : (const void*)eval_kernel<false>;
+    const void* fn = eval_kernel_fn(counting, hp.rmod);
     SIDR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SIDR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
@@ -268,15 +278,16 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
     return SIDR_OK;
 }
 
-sidr_status launch(sidr_ctx* c, const DevBatch& b, bool counting, int grid, int block, size_t smem,
-                   cudaStream_t st) {
+sidr_status launch(sidr_ctx* c, const DevBatch& b, bool counting, bool rmod, int grid, int block,
+                   size_t smem, cudaStream_t st) {
     SIDR_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), st));
     if (b.error) SIDR_CUDA(cudaMemsetAsync(b.error, 0, sizeof(int), st));
     if (counting && b.stats) SIDR_CUDA(cudaMemsetAsync(b.stats, 0, kStats * sizeof(unsigned long long), st));
     if ((long long)b.P * b.T == 0) return SIDR_OK;
-    if (counting) eval_kernel<true><<<grid, block, smem, st>>>(c->inst, b);
-    else eval_kernel<false><<<grid, block, smem, st>>>(c->inst, b);
-    SIDR_CUDA(cudaGetLastError());
+    DevInst inst = c->inst;
+    DevBatch bb = b;
+    void* args[] = {&inst, &bb};
+    SIDR_CUDA(cudaLaunchKernel(eval_kernel_fn(counting, rmod), dim3(grid), dim3(block), args, smem, st));
     g_launches.fetch_add(1);
     return SIDR_OK;
 }
@@ -369,7 +380,7 @@ sidr_status evaluate_common(sidr_ctx* c, const sidr_rules_desc* r, const double*
     size_t smem;
     s = plan_launch(c, hp, (long long)P * T, false, grid, block, smem);
     if (s) return s;
-    s = launch(c, b, false, grid, block, smem, st);
+    s = launch(c, b, false, hp.rmod, grid, block, smem, st);
     if (s) return s;
     SIDR_CUDA(cudaMemcpyAsync(out, c->out.p, (size_t)P * T * sizeof(double), cudaMemcpyDeviceToHost, st));
     return read_error_word(b.error, st);
@@ -761,6 +772,7 @@ sidr_status sidr_batch_create(sidr_ctx* c, const sidr_rules_desc* r, const doubl
     bt->T = T;
     bt->G = G;
     bt->group_size = group_size;
+    bt->rmod = hp.rmod;
     auto bail = [&](cudaError_t err, const char* what) {
         sidr_batch_destroy(bt);
         return fail(SIDR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
@@ -831,7 +843,7 @@ sidr_status sidr_batch_run(sidr_batch* bt, void* stream) {
     DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
     cudaStream_t st = (cudaStream_t)stream;  // 0 = the legacy default stream
-    sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->grid, bt->block, bt->smem, st);
+    sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->rmod, bt->grid, bt->block, bt->smem, st);
     if (s) return s;
     if (bt->P > 0) {
         fitness_kernel<<<(bt->P + 127) / 128, 128, 0, st>>>(bt->b.out, bt->P, bt->T,
@@ -874,7 +886,7 @@ sidr_status sidr_batch_guard_check(sidr_batch* bt) {
     b.prog_cap = 0;  // slices with room for no instruction and the minimum of rows
     b.rows = 0;
     cudaStream_t st = bt->ctx->stream;
-    sidr_status s = launch(bt->ctx, b, false, bt->grid, bt->block, bt->smem, st);
+    sidr_status s = launch(bt->ctx, b, false, bt->rmod, bt->grid, bt->block, bt->smem, st);
     if (s) return s;
     return read_error_word(b.error, st);
 }
@@ -1090,7 +1102,7 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
     size_t smem;
     s = plan_launch(&geo, hp, (long long)P * T, false, grid, block, smem);
     if (s) return s;
-    s = launch(&geo, b, false, grid, block, smem, st);
+    s = launch(&geo, b, false, hp.rmod, grid, block, smem, st);
     if (s) return s;
     SIDR_CUDA(cudaMemcpyAsync(out, base + at_out, (size_t)P * T * 8, cudaMemcpyDeviceToHost, st));
     s = read_error_word(b.error, st);  // waits for the call's work; launch() cleared the word
@@ -1110,11 +1122,11 @@ namespace {
 
 // The compiled block shapes of eval_multi_kernel: {warps per block, min blocks}.
 constexpr int kShapes[SIDR_MULTI_SHAPES][2] = {{4, 3}, {8, 2}, {2, 6}};
-const void* multi_kernel(int shape) {
+const void* multi_kernel(int shape, bool rmod) {
     switch (shape) {
-    case 0: return (const void*)eval_multi_kernel<4, 3>;
-    case 1: return (const void*)eval_multi_kernel<8, 2>;
-    default: return (const void*)eval_multi_kernel<2, 6>;
+    case 0: return rmod ? (const void*)eval_multi_kernel<4, 3, true> : (const void*)eval_multi_kernel<4, 3, false>;
+    case 1: return rmod ? (const void*)eval_multi_kernel<8, 2, true> : (const void*)eval_multi_kernel<8, 2, false>;
+    default: return rmod ? (const void*)eval_multi_kernel<2, 6, true> : (const void*)eval_multi_kernel<2, 6, false>;
     }
 }
 
@@ -1133,6 +1145,7 @@ struct sidr_multi {
     size_t smem[SIDR_MULTI_SHAPES] = {};
     std::string key;
     std::vector<int32_t> order;  // the longest-first work order (host copy)
+    bool rmod = false;           // some rule uses rmod: the RMOD kernels
     cudaStream_t gstream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -1166,7 +1179,7 @@ sidr_status multi_launch(sidr_multi* m, int shape, cudaStream_t st) {
     SIDR_CUDA(cudaMemsetAsync(m->b.counter, 0, sizeof(unsigned long long), st));
     SIDR_CUDA(cudaMemsetAsync(m->b.error, 0, sizeof(int), st));
     void* args[] = {&m->b};
-    SIDR_CUDA(cudaLaunchKernel(multi_kernel(shape), dim3(m->grid[shape]), dim3(m->block[shape]),
+    SIDR_CUDA(cudaLaunchKernel(multi_kernel(shape, m->rmod), dim3(m->grid[shape]), dim3(m->block[shape]),
                                args, m->smem[shape], st));
     g_launches.fetch_add(1);
     return SIDR_OK;
@@ -1234,6 +1247,7 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
     sidr_multi* m = new sidr_multi();
     m->device = device;
     m->K = K;
+    m->rmod = hp.rmod;
     m->P = r->P;
     m->T = T;
     auto bail = [&](cudaError_t err, const char* what) {
@@ -1318,8 +1332,8 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
     int nmax = 0;
     for (int k = 0; k < K; k++) nmax = std::max(nmax, hs[k].n);
     char kb[256];
-    std::snprintf(kb, sizeof kb, "K%d P%d T%d rows%d prog%d sm%d nmax%d|", K, r->P, T, hp.rows,
-                  hp.prog_cap, m->sm_count, nmax);
+    std::snprintf(kb, sizeof kb, "K%d P%d T%d rows%d prog%d sm%d nmax%d rmod%d|", K, r->P, T, hp.rows,
+                  hp.prog_cap, m->sm_count, nmax, (int)hp.rmod);
     m->key = kb;
     for (int k = 0; k < K; k++) m->key += std::to_string(hs[k].n) + ",";
     for (int sh = 0; sh < SIDR_MULTI_SHAPES; sh++) {
@@ -1330,11 +1344,11 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
             multi_free(m);
             return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
         }
-        if ((e = cudaFuncSetAttribute(multi_kernel(sh), cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if ((e = cudaFuncSetAttribute(multi_kernel(sh, m->rmod), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)m->smem[sh])) != cudaSuccess)
             return bail(e, "cudaFuncSetAttribute");
         int per_sm = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_kernel(sh), m->block[sh],
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_kernel(sh, m->rmod), m->block[sh],
                                                                m->smem[sh])) != cudaSuccess)
             return bail(e, "occupancy");
         const long long items = (long long)r->P * T;

@@ -424,6 +424,7 @@ std::string compile_rule(const int32_t* ops, const int32_t* args, int len, const
             const uint32_t dst = (uint32_t)(out.K + pos);
             if (pos + 1 > maxtemp) maxtemp = pos + 1;
             out.prog.push_back((uint32_t)o | (a << 3) | (b << 13) | (dst << 23));
+            if (o == 6) out.need |= kNeedRmod;
             st.push_back(dst);
         }
     }

@@ -101,6 +101,7 @@ enum NeedBits : uint32_t {
     kNeedFScore = 1u << 12,  // FEASCORE (51)
     kNeedNFeasRob = 1u << 13, // NFEASROB (52)
     kNeedExplore = 1u << 14, // slots computed by the direct per-lane path
+    kNeedRmod = 1u << 15,    // the program has rmod instructions (opcode 6)
     kNeedNSFused = kNeedNS | kNeedMaxN | kNeedReach2 | kNeedNSTW,
     kNeedRob = kNeedNSRob | kNeedReach2Rob,
     kNeedAfterC = kNeedStruct | kNeedPBust | kNeedReachK,

@@ -685,7 +685,7 @@ __device__ __forceinline__ AtRiskView at_risk_view(const DevInst& I, const WarpS
 // Terminals of candidate i into the lane's value rows, then the rule program.
 // Returns the priority (NaN mapped to -1e300).  eloss: the candidate's ATRISK
 // value (at_risk), when the rule reads it.
-template <bool COUNT>
+template <bool COUNT, bool RMOD>
 __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
                                   const Decision& d, int i, double eloss, WarpCounts& wc) {
     const int lane = threadIdx.x & 31;
@@ -995,13 +995,12 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         case 3: r = fabs(b) < 1e-10 ? 1.0 : a / b; break;
         case 4: r = a < b ? a : b; break;
         case 5: r = a > b ? a : b; break;
-        default: {  // rmod: glibc's pow restated (libm::pow_), so the result is the CPU's
-            const double base = a > 0.0 ? a : 0.0;
-            double e = b;
-            if (e < 0.0) e = 0.0;
-            else if (e > 1.0) e = 1.0;
-            r = libm::pow_(base, 1.0 + e);
-        }
+        default:
+            // rmod: glibc's pow restated, so the result is the CPU's.  Only the
+            // RMOD instantiation has this code; the others never see opcode 6
+            // (the host picks the kernel, the staging guard refuses such rules).
+            if constexpr (RMOD) r = libm::rmod_(a, b);
+            else r = 0.0;
         }
         S.rows[od * 32 + lane] = r;
     }
@@ -1021,7 +1020,7 @@ struct CaptureAt {
 // One decision: returns the chosen customer or -1 (pick_best).  CAPTURE:
 // every candidate's terminal rows (the first B.cap_k rows: the rule was
 // compiled with all active slots as rows) and the choice are recorded.
-template <bool COUNT, bool CAPTURE = false>
+template <bool COUNT, bool RMOD, bool CAPTURE = false>
 __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, Decision& d,
                       WarpCounts& wc, CaptureAt cap = CaptureAt{nullptr, -1}) {
     const int lane = threadIdx.x & 31;
@@ -1102,7 +1101,7 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         SIDR_SEC_ADD(10, t_atr);
         if (k < ncand) {
             idx = S.cand[k];
-            pri = score_candidate<COUNT>(I, S, rm, d, idx, eloss, wc);
+            pri = score_candidate<COUNT, RMOD>(I, S, rm, d, idx, eloss, wc);
             if (CAPTURE && cap.slot >= 0 && k < cap.C->cand) {
                 const CaptureBuf& C = *cap.C;
                 const size_t at = (size_t)cap.slot * C.cand + k;
@@ -1135,7 +1134,7 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
 
 // sim_one (engine/sim_core.hpp:207-238) for one pair; every lane returns the
 // same total.
-template <bool COUNT, bool CAPTURE = false>
+template <bool COUNT, bool RMOD, bool CAPTURE = false>
 __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
                           const double* smp, WarpCounts& wc, const CaptureBuf* capC = nullptr,
                           int scenario = 0) {
@@ -1159,9 +1158,9 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
             if constexpr (CAPTURE) {
                 CaptureAt cap{capC, dec_no < capC->dec ? scenario * capC->dec + dec_no : -1};
                 dec_no++;
-                b = decide<COUNT, true>(I, S, rm, d, wc, cap);
+                b = decide<COUNT, RMOD, true>(I, S, rm, d, wc, cap);
             } else {
-                b = decide<COUNT>(I, S, rm, d, wc);
+                b = decide<COUNT, RMOD>(I, S, rm, d, wc);
             }
             if (b < 0) break;
             SIDR_SEC_MARK(t_upd)
@@ -1180,20 +1179,22 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
 
 // Why a rule record cannot run in a warp slice carved for B (0 = it can):
 // program, constants and rows beyond the slice's capacities, a result operand
-// outside them, or (multi-instance batches) an instance outside the batch.
-__device__ __forceinline__ int rule_record_error(const RuleMeta& m, const DevBatch& B, bool multi) {
+// outside them, rmod instructions in a kernel built without them, or
+// (multi-instance batches) an instance outside the batch.
+__device__ __forceinline__ int rule_record_error(const RuleMeta& m, const DevBatch& B, bool multi,
+                                                 bool rmod) {
     const bool fits = m.n_ins >= 0 && m.n_ins <= B.prog_cap && m.n_const >= 0 &&
                       m.n_const <= B.const_cap && m.K >= 0 && m.K <= 64 && m.D >= 0 &&
                       m.K + m.D <= B.rows && m.res >= 0 &&
                       ((m.res & kOpConst) ? (m.res & 511) < m.n_const : m.res < m.K + m.D);
-    if (!fits) return kErrRuleRecord;
+    if (!fits || (!rmod && (m.need & kNeedRmod))) return kErrRuleRecord;
     if (multi && (m.inst < 0 || m.inst >= B.n_inst)) return kErrInstance;
     return 0;
 }
 
 // The persistent work loop.  MULTI: every rule carries its instance; the
 // warp stages the instance descriptor with the rule's program.
-template <bool COUNT, bool MULTI, bool CAPTURE = false>
+template <bool COUNT, bool MULTI, bool RMOD, bool CAPTURE = false>
 __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
                                           const CaptureBuf* capC = nullptr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1220,7 +1221,7 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
             // was not sized for is refused (error word set, score NaN) before
             // anything of it is staged.  Host validation makes this unreachable;
             // the host reads the word back after every launch.
-            const int code = (p < 0 || p >= B.P) ? kErrRuleIndex : rule_record_error(B.meta[p], B, MULTI);
+            const int code = (p < 0 || p >= B.P) ? kErrRuleIndex : rule_record_error(B.meta[p], B, MULTI, RMOD);
             if (code) {
                 if (lane == 0) {
                     atomicCAS(B.error, 0, code);
@@ -1248,8 +1249,8 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
             MULTI ? B.sampled + B.smp_off[rm.inst] + (size_t)s * I.n
                   : B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
         double tot;
-        if constexpr (CAPTURE) tot = rollout<COUNT, true>(I, S, rm, smp, wc, capC, s);
-        else tot = rollout<COUNT>(I, S, rm, smp, wc);
+        if constexpr (CAPTURE) tot = rollout<COUNT, RMOD, true>(I, S, rm, smp, wc, capC, s);
+        else tot = rollout<COUNT, RMOD>(I, S, rm, smp, wc);
         if (lane == 0) B.out[(size_t)p * B.T + s] = tot;
     }
     if (COUNT) {
@@ -1267,24 +1268,26 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
 }
 
 // Single-instance evaluator (the instance travels as a kernel parameter).
-template <bool COUNT>
+// RMOD: the batch has rules with rmod; the kernels without it carry no code
+// for the power function, which would cost the others several percent.
+template <bool COUNT, bool RMOD>
 __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
     eval_kernel(const DevInst I, const DevBatch B) {
-    eval_body<COUNT, false>(I, B);
+    eval_body<COUNT, false, RMOD>(I, B);
 }
 
 // Decision-situation capture: one rule on B.T scenarios, every decision's
 // candidate terminal tables recorded (DevBatch cap_* fields).
 __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
     capture_kernel(const DevInst I, const DevBatch B, const CaptureBuf C) {
-    eval_body<false, false, true>(I, B, &C);
+    eval_body<false, false, true, true>(I, B, &C);
 }
 
 // Multi-instance evaluator, one instantiation per block shape (warps per
 // block x minimum resident blocks); the autotuner picks among them.
-template <int WPB, int MINB>
+template <int WPB, int MINB, bool RMOD>
 __global__ void __launch_bounds__(32 * WPB, MINB) eval_multi_kernel(const DevBatch B) {
-    eval_body<false, true>(DevInst{}, B);
+    eval_body<false, true, RMOD>(DevInst{}, B);
 }
 
 }  // namespace sidr

@@ -316,6 +316,31 @@ SIDR_HD_CALL double pow_(double x, double y) {
     return exp_tail_(ehi, elo, sign_bias);
 }
 
+// rmod's operation (engine/sim_core.hpp:30-35): pow(max(a, 0), 1 + clip(b, 0, 1)).
+// On that domain (x >= +0, y in [1, 2] or NaN) glibc's pow reduces to: NaN y
+// gives x + y (1 for x == 1), +0 and +inf give x * x, a subnormal x is
+// normalised, and the rest is the main path of pow_ above; the branches for
+// negative bases and for tiny or huge exponents are left out.
+SIDR_HD_CALL double rmod_(double a, double b) {
+    const double x = a > 0.0 ? a : 0.0;
+    double e = b;
+    if (e < 0.0) e = 0.0;
+    else if (e > 1.0) e = 1.0;
+    const double y = 1.0 + e;
+    if (y != y) return x == 1.0 ? 1.0 : x + y;
+    uint64_t ix = bits_of(x);
+    if (x == 0.0 || ix >= 0x7ff0000000000000ull) return x * x;  // +0 and +inf
+    if (ix < 0x0010000000000000ull) {  // subnormal: the exponent becomes negative
+        ix = bits_of(x * 0x1p52) & 0x7fffffffffffffffull;
+        ix -= 52ull << 52;
+    }
+    double lo;
+    const double hi = log_tail_(ix, &lo);
+    const double ehi = y * hi;
+    const double elo = fused(y, lo, fused(y, hi, -ehi));
+    return exp_tail_(ehi, elo, 0);
+}
+
 // ------------------------------------------------------------- erf, erfc
 
 // fdlibm's coefficients.

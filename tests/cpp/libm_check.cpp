@@ -125,5 +125,32 @@ int main(int argc, char** argv) {
         std::printf("pow specials - %ld %ld\n", bad, cnt);
         bad_total += bad != 0;
     }
+    {  // rmod_ (a, b) -> pow(max(a, 0), 1 + clip(b, 0, 1)) on every kind of operand
+        long bad = 0;
+        const double special[] = {0.0, -0.0, 1.0, -1.0, 0.5, 2.0, 5e-324, 1e-310, 1e308, INFINITY,
+                                  -INFINITY, NAN, -NAN, 1.5, 3.0};
+        auto check = [&](double a, double b) {
+            const double x = a > 0.0 ? a : 0.0;
+            const double e = b < 0.0 ? 0.0 : (b > 1.0 ? 1.0 : b);
+            // a volatile exponent: where the clamp gives 2, the compiler would otherwise
+            // fold pow(x, 2.0) into x * x, which is not what the C library returns
+            volatile double y = 1.0 + e;
+            const double want = std::pow(x, (double)y), got = sidr::libm::rmod_(a, b);
+            if (bits(got) != bits(want) && !(got != got && want != want)) {
+                if (bad < 2) std::printf("# rmod(%a, %a): ours %a libc %a\n", a, b, got, want);
+                bad++;
+            }
+        };
+        for (double a : special)
+            for (double b : special) check(a, b);
+        for (long k = 0; k < n; k++) {
+            const double mag = std::exp2(uniform(-1074.0, 1023.9));
+            const double a = (next_u64() & 3) == 0 ? -mag : mag;
+            const double b = uniform(-0.5, 1.5);
+            check(a, b);
+        }
+        std::printf("rmod all - %ld %ld\n", bad, n);
+        bad_total += bad != 0;
+    }
     return bad_total ? 1 : 0;
 }

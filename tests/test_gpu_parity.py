@@ -303,3 +303,17 @@ def test_rmod_heavy_rules_match_oracle(oracle):
     out = ctx.evaluate(rules, w.sampled, w.S, mask)
     ctx.close()
     assert_bitexact(out, oracle.eval_pairs(w.sd, zp, rules, w.sampled, w.S, mask), "rmod rules")
+
+
+def test_rmod_last_bit_rules_match_oracle(oracle):
+    """Rules in which the last bit of pow(x, 2.0) decides the route (rmod with
+    the regime clipped to 1, minus x * x): the restated pow gives the CPU
+    simulator's routes."""
+    w = workload.gp_generation(P=1, S=300)
+    mask = R.term_mask_from(workload.MENU29 + ["ERC"])
+    rules = R.pack([f"(- (rmod {t} 1.5) (* {t} {t}))" for t in ("NSTW", "TFV", "BOLSAO", "HARVEST")])
+    zp = sidr.zstats(w.sd)
+    ctx = sidr.Context(w.sd, zp)
+    out = ctx.evaluate(rules, w.sampled, w.S, mask)
+    ctx.close()
+    assert_bitexact(out, oracle.eval_pairs(w.sd, zp, rules, w.sampled, w.S, mask), "rmod last bit")

@@ -23,7 +23,7 @@ def test_host_build_matches_libc(tmp_path):
                    check=True)
     r = subprocess.run([str(exe), "200000", "3"], capture_output=True, text=True)
     rows = [ln.split() for ln in r.stdout.splitlines() if not ln.startswith("#")]
-    assert len(rows) == 27 + 8  # 27 erf/erfc/exp intervals, 7 pow families, pow specials
+    assert len(rows) == 27 + 8 + 1  # erf/erfc/exp intervals, 7 pow families, pow specials, rmod
     bad = [row for row in rows if row[3] != "0"]
     assert not bad and r.returncode == 0, r.stdout
 

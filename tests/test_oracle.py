@@ -9,6 +9,7 @@ import pytest
 from conftest import GOLDEN
 
 from sidr.instance import SimData
+from sidr import rules as R
 from sidr.rules import EXTRA, NS_TERMINALS, PackedRules, pack_compiled, term_mask_from
 
 
@@ -136,3 +137,22 @@ def test_rng_matches_reference_golden_stream(reference_tree):
             want = struct.unpack("<d", struct.pack("<Q", int(p[1], 16)))[0]
             assert rng.gauss(5.0, 1.5) == want
     assert checked > 1000
+
+
+def test_reference_rmod_calls_pow_at_run_time(reference, oracle):
+    """rmod with the regime clipped to 1 is pow(x, 2.0), which a compiler may
+    fold into x * x; the C library's pow differs from x * x in the last bit for
+    a few arguments.  Rules that subtract x * x from rmod(x, 1.5) make that bit
+    decide: the reference's compiled simulator scores them differently from an
+    all-zero priority (so it calls pow at run time, as the evaluator's restated
+    pow does), and the oracle gives the reference's scores bit for bit."""
+    from sidr import workload
+    w = workload.gp_generation(P=1, S=300)
+    mask = R.term_mask_from(workload.MENU29 + ["ERC"])
+    terms = ["NSTW", "TFV", "BOLSAO"]
+    rules = R.pack([f"(- (rmod {t} 1.5) (* {t} {t}))" for t in terms] +
+                   [f"(- (* {t} {t}) (* {t} {t}))" for t in terms])
+    ref = reference.eval_pairs(w.sd, reference.zp_of(w.sd), rules, w.sampled, 300, mask)
+    ora = oracle.eval_pairs(w.sd, oracle.zstats(w.sd), rules, w.sampled, 300, mask)
+    assert np.array_equal(ref.view(np.uint64), ora.view(np.uint64))
+    assert all(not np.array_equal(ref[k], ref[k + 3]) for k in range(3))

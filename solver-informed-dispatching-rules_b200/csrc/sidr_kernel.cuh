@@ -471,12 +471,26 @@ struct AtRiskClass {
     double bnum, bden;
 };
 
-__device__ __forceinline__ AtRiskClass at_risk_class(const AtRiskView& v, int j, bool live,
-                                                     double hw, double lw) {
+// The four 16-byte loads of pair (candidate, j): {dist(c, j), P1(c, j)} and
+// the customer's {close, open}, {P0, dur}, {d2d, score}.
+struct AtRiskLoad {
+    double2 dp, co, pd, es;
+};
+
+__device__ __forceinline__ AtRiskLoad at_risk_load(const AtRiskView& v, int j, bool live) {
     const int js = live ? j : 0;
-    const double2 dp = v.DPc[(size_t)js * v.n];
     const double2* cu = v.CU + 3 * (size_t)js;
-    const double2 co = cu[0], pd = cu[1], es = cu[2];
+    AtRiskLoad L;
+    L.dp = v.DPc[(size_t)js * v.n];
+    L.co = cu[0];
+    L.pd = cu[1];
+    L.es = cu[2];
+    return L;
+}
+
+__device__ __forceinline__ AtRiskClass at_risk_compute(const AtRiskView& v, const AtRiskLoad& L,
+                                                       bool live, double hw, double lw) {
+    const double2 dp = L.dp, co = L.co, pd = L.pd, es = L.es;
     const double cj = co.x, oj = co.y, p0 = pd.x, dj = pd.y, ej = es.x;
     const double marr = v.fin_c + dp.x;
     const double dw = cj - marr;
@@ -502,11 +516,14 @@ __device__ __forceinline__ AtRiskClass at_risk_class(const AtRiskView& v, int j,
     return c;
 }
 
+__device__ __forceinline__ AtRiskClass at_risk_class(const AtRiskView& v, int j, bool live,
+                                                     double hw, double lw) {
+    return at_risk_compute(v, at_risk_load(v, j, live), live, hw, lw);
+}
+
 __device__ __forceinline__ double norm_cdf_ratio(double num, double den) {
     return 0.5 * (1.0 + libm::erf_((num / den) * 0.7071067811865476));
 }
-
-constexpr int kAtRiskUnroll = 2;
 
 // ATRISK (t_eloss_chance, engine/sim_terms.hpp:225-257) of each lane's
 // candidate v.ci (-1: the lane has none), called by the whole warp at the
@@ -515,8 +532,8 @@ constexpr int kAtRiskUnroll = 2;
 // ascending j; that set (S.atr) is the decision's, so every lane walks the
 // same list, the per-customer loads are broadcasts and the lanes' pair loads
 // fall in one row of DP.  The list is taken 32 customers (one word) at a
-// time.  Pass 1 classifies the word's pairs, kAtRiskUnroll independent ones
-// per step, into per-lane bit masks, and queues the (numerator,
+// time.  Pass 1 classifies the word's pairs, one per step with the next
+// pair's loads already issued, into per-lane bit masks, and queues the (numerator,
 // denominator) of every erf argument warp-wide in the value rows; the warp
 // evaluates the queue 32 entries at a time; pass 2 adds the terms in order
 // from the masks, the word's scores (one per lane, shuffled) and the queue
@@ -550,7 +567,6 @@ __device__ __noinline__ double at_risk_word_direct(const AtRiskView v, int w, ui
 
 template <bool COUNT>
 __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
-    constexpr int U = kAtRiskUnroll;
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     const double hw = 8.5 * v.sd_c, lw = -8.5 * v.sd_c;
@@ -568,42 +584,42 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
         SIDR_SEC_MARK(t_p1)
         uint32_t addm = 0, ewm = 0, ebm = 0, pbm = 0;
         int qn = 0;
-        for (uint32_t bits = word; bits;) {
-            int b[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                b[u] = bits ? __ffs(bits) - 1 : -1;
-                bits &= bits - 1;
+        // one pair per step, the next pair's loads issued before this one's
+        // classification
+        int bc = __ffs(word) - 1;
+        uint32_t bits = word & (word - 1);
+        bool lc = has && !((own >> bc) & 1u);
+        AtRiskLoad Lc = at_risk_load(v, (w << 5) + bc, lc);
+        for (;;) {
+            const bool more = bits != 0;  // warp-uniform
+            const int bn = more ? __ffs(bits) - 1 : bc;
+            bits &= bits - 1;
+            const bool ln = has && !((own >> bn) & 1u);
+            const AtRiskLoad Ln = at_risk_load(v, (w << 5) + bn, ln);
+            const AtRiskClass c = at_risk_compute(v, Lc, lc, hw, lw);
+            const uint32_t m = 1u << bc;
+            addm |= c.add ? m : 0u;
+            ewm |= c.ew ? m : 0u;
+            ebm |= c.eb ? m : 0u;
+            pbm |= c.pb1 ? m : 0u;
+            const uint32_t bw = __ballot_sync(kFull, c.ew);
+            const uint32_t bb = __ballot_sync(kFull, c.eb);
+            const int pw = qn + __popc(bw & lt);
+            qn += __popc(bw);
+            const int pb = qn + __popc(bb & lt);
+            qn += __popc(bb);
+            if (c.ew && pw < v.cap) {
+                Q[2 * pw] = c.wnum;
+                Q[2 * pw + 1] = v.sd_c;
             }
-            AtRiskClass c[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const bool live = has && b[u] >= 0 && !((own >> (b[u] & 31)) & 1u);
-                c[u] = at_risk_class(v, (w << 5) + b[u], live, hw, lw);
+            if (c.eb && pb < v.cap) {
+                Q[2 * pb] = c.bnum;
+                Q[2 * pb + 1] = c.bden;
             }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                if (b[u] < 0) break;  // warp-uniform
-                const uint32_t m = 1u << b[u];
-                addm |= c[u].add ? m : 0u;
-                ewm |= c[u].ew ? m : 0u;
-                ebm |= c[u].eb ? m : 0u;
-                pbm |= c[u].pb1 ? m : 0u;
-                const uint32_t bw = __ballot_sync(kFull, c[u].ew);
-                const uint32_t bb = __ballot_sync(kFull, c[u].eb);
-                const int pw = qn + __popc(bw & lt);
-                qn += __popc(bw);
-                const int pb = qn + __popc(bb & lt);
-                qn += __popc(bb);
-                if (c[u].ew && pw < v.cap) {
-                    Q[2 * pw] = c[u].wnum;
-                    Q[2 * pw + 1] = v.sd_c;
-                }
-                if (c[u].eb && pb < v.cap) {
-                    Q[2 * pb] = c[u].bnum;
-                    Q[2 * pb + 1] = c[u].bden;
-                }
-            }
+            if (!more) break;
+            bc = bn;
+            lc = ln;
+            Lc = Ln;
         }
         SIDR_SEC_ADD(11, t_p1);
         if (qn > v.cap) {  // warp-uniform

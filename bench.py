@@ -336,6 +336,10 @@ def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, wor
     torch.cuda.synchronize()
     counts = batch.counts()
     batch.set_counting(False)
+    # block shape timed on every 16th rule (untimed); the same shape for the
+    # device-timed steps and the end-to-end calls
+    shape, shape_ms = batch.autotune_sampled(stride=16, reps=1)
+    ctx.set_shape(shape)
     for _ in range(warmup):
         flush.zero_()
         batch.run(sh)
@@ -394,9 +398,13 @@ def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, wor
         hbm = {"achieved": traffic / avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                "frac": traffic / avg_s / 1e9 / hbm_peak, "peak_source": hbm_src,
                "traffic_bytes_per_launch": traffic}
+    ctx.set_shape(0)
     return {"value": value, "total_ms": total_ms, "e2e": e2e, "launches": launches,
             "roofline": roofline, "hbm": hbm, "clocks": clk, "counts": counts,
-            "repeat_runs_identical": same, "out": ref_out}
+            "repeat_runs_identical": same, "out": ref_out,
+            "block_shape": {"warps_per_block": sidr.Batch.SHAPES[shape][0],
+                            "blocks_per_sm": sidr.Batch.SHAPES[shape][1],
+                            "ms_on_sample": shape_ms, "sample": "every 16th rule, all scenarios"}}
 
 
 def run_ours(args, rank, world, local):
@@ -439,7 +447,7 @@ def run_ours(args, rank, world, local):
             "data": "synthetic", "config": config_of(args.P, args.S, world),
             "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"],
             "hbm": r["hbm"], "clocks": r["clocks"], "counts": r["counts"],
-            "repeat_runs_identical": r["repeat_runs_identical"]}
+            "block_shape": r["block_shape"], "repeat_runs_identical": r["repeat_runs_identical"]}
     if args.evolved_steps > 0:
         # the same instance and scenarios with generation 49 of the benchmark GP run: the
         # populations a GP spends 49 of its 50 generations on
@@ -453,6 +461,7 @@ def run_ours(args, rank, world, local):
                            "unit": UNIT, "steps": args.evolved_steps, "warmup": 3,
                            "ms_per_step": re["total_ms"] / args.evolved_steps, "e2e": re["e2e"],
                            "roofline": re["roofline"], "counts": re["counts"],
+                           "block_shape": re["block_shape"],
                            "repeat_runs_identical": re["repeat_runs_identical"]}
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             # a bounded sample: the evolved rules cost the CPU simulator about 3x more per pair

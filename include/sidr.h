@@ -148,6 +148,23 @@ typedef struct sidr_counts {
 sidr_status sidr_batch_set_counting(sidr_batch* b, int enable);
 sidr_status sidr_batch_counts(sidr_batch* b, sidr_counts* out);
 
+/* Block shape of a batch's launches (no reference counterpart).  Shape 0 (the
+ * default) budgets 128 registers per thread for 4 resident blocks of 4 warps
+ * per SM; shape 1 budgets 96 for 5, which hides more latency at the price of
+ * spills and pays on rules that spend their time in ATRISK.  Both give the
+ * same scores.  sidr_batch_autotune_sampled times each shape on every
+ * stride-th rule of the batch (all its scenarios; the first of reps + 1 runs
+ * warms up), keeps the faster for sidr_batch_run and reports it in *chosen and
+ * the times in ms[SIDR_BATCH_SHAPES] (either may be null).  The sampled rules'
+ * scores are overwritten; run the batch afterwards.  The counting launch
+ * always uses shape 0. */
+#define SIDR_BATCH_SHAPES 2
+sidr_status sidr_batch_set_shape(sidr_batch* b, int32_t shape);
+/* The block shape of a context's sidr_evaluate* calls (default 0). */
+sidr_status sidr_ctx_set_shape(sidr_ctx* ctx, int32_t shape);
+sidr_status sidr_batch_autotune_sampled(sidr_batch* b, int32_t reps, int32_t stride,
+                                        int32_t* chosen, float* ms);
+
 /* Multi-instance batches (no reference counterpart; the reference evaluates
  * one instance per FactoryContext).  K instances of uneven size, each with its
  * own rules, scenarios and mask, evaluated together in ONE persistent launch:

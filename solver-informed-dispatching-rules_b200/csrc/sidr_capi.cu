@@ -108,6 +108,7 @@ struct sidr_ctx {
     DevInst inst{};
     std::vector<void*> owned;  // instance arrays and tables
     cudaStream_t stream = nullptr;
+    int shape = 0;  // block shape of the reference-shaped evaluate* calls (sidr_ctx_set_shape)
     // grow-only scratch of the reference-shaped evaluate* calls
     DevBuf prog, consts, slots, meta, sampled, out, counter, stats, error;
 };
@@ -118,8 +119,11 @@ struct sidr_batch {
     int P = 0, T = 0, G = 0, group_size = 1;
     bool counting = false;
     bool rmod = false;  // the batch's rules use rmod
-    int grid = 0, block = 0;
+    int grid = 0, block = 0;  // the launch of shape 0 (also the counting launch's)
     size_t smem = 0;
+    int shape = 0;                               // eval_kernel_fn's shape for sidr_batch_run
+    int grid_s[2] = {}, block_s[2] = {};         // the launch of each shape
+    size_t smem_s[2] = {};
     DevBuf prog, consts, slots, meta, sampled, out, counter, stats, error, fit;
     bool ran = false;
 };
@@ -254,13 +258,21 @@ sidr_status read_error_word(const int* dev_word, cudaStream_t st) {
 // memory each warp's slice takes; one persistent grid over all SMs.
 // The single-instance kernel for a launch: counting instantiation or not, with
 // or without the rmod code (only batches that use rmod pay for it).
-const void* eval_kernel_fn(bool counting, bool rmod) {
-    if (counting) return rmod ? (const void*)eval_kernel<true, true> : (const void*)eval_kernel<true, false>;
-    return rmod ? (const void*)eval_kernel<false, true> : (const void*)eval_kernel<false, false>;
+// shape: 0 = SIDR_MIN_BLOCKS resident blocks per SM, 1 = kMoreBlocks (the
+// counting instantiation exists for shape 0 only).
+const void* eval_kernel_fn(bool counting, bool rmod, int shape = 0) {
+    if (counting)
+        return rmod ? (const void*)eval_kernel<true, true, SIDR_MIN_BLOCKS>
+                    : (const void*)eval_kernel<true, false, SIDR_MIN_BLOCKS>;
+    if (shape == 1)
+        return rmod ? (const void*)eval_kernel<false, true, kMoreBlocks>
+                    : (const void*)eval_kernel<false, false, kMoreBlocks>;
+    return rmod ? (const void*)eval_kernel<false, true, SIDR_MIN_BLOCKS>
+                : (const void*)eval_kernel<false, false, SIDR_MIN_BLOCKS>;
 }
 
 sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bool counting,
-                        int& grid, int& block, size_t& smem) {
+                        int& grid, int& block, size_t& smem, int shape = 0) {
     const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
     if (slice > c->smem_optin)
         return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
@@ -268,7 +280,7 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
     if (wpb < 1) wpb = 1;
     block = 32 * wpb;
     smem = slice * wpb;
-    const void* fn = eval_kernel_fn(counting, hp.rmod);
+    const void* fn = eval_kernel_fn(counting, hp.rmod, shape);
     SIDR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SIDR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
@@ -279,7 +291,7 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
 }
 
 sidr_status launch(sidr_ctx* c, const DevBatch& b, bool counting, bool rmod, int grid, int block,
-                   size_t smem, cudaStream_t st) {
+                   size_t smem, cudaStream_t st, int shape = 0) {
     SIDR_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), st));
     if (b.error) SIDR_CUDA(cudaMemsetAsync(b.error, 0, sizeof(int), st));
     if (counting && b.stats) SIDR_CUDA(cudaMemsetAsync(b.stats, 0, kStats * sizeof(unsigned long long), st));
@@ -287,7 +299,8 @@ sidr_status launch(sidr_ctx* c, const DevBatch& b, bool counting, bool rmod, int
     DevInst inst = c->inst;
     DevBatch bb = b;
     void* args[] = {&inst, &bb};
-    SIDR_CUDA(cudaLaunchKernel(eval_kernel_fn(counting, rmod), dim3(grid), dim3(block), args, smem, st));
+    SIDR_CUDA(cudaLaunchKernel(eval_kernel_fn(counting, rmod, counting ? 0 : shape), dim3(grid),
+                               dim3(block), args, smem, st));
     g_launches.fetch_add(1);
     return SIDR_OK;
 }
@@ -378,9 +391,9 @@ sidr_status evaluate_common(sidr_ctx* c, const sidr_rules_desc* r, const double*
     b.const_cap = hp.const_cap;
     int grid, block;
     size_t smem;
-    s = plan_launch(c, hp, (long long)P * T, false, grid, block, smem);
+    s = plan_launch(c, hp, (long long)P * T, false, grid, block, smem, c->shape);
     if (s) return s;
-    s = launch(c, b, false, hp.rmod, grid, block, smem, st);
+    s = launch(c, b, false, hp.rmod, grid, block, smem, st, c->shape);
     if (s) return s;
     SIDR_CUDA(cudaMemcpyAsync(out, c->out.p, (size_t)P * T * sizeof(double), cudaMemcpyDeviceToHost, st));
     return read_error_word(b.error, st);
@@ -816,10 +829,14 @@ sidr_status sidr_batch_create(sidr_ctx* c, const sidr_rules_desc* r, const doubl
     b.prog_cap = hp.prog_cap;
     b.const_cap = hp.const_cap;
     s = plan_launch(c, hp, (long long)P * T, false, bt->grid, bt->block, bt->smem);
+    if (!s) s = plan_launch(c, hp, (long long)P * T, false, bt->grid_s[1], bt->block_s[1], bt->smem_s[1], 1);
     if (s) {
         sidr_batch_destroy(bt);
         return s;
     }
+    bt->grid_s[0] = bt->grid;
+    bt->block_s[0] = bt->block;
+    bt->smem_s[0] = bt->smem;
     int g2, b2;
     size_t s2;
     s = plan_launch(c, hp, (long long)P * T, true, g2, b2, s2);
@@ -843,7 +860,9 @@ sidr_status sidr_batch_run(sidr_batch* bt, void* stream) {
     DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(bt->ctx->device));
     cudaStream_t st = (cudaStream_t)stream;  // 0 = the legacy default stream
-    sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->rmod, bt->grid, bt->block, bt->smem, st);
+    const int sh = bt->counting ? 0 : bt->shape;
+    sidr_status s = launch(bt->ctx, bt->b, bt->counting, bt->rmod, bt->grid_s[sh], bt->block_s[sh],
+                           bt->smem_s[sh], st, sh);
     if (s) return s;
     if (bt->P > 0) {
         fitness_kernel<<<(bt->P + 127) / 128, 128, 0, st>>>(bt->b.out, bt->P, bt->T,
@@ -852,6 +871,75 @@ sidr_status sidr_batch_run(sidr_batch* bt, void* stream) {
         g_launches.fetch_add(1);
     }
     bt->ran = true;
+    return SIDR_OK;
+}
+
+sidr_status sidr_ctx_set_shape(sidr_ctx* c, int32_t shape) {
+    if (!c) return fail(SIDR_ERR_INVALID, "context is null");
+    if (shape < 0 || shape >= SIDR_BATCH_SHAPES) return fail(SIDR_ERR_INVALID, "shape out of range");
+    c->shape = shape;
+    return SIDR_OK;
+}
+
+sidr_status sidr_batch_set_shape(sidr_batch* bt, int32_t shape) {
+    if (!bt) return fail(SIDR_ERR_INVALID, "batch is null");
+    if (shape < 0 || shape >= SIDR_BATCH_SHAPES) return fail(SIDR_ERR_INVALID, "shape out of range");
+    bt->shape = shape;
+    return SIDR_OK;
+}
+
+sidr_status sidr_batch_autotune_sampled(sidr_batch* bt, int32_t reps, int32_t stride, int32_t* chosen,
+                                        float* ms) {
+    if (!bt || stride < 1) return fail(SIDR_ERR_INVALID, "null batch or stride < 1");
+    DeviceGuard device_guard;
+    SIDR_CUDA(cudaSetDevice(bt->ctx->device));
+    if ((long long)bt->P * bt->T == 0) {
+        if (chosen) *chosen = bt->shape;
+        return SIDR_OK;
+    }
+    // every stride-th rule: the sample keeps the batch's mix of rule costs
+    std::vector<int32_t> sample;
+    for (int p = 0; p < bt->P; p += stride) sample.push_back(p);
+    int32_t* d_order = nullptr;
+    SIDR_CUDA(cudaMalloc(&d_order, sample.size() * sizeof(int32_t)));
+    cudaStream_t st = bt->ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(d_order, sample.data(), sample.size() * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, st);
+    DevBatch b = bt->b;
+    b.order = d_order;
+    b.P_items = (int)sample.size();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!e) e = cudaEventCreate(&e0);
+    if (!e) e = cudaEventCreate(&e1);
+    float best = 1e30f;
+    int best_sh = 0;
+    sidr_status s = SIDR_OK;
+    for (int sh = 0; sh < SIDR_BATCH_SHAPES && !e && !s; sh++) {
+        float t_best = 1e30f;
+        for (int k = 0; k < (reps < 1 ? 1 : reps) + 1 && !e && !s; k++) {  // the first run warms up
+            e = cudaEventRecord(e0, st);
+            if (!e) s = launch(bt->ctx, b, false, bt->rmod, bt->grid_s[sh], bt->block_s[sh], bt->smem_s[sh], st, sh);
+            if (!e && !s) e = cudaEventRecord(e1, st);
+            if (!e && !s) e = cudaEventSynchronize(e1);
+            float t = 0.f;
+            if (!e && !s) e = cudaEventElapsedTime(&t, e0, e1);
+            if (k > 0 && t < t_best) t_best = t;
+        }
+        if (ms) ms[sh] = t_best;
+        if (t_best < best) {
+            best = t_best;
+            best_sh = sh;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    cudaFree(d_order);
+    if (s) return s;
+    if (e) return fail(SIDR_ERR_CUDA, std::string("batch autotune: ") + cudaGetErrorString(e));
+    if ((s = read_error_word(b.error, st))) return s;
+    bt->shape = best_sh;
+    if (chosen) *chosen = best_sh;
     return SIDR_OK;
 }
 

@@ -1291,8 +1291,14 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
 // Single-instance evaluator (the instance travels as a kernel parameter).
 // RMOD: the batch has rules with rmod; the kernels without it carry no code
 // for the power function, which would cost the others several percent.
-template <bool COUNT, bool RMOD>
-__global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
+// MINB: resident blocks per SM the registers are budgeted for --
+// SIDR_MIN_BLOCKS (4: 128 registers) by default, or kMoreBlocks (5: 96
+// registers, more warps to hide latency, more spills), which pays on
+// populations that spend their time in ATRISK's long classification loops.
+constexpr int kMoreBlocks = 5;
+
+template <bool COUNT, bool RMOD, int MINB>
+__global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, MINB)
     eval_kernel(const DevInst I, const DevBatch B) {
     eval_body<COUNT, false, RMOD>(I, B);
 }

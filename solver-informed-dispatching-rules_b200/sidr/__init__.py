@@ -67,6 +67,7 @@ EXPORTS = [
     "sidr_evaluate_static", "sidr_multi_create", "sidr_multi_autotune", "sidr_multi_set_shape",
     "sidr_multi_capture", "sidr_multi_run", "sidr_multi_read", "sidr_multi_destroy",
     "sidr_libm_eval", "sidr_batch_guard_check", "sidr_libm_pow", "sidr_multi_autotune_sampled",
+    "sidr_batch_set_shape", "sidr_batch_autotune_sampled", "sidr_ctx_set_shape",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -103,6 +104,10 @@ def load() -> C.CDLL:
     L.sidr_batch_set_counting.argtypes = [C.c_void_p, C.c_int]
     L.sidr_batch_counts.argtypes = [C.c_void_p, C.POINTER(_Counts)]
     L.sidr_batch_guard_check.argtypes = [C.c_void_p]
+    L.sidr_batch_set_shape.argtypes = [C.c_void_p, C.c_int32]
+    L.sidr_ctx_set_shape.argtypes = [C.c_void_p, C.c_int32]
+    L.sidr_batch_autotune_sampled.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                              C.POINTER(C.c_float)]
     L.sidr_libm_pow.argtypes = [_dp, _dp, C.c_int64, C.c_int, _dp]
     L.sidr_kernel_launches.restype = C.c_int64
     L.sidr_rules_check.argtypes = [C.POINTER(_Rules), _lp, C.c_int32, C.POINTER(C.c_int32)]
@@ -264,6 +269,21 @@ class Batch:
     def set_counting(self, on: bool) -> None:
         _check(load().sidr_batch_set_counting(self.h, int(on)))
 
+    SHAPES = ((4, 4), (4, 5))  # warps per block, resident blocks per SM
+
+    def set_shape(self, shape: int) -> None:
+        """sidr_batch_set_shape: the block shape of the following runs."""
+        _check(load().sidr_batch_set_shape(self.h, shape))
+
+    def autotune_sampled(self, stride: int = 16, reps: int = 1):
+        """sidr_batch_autotune_sampled: times each block shape on every
+        stride-th rule and keeps the faster; returns (shape, [ms per shape]).
+        The sampled rules' scores are overwritten: run the batch afterwards."""
+        ch = C.c_int32()
+        ms = (C.c_float * len(self.SHAPES))()
+        _check(load().sidr_batch_autotune_sampled(self.h, reps, stride, C.byref(ch), ms))
+        return ch.value, [float(x) for x in ms]
+
     def guard_check(self) -> int:
         """sidr_batch_guard_check: the kernel's rule-record guard, tripped on
         purpose; returns the status (SIDR_ERR_KERNEL expected)."""
@@ -309,6 +329,11 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_shape(self, shape: int) -> None:
+        """sidr_ctx_set_shape: the block shape of this context's evaluate*
+        calls (Batch.SHAPES)."""
+        _check(load().sidr_ctx_set_shape(self.h, shape))
 
     # -- the reference-shaped calls (host buffers, synchronous)
     def evaluate(self, rules, sampled, N, term_mask) -> np.ndarray:

@@ -404,6 +404,8 @@ def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, wor
             "repeat_runs_identical": same, "out": ref_out,
             "block_shape": {"warps_per_block": sidr.Batch.SHAPES[shape][0],
                             "blocks_per_sm": sidr.Batch.SHAPES[shape][1],
+                            "lanes_per_pair": sidr.Batch.SHAPES[shape][2],
+                            "shapes": [list(x) for x in sidr.Batch.SHAPES],
                             "ms_on_sample": shape_ms, "sample": "every 16th rule, all scenarios"}}
 
 
@@ -489,12 +491,14 @@ def run_ours(args, rank, world, local):
 
 def multi_leg(args, stream):
     """The uneven batch (40 instances: 25/50/100/288 customers, three layouts,
-    m 2-4, H 230/1000, rules of log-uniform length 3-255) in one persistent
-    launch: block shape autotuned on a sample of the batch (every 16th rule of
-    the longest-first order) unless --multi-shape is given, CUDA-graph replay,
-    device-timed.  Then, per instance-size class, the same instances in a
-    launch of their own and one by one through the single-instance path, which
-    shows where the batch's time goes."""
+    m 2-4, H 230/1000, rules of log-uniform length 3-255): one persistent
+    launch per instance-size class, each class's block shape (warps, blocks,
+    lanes per pair) autotuned on a sample of the class (every 16th rule of its
+    longest-first order) unless --multi-shape is given, all captured in one
+    CUDA graph, device-timed.  Then, per size class, the same instances in a
+    launch of their own (at the chosen shape and at a warp per pair) and one
+    by one through the single-instance path, which shows where the batch's
+    time goes."""
     import numpy as np
     import torch
     import sidr
@@ -521,10 +525,10 @@ def multi_leg(args, stream):
     prep = time.perf_counter() - t0
     t_tune = time.perf_counter()
     if args.multi_shape >= 0:
-        chosen, ms = args.multi_shape, None
-        m.set_shape(chosen)
+        chosen, ms = [args.multi_shape] * len(sidr.Multi.CLASSES), None
+        m.set_shape(args.multi_shape)
     else:
-        chosen, ms = m.autotune_sampled(stride=16, reps=1)
+        chosen, ms = m.autotune_classes(stride=16, reps=1)
     t_tune = time.perf_counter() - t_tune
     m.capture()
     t = timed(lambda: m.run(stream.cuda_stream))
@@ -543,10 +547,15 @@ def multi_leg(args, stream):
     classes = {}
     for n in sorted({sd.n for sd in mw.sds}):
         ks = [k for k, sd in enumerate(mw.sds) if sd.n == n]
+        c = next(i for i, (lo, hi) in enumerate(sidr.Multi.CLASSES) if lo <= n <= hi)
         mc = sidr.Multi([mw.sds[k] for k in ks], [zps[k] for k in ks], [mw.rules[k] for k in ks],
                         [mw.sampled[k] for k in ks], mw.S, [mw.masks[k] for k in ks])
-        mc.set_shape(chosen)
+        mc.set_shape(chosen[c])
         tc = timed(lambda: mc.run(stream.cuda_stream), reps=1)
+        tw = tc
+        if sidr.Multi.SHAPES[chosen[c]][2] != 32:
+            mc.set_shape(0)
+            tw = timed(lambda: mc.run(stream.cuda_stream), reps=1)
         mc.close()
         t_one = 0.0
         for k in ks:
@@ -556,13 +565,17 @@ def multi_leg(args, stream):
             b.close()
             ctx.close()
         ev = sum(mw.rules[k].P for k in ks) * mw.S
-        classes[str(n)] = {"instances": len(ks), "evaluations": ev, "own_launch_seconds": tc,
-                           "own_launch_evals_per_s": ev / tc, "one_by_one_seconds": t_one,
+        classes[str(n)] = {"instances": len(ks), "evaluations": ev,
+                           "shape": list(sidr.Multi.SHAPES[chosen[c]]), "own_launch_seconds": tc,
+                           "own_launch_evals_per_s": ev / tc,
+                           "own_launch_warp_per_pair_seconds": tw, "one_by_one_seconds": t_one,
                            "one_by_one_evals_per_s": ev / t_one}
     return {"workload": f"40 instances x {args.multi_rules} rules x {args.multi_S} scenarios",
             "evaluations": P * mw.S, "seconds": t, "evals_per_s": P * mw.S / t,
-            "shapes_ms_on_sample": ms, "tuning_seconds": t_tune,
-            "chosen_shape": list(sidr.Multi.SHAPES[chosen]), "host_prep_seconds": prep,
+            "shapes": [list(x) for x in sidr.Multi.SHAPES],
+            "class_shapes_ms_on_sample": ms, "tuning_seconds": t_tune,
+            "chosen_shape_per_class": [list(sidr.Multi.SHAPES[x]) if x >= 0 else None for x in chosen],
+            "host_prep_seconds": prep,
             "spot_check_pairs": pairs, "spot_check_mismatches": mism, "per_size_class": classes}
 
 

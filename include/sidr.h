@@ -151,14 +151,18 @@ sidr_status sidr_batch_counts(sidr_batch* b, sidr_counts* out);
 /* Block shape of a batch's launches (no reference counterpart).  Shape 0 (the
  * default) budgets 128 registers per thread for 4 resident blocks of 4 warps
  * per SM; shape 1 budgets 96 for 5, which hides more latency at the price of
- * spills and pays on rules that spend their time in ATRISK.  Both give the
- * same scores.  sidr_batch_autotune_sampled times each shape on every
+ * spills and pays on rules that spend their time in ATRISK.  Shapes 0 and 1
+ * run one (rule, scenario) pair per warp, shapes 2 and 3 (the same register
+ * budgets) two pairs per warp, 16 lanes each, which keeps more lanes busy
+ * when decisions have few candidates.  All give the same scores
+ * (the reference runs one thread per pair, engine/factory.cuh:42-61; these
+ * are the other end of the range).  sidr_batch_autotune_sampled times each shape on every
  * stride-th rule of the batch (all its scenarios; the first of reps + 1 runs
  * warms up), keeps the faster for sidr_batch_run and reports it in *chosen and
  * the times in ms[SIDR_BATCH_SHAPES] (either may be null).  The sampled rules'
  * scores are overwritten; run the batch afterwards.  The counting launch
  * always uses shape 0. */
-#define SIDR_BATCH_SHAPES 2
+#define SIDR_BATCH_SHAPES 4
 sidr_status sidr_batch_set_shape(sidr_batch* b, int32_t shape);
 /* The block shape of a context's sidr_evaluate* calls (default 0). */
 sidr_status sidr_ctx_set_shape(sidr_ctx* ctx, int32_t shape);
@@ -171,16 +175,23 @@ sidr_status sidr_batch_autotune_sampled(sidr_batch* b, int32_t reps, int32_t str
  * rule p belongs to instance rule_instance[p], reads the [T][n_k] scenario
  * block at sampled + sampled_offsets[k] (in doubles; the flat host buffer
  * holds n_sampled doubles) and mask row k of masks [K][61]; out[p*T + s].
- * Work is handed out longest-estimated-rule first.  Several block shapes of
- * the kernel are compiled in; sidr_multi_autotune times each on this batch
- * (reps runs, best time), keeps the fastest and remembers the choice for
- * batches of the same shape (instances' sizes, rule and scenario counts,
- * program sizes, SM count) in this process; ms[] (may be NULL) receives
- * each shape's time, *chosen its index.  sidr_multi_capture records the
- * launch (counter reset + kernel) as a CUDA graph that sidr_multi_run then
- * replays. */
+ * Rules are grouped by the size class of their instance (SIDR_SIZE_CLASSES:
+ * n <= 32, n <= 64, n <= 128, larger); each non-empty class is one launch,
+ * with a block shape of its own, and within a class work is handed out
+ * longest-estimated-rule first.  Block shapes compiled in (warps per block x
+ * minimum resident blocks per SM x lanes per pair): 0: 4x3x32, 1: 8x2x32,
+ * 2: 2x6x32, 3: 4x3x16, 4: 4x3x8; 16 and 8 lanes per pair run 2 and 4 pairs
+ * per warp, for small instances whose decisions have few candidates.
+ * sidr_multi_autotune times each shape on this batch (every class at that
+ * shape; reps runs, best time), keeps the fastest and remembers the choice
+ * for batches of the same layout (instances' sizes, rule and scenario
+ * counts, program sizes, SM count) in this process; ms[] (may be NULL)
+ * receives each shape's time, *chosen its index.  sidr_multi_capture records
+ * the launches (counter reset + kernel per class) as a CUDA graph that
+ * sidr_multi_run then replays. */
 typedef struct sidr_multi sidr_multi;
-#define SIDR_MULTI_SHAPES 3
+#define SIDR_MULTI_SHAPES 5
+#define SIDR_SIZE_CLASSES 4
 sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps, int32_t K,
                               const sidr_rules_desc* rules, const int32_t* rule_instance,
                               const double* sampled, int64_t n_sampled,
@@ -193,7 +204,19 @@ sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, fl
  * tuning of a full-size batch takes about 1/stride of a launch per shape. */
 sidr_status sidr_multi_autotune_sampled(sidr_multi* m, int32_t reps, int32_t stride, int32_t* chosen,
                                         float* ms);
+/* A shape per size class, chosen on a sample of the class: each shape runs
+ * every stride-th rule of the class's part of the work order (all T
+ * scenarios) in one launch; the fastest is kept for that class.
+ * chosen[SIDR_SIZE_CLASSES] (may be NULL) receives each class's shape (-1 for
+ * a class without rules), ms[SIDR_SIZE_CLASSES * SIDR_MULTI_SHAPES] (may be
+ * NULL) the times, ms[c * SIDR_MULTI_SHAPES + shape] (-1 where not timed). */
+sidr_status sidr_multi_autotune_classes(sidr_multi* m, int32_t reps, int32_t stride, int32_t* chosen,
+                                        float* ms);
+/* The same shape for every class (sidr_multi_set_shape) or for one. */
 sidr_status sidr_multi_set_shape(sidr_multi* m, int32_t shape);
+sidr_status sidr_multi_set_class_shape(sidr_multi* m, int32_t size_class, int32_t shape);
+/* Each class's shape and number of rules (either pointer may be NULL). */
+sidr_status sidr_multi_shapes(sidr_multi* m, int32_t* shapes, int32_t* class_rules);
 sidr_status sidr_multi_capture(sidr_multi* m);
 sidr_status sidr_multi_run(sidr_multi* m, void* stream);
 sidr_status sidr_multi_read(sidr_multi* m, double* out);

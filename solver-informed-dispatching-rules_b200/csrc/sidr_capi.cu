@@ -122,8 +122,8 @@ struct sidr_batch {
     int grid = 0, block = 0;  // the launch of shape 0 (also the counting launch's)
     size_t smem = 0;
     int shape = 0;                               // eval_kernel_fn's shape for sidr_batch_run
-    int grid_s[2] = {}, block_s[2] = {};         // the launch of each shape
-    size_t smem_s[2] = {};
+    int grid_s[SIDR_BATCH_SHAPES] = {}, block_s[SIDR_BATCH_SHAPES] = {};  // the launch of each shape
+    size_t smem_s[SIDR_BATCH_SHAPES] = {};
     DevBuf prog, consts, slots, meta, sampled, out, counter, stats, error, fit;
     bool ran = false;
 };
@@ -254,26 +254,39 @@ sidr_status read_error_word(const int* dev_word, cudaStream_t st) {
     return SIDR_OK;
 }
 
-// Launch geometry for a program set: warps per block bounded by the shared
-// memory each warp's slice takes; one persistent grid over all SMs.
 // The single-instance kernel for a launch: counting instantiation or not, with
-// or without the rmod code (only batches that use rmod pay for it).
-// shape: 0 = SIDR_MIN_BLOCKS resident blocks per SM, 1 = kMoreBlocks (the
-// counting instantiation exists for shape 0 only).
+// or without the rmod code (only batches that use rmod pay for it), and the
+// block shape: {resident blocks per SM the registers are budgeted for, lanes
+// per pair} (the counting instantiation exists for shape 0 only).
+constexpr int kBatchShapes[SIDR_BATCH_SHAPES][2] = {
+    {SIDR_MIN_BLOCKS, 32}, {kMoreBlocks, 32}, {SIDR_MIN_BLOCKS, 16}, {kMoreBlocks, 16}};
 const void* eval_kernel_fn(bool counting, bool rmod, int shape = 0) {
     if (counting)
         return rmod ? (const void*)eval_kernel<true, true, SIDR_MIN_BLOCKS>
                     : (const void*)eval_kernel<true, false, SIDR_MIN_BLOCKS>;
-    if (shape == 1)
+    switch (shape) {
+    case 1:
         return rmod ? (const void*)eval_kernel<false, true, kMoreBlocks>
                     : (const void*)eval_kernel<false, false, kMoreBlocks>;
-    return rmod ? (const void*)eval_kernel<false, true, SIDR_MIN_BLOCKS>
-                : (const void*)eval_kernel<false, false, SIDR_MIN_BLOCKS>;
+    case 2:
+        return rmod ? (const void*)eval_kernel<false, true, SIDR_MIN_BLOCKS, 16>
+                    : (const void*)eval_kernel<false, false, SIDR_MIN_BLOCKS, 16>;
+    case 3:
+        return rmod ? (const void*)eval_kernel<false, true, kMoreBlocks, 16>
+                    : (const void*)eval_kernel<false, false, kMoreBlocks, 16>;
+    default:
+        return rmod ? (const void*)eval_kernel<false, true, SIDR_MIN_BLOCKS>
+                    : (const void*)eval_kernel<false, false, SIDR_MIN_BLOCKS>;
+    }
 }
 
+// Launch geometry for a program set: warps per block bounded by the shared
+// memory each warp's pair groups take; one persistent grid over all SMs.
 sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bool counting,
                         int& grid, int& block, size_t& smem, int shape = 0) {
-    const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
+    const int lpp = counting ? 32 : kBatchShapes[shape][1];
+    const int gpw = 32 / lpp;  // pairs per warp
+    const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap, lpp) * gpw;
     if (slice > c->smem_optin)
         return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
     int wpb = (int)std::min<size_t>(SIDR_WARPS_PER_BLOCK, c->smem_optin / slice);
@@ -285,7 +298,8 @@ sidr_status plan_launch(sidr_ctx* c, const HostPrograms& hp, long long items, bo
     int per_sm = 0;
     SIDR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
     if (per_sm < 1) per_sm = 1;
-    long long want = (items + wpb - 1) / wpb;
+    const long long per_block = (long long)wpb * gpw;
+    long long want = (items + per_block - 1) / per_block;
     grid = (int)std::max<long long>(1, std::min<long long>(want, (long long)c->sm_count * per_sm));
     return SIDR_OK;
 }
@@ -829,7 +843,8 @@ sidr_status sidr_batch_create(sidr_ctx* c, const sidr_rules_desc* r, const doubl
     b.prog_cap = hp.prog_cap;
     b.const_cap = hp.const_cap;
     s = plan_launch(c, hp, (long long)P * T, false, bt->grid, bt->block, bt->smem);
-    if (!s) s = plan_launch(c, hp, (long long)P * T, false, bt->grid_s[1], bt->block_s[1], bt->smem_s[1], 1);
+    for (int sh = 1; sh < SIDR_BATCH_SHAPES && !s; sh++)
+        s = plan_launch(c, hp, (long long)P * T, false, bt->grid_s[sh], bt->block_s[sh], bt->smem_s[sh], sh);
     if (s) {
         sidr_batch_destroy(bt);
         return s;
@@ -1204,22 +1219,33 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
 // ----------------------------------------------------------------------------
 // Multi-instance batches (sidr_multi_*).
 
+#include <array>
 #include <map>
 
 namespace {
 
-// The compiled block shapes of eval_multi_kernel: {warps per block, min blocks}.
-constexpr int kShapes[SIDR_MULTI_SHAPES][2] = {{4, 3}, {8, 2}, {2, 6}};
+// The compiled block shapes of eval_multi_kernel: {warps per block, min
+// blocks per SM, lanes per pair}.
+constexpr int kShapes[SIDR_MULTI_SHAPES][3] = {{4, 3, 32}, {8, 2, 32}, {2, 6, 32}, {4, 3, 16}, {4, 3, 8}};
 const void* multi_kernel(int shape, bool rmod) {
     switch (shape) {
     case 0: return rmod ? (const void*)eval_multi_kernel<4, 3, true> : (const void*)eval_multi_kernel<4, 3, false>;
     case 1: return rmod ? (const void*)eval_multi_kernel<8, 2, true> : (const void*)eval_multi_kernel<8, 2, false>;
-    default: return rmod ? (const void*)eval_multi_kernel<2, 6, true> : (const void*)eval_multi_kernel<2, 6, false>;
+    case 2: return rmod ? (const void*)eval_multi_kernel<2, 6, true> : (const void*)eval_multi_kernel<2, 6, false>;
+    case 3:
+        return rmod ? (const void*)eval_multi_kernel<4, 3, true, 16> : (const void*)eval_multi_kernel<4, 3, false, 16>;
+    default:
+        return rmod ? (const void*)eval_multi_kernel<4, 3, true, 8> : (const void*)eval_multi_kernel<4, 3, false, 8>;
     }
 }
 
+// Size class of an instance of n customers (each class runs in a launch of
+// its own, with its own block shape).
+int size_class(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : 3; }
+
+using ClassShapes = std::array<int, SIDR_SIZE_CLASSES>;
 std::mutex g_tune_lock;
-std::map<std::string, int> g_tune_cache;  // batch shape -> chosen block shape
+std::map<std::string, ClassShapes> g_tune_cache;  // batch layout -> chosen block shape per size class
 
 }  // namespace
 
@@ -1228,11 +1254,14 @@ struct sidr_multi {
     size_t smem_optin = 0;
     std::vector<void*> owned;
     DevBatch b{};
-    int shape = 0;
-    int grid[SIDR_MULTI_SHAPES] = {}, block[SIDR_MULTI_SHAPES] = {};
+    ClassShapes shape{};                         // block shape of each size class's launch
+    int cls_first[SIDR_SIZE_CLASSES] = {};       // the class's first rule in the work order
+    int cls_items[SIDR_SIZE_CLASSES] = {};       // its number of rules
+    int block[SIDR_MULTI_SHAPES] = {};
+    int full_grid[SIDR_MULTI_SHAPES] = {};       // resident blocks of each shape on all SMs
     size_t smem[SIDR_MULTI_SHAPES] = {};
     std::string key;
-    std::vector<int32_t> order;  // the longest-first work order (host copy)
+    std::vector<int32_t> order;  // the work order (host copy): class by class, longest first in each
     bool rmod = false;           // some rule uses rmod: the RMOD kernels
     cudaStream_t gstream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -1263,14 +1292,47 @@ cudaError_t put_dev(sidr_multi* m, const void* src, size_t bytes, const void** d
     return cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
 }
 
-sidr_status multi_launch(sidr_multi* m, int shape, cudaStream_t st) {
+// One launch of block shape `shape` over n_rules rules of the work order
+// (device array `order`), all T scenarios each; the persistent grid is cut to
+// the items there are.
+sidr_status launch_part(sidr_multi* m, int shape, const int32_t* order, int n_rules, cudaStream_t st) {
+    if (n_rules <= 0 || m->T <= 0) return SIDR_OK;
+    DevBatch b = m->b;
+    b.order = order;
+    b.P_items = n_rules;
+    const long long per_block = (long long)kShapes[shape][0] * (32 / kShapes[shape][2]);
+    const long long items = (long long)n_rules * m->T;
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>((items + per_block - 1) / per_block, m->full_grid[shape]));
     SIDR_CUDA(cudaMemsetAsync(m->b.counter, 0, sizeof(unsigned long long), st));
-    SIDR_CUDA(cudaMemsetAsync(m->b.error, 0, sizeof(int), st));
-    void* args[] = {&m->b};
-    SIDR_CUDA(cudaLaunchKernel(multi_kernel(shape, m->rmod), dim3(m->grid[shape]), dim3(m->block[shape]),
-                               args, m->smem[shape], st));
+    void* args[] = {&b};
+    SIDR_CUDA(cudaLaunchKernel(multi_kernel(shape, m->rmod), dim3(grid), dim3(m->block[shape]), args,
+                               m->smem[shape], st));
     g_launches.fetch_add(1);
     return SIDR_OK;
+}
+
+// The whole batch: one launch per non-empty size class, each with its shape,
+// one after another on st; the error word is cleared once before them.
+sidr_status multi_launch(sidr_multi* m, const ClassShapes& shapes, cudaStream_t st) {
+    SIDR_CUDA(cudaMemsetAsync(m->b.error, 0, sizeof(int), st));
+    for (int c = SIDR_SIZE_CLASSES - 1; c >= 0; c--) {
+        const sidr_status s = launch_part(m, shapes[c], m->b.order + m->cls_first[c], m->cls_items[c], st);
+        if (s) return s;
+    }
+    return SIDR_OK;
+}
+
+int class_launches(const sidr_multi* m) {
+    int k = 0;
+    for (int c = 0; c < SIDR_SIZE_CLASSES; c++) k += m->cls_items[c] > 0 && m->T > 0;
+    return k;
+}
+
+ClassShapes all_classes(int shape) {
+    ClassShapes a;
+    a.fill(shape);
+    return a;
 }
 
 }  // namespace
@@ -1329,6 +1391,20 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
         order[p] = p;
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return est[a] > est[b]; });
+    // then grouped by the size class of the rule's instance, largest class
+    // first: each class is one launch of its own block shape
+    int cls_first[SIDR_SIZE_CLASSES] = {}, cls_items[SIDR_SIZE_CLASSES] = {};
+    {
+        std::vector<int32_t> by_class;
+        by_class.reserve(order.size());
+        for (int c = SIDR_SIZE_CLASSES - 1; c >= 0; c--) {
+            cls_first[c] = (int)by_class.size();
+            for (int32_t p : order)
+                if (size_class(hs[hp.meta[p].inst].n) == c) by_class.push_back(p);
+            cls_items[c] = (int)by_class.size() - cls_first[c];
+        }
+        order.swap(by_class);
+    }
 
     DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(device));
@@ -1408,6 +1484,10 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
         return bail(e, "batch upload");
     b.n_inst = K;
     m->order = order;
+    for (int c = 0; c < SIDR_SIZE_CLASSES; c++) {
+        m->cls_first[c] = cls_first[c];
+        m->cls_items[c] = cls_items[c];
+    }
     b.P = r->P;
     b.T = T;
     b.group_size = r->P > 0 ? r->P : 1;
@@ -1416,7 +1496,6 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
     b.rows = hp.rows;
     b.prog_cap = hp.prog_cap;
     b.const_cap = hp.const_cap;
-    const size_t slice = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap);
     int nmax = 0;
     for (int k = 0; k < K; k++) nmax = std::max(nmax, hs[k].n);
     char kb[256];
@@ -1425,9 +1504,9 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
     m->key = kb;
     for (int k = 0; k < K; k++) m->key += std::to_string(hs[k].n) + ",";
     for (int sh = 0; sh < SIDR_MULTI_SHAPES; sh++) {
-        const int wpb = kShapes[sh][0];
+        const int wpb = kShapes[sh][0], lpp = kShapes[sh][2];
         m->block[sh] = 32 * wpb;
-        m->smem[sh] = slice * wpb;
+        m->smem[sh] = warp_slice_bytes(hp.rows, hp.const_cap, hp.prog_cap, lpp) * (32 / lpp) * wpb;
         if (m->smem[sh] > m->smem_optin) {
             multi_free(m);
             return fail(SIDR_ERR_TOO_LARGE, "rule programs need more shared memory than one block has");
@@ -1439,9 +1518,7 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_kernel(sh, m->rmod), m->block[sh],
                                                                m->smem[sh])) != cudaSuccess)
             return bail(e, "occupancy");
-        const long long items = (long long)r->P * T;
-        m->grid[sh] = (int)std::max<long long>(
-            1, std::min<long long>((items + wpb - 1) / wpb, (long long)m->sm_count * std::max(per_sm, 1)));
+        m->full_grid[sh] = m->sm_count * std::max(per_sm, 1);
     }
     {
         std::lock_guard<std::mutex> g(g_tune_lock);
@@ -1455,9 +1532,63 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
 sidr_status sidr_multi_set_shape(sidr_multi* m, int32_t shape) {
     if (!m || shape < 0 || shape >= SIDR_MULTI_SHAPES) return fail(SIDR_ERR_INVALID, "bad shape");
     if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
-    m->shape = shape;
+    m->shape = all_classes(shape);
     return SIDR_OK;
 }
+
+sidr_status sidr_multi_set_class_shape(sidr_multi* m, int32_t cls, int32_t shape) {
+    if (!m || cls < 0 || cls >= SIDR_SIZE_CLASSES || shape < 0 || shape >= SIDR_MULTI_SHAPES)
+        return fail(SIDR_ERR_INVALID, "bad class or shape");
+    if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
+    m->shape[cls] = shape;
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_shapes(sidr_multi* m, int32_t* shapes, int32_t* class_rules) {
+    if (!m) return fail(SIDR_ERR_INVALID, "null batch");
+    for (int c = 0; c < SIDR_SIZE_CLASSES; c++) {
+        if (shapes) shapes[c] = m->shape[c];
+        if (class_rules) class_rules[c] = m->cls_items[c];
+    }
+    return SIDR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Best of reps timed runs (after one warm-up run) of launch(); 0 or an error.
+template <class F>
+sidr_status time_best(int reps, cudaStream_t st, F launch, float& t_best) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (!e) e = cudaEventCreate(&e1);
+    sidr_status s = SIDR_OK;
+    t_best = 1e30f;
+    for (int k = 0; k < (reps < 1 ? 1 : reps) + 1 && !e && !s; k++) {
+        e = cudaEventRecord(e0, st);
+        if (!e) s = launch();
+        if (!e && !s) e = cudaEventRecord(e1, st);
+        if (!e && !s) e = cudaEventSynchronize(e1);
+        float t = 0.f;
+        if (!e && !s) e = cudaEventElapsedTime(&t, e0, e1);
+        if (!e && !s && k > 0 && t < t_best) t_best = t;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) return s;
+    if (e) return fail(SIDR_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    return SIDR_OK;
+}
+
+void remember(sidr_multi* m) {
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    g_tune_cache[m->key] = m->shape;
+}
+
+}  // namespace
+
+extern "C" {
 
 sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, float* ms) {
     if (!m) return fail(SIDR_ERR_INVALID, "null batch");
@@ -1465,39 +1596,25 @@ sidr_status sidr_multi_autotune(sidr_multi* m, int32_t reps, int32_t* chosen, fl
     DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(m->device));
     if ((long long)m->P * m->T == 0) {
-        if (chosen) *chosen = m->shape;
+        if (chosen) *chosen = m->shape[0];
         return SIDR_OK;
     }
-    cudaEvent_t e0, e1;
-    SIDR_CUDA(cudaEventCreate(&e0));
-    SIDR_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     int best_sh = 0;
     for (int sh = 0; sh < SIDR_MULTI_SHAPES; sh++) {
-        float t_best = 1e30f;
-        for (int k = 0; k < (reps < 1 ? 1 : reps) + 1; k++) {  // first run warms up
-            SIDR_CUDA(cudaEventRecord(e0, 0));
-            sidr_status s = multi_launch(m, sh, 0);
-            if (s) return s;
-            SIDR_CUDA(cudaEventRecord(e1, 0));
-            SIDR_CUDA(cudaEventSynchronize(e1));
-            float t = 0.f;
-            SIDR_CUDA(cudaEventElapsedTime(&t, e0, e1));
-            if (k > 0 && t < t_best) t_best = t;
-        }
-        if (ms) ms[sh] = t_best;
-        if (t_best < best) {
-            best = t_best;
+        float t = 0.f;
+        const sidr_status s = time_best(reps, 0, [&] { return multi_launch(m, all_classes(sh), 0); }, t);
+        if (s) return s;
+        if (ms) ms[sh] = t;
+        if (t < best) {
+            best = t;
             best_sh = sh;
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    m->shape = best_sh;
-    {
-        std::lock_guard<std::mutex> g(g_tune_lock);
-        g_tune_cache[m->key] = best_sh;
-    }
+    sidr_status s = read_error_word(m->b.error, 0);
+    if (s) return s;
+    m->shape = all_classes(best_sh);
+    remember(m);
     if (chosen) *chosen = best_sh;
     return SIDR_OK;
 }
@@ -1509,54 +1626,85 @@ sidr_status sidr_multi_autotune_sampled(sidr_multi* m, int32_t reps, int32_t str
     DeviceGuard device_guard;
     SIDR_CUDA(cudaSetDevice(m->device));
     if ((long long)m->P * m->T == 0) {
-        if (chosen) *chosen = m->shape;
+        if (chosen) *chosen = m->shape[0];
         return SIDR_OK;
     }
-    // every stride-th rule of the longest-first order: the sample keeps the batch's mix of costs
+    // every stride-th rule of the work order: the sample keeps the batch's mix
+    // of instance sizes and rule costs; each shape runs it in one launch
     std::vector<int32_t> sample;
     for (size_t i = 0; i < m->order.size(); i += (size_t)stride) sample.push_back(m->order[i]);
     int32_t* d_order = nullptr;
     SIDR_CUDA(cudaMalloc(&d_order, sample.size() * sizeof(int32_t)));
     cudaError_t e = cudaMemcpy(d_order, sample.data(), sample.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
-    const DevBatch full = m->b;
-    m->b.order = d_order;
-    m->b.P_items = (int)sample.size();
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (!e) e = cudaEventCreate(&e0);
-    if (!e) e = cudaEventCreate(&e1);
     float best = 1e30f;
     int best_sh = 0;
-    sidr_status s = SIDR_OK;
-    for (int sh = 0; sh < SIDR_MULTI_SHAPES && !e && !s; sh++) {
-        float t_best = 1e30f;
-        for (int k = 0; k < (reps < 1 ? 1 : reps) + 1 && !e && !s; k++) {  // first run warms up
-            e = cudaEventRecord(e0, 0);
-            if (!e) s = multi_launch(m, sh, 0);
-            if (!e && !s) e = cudaEventRecord(e1, 0);
-            if (!e && !s) e = cudaEventSynchronize(e1);
-            float t = 0.f;
-            if (!e && !s) e = cudaEventElapsedTime(&t, e0, e1);
-            if (k > 0 && t < t_best) t_best = t;
-        }
-        if (ms) ms[sh] = t_best;
-        if (t_best < best) {
-            best = t_best;
+    sidr_status s = e ? fail(SIDR_ERR_CUDA, std::string("sampled autotune: ") + cudaGetErrorString(e)) : SIDR_OK;
+    for (int sh = 0; sh < SIDR_MULTI_SHAPES && !s; sh++) {
+        float t = 0.f;
+        s = time_best(reps, 0, [&] { return launch_part(m, sh, d_order, (int)sample.size(), 0); }, t);
+        if (s) break;
+        if (ms) ms[sh] = t;
+        if (t < best) {
+            best = t;
             best_sh = sh;
         }
     }
-    m->b = full;
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
     cudaFree(d_order);
     if (s) return s;
-    if (e) return fail(SIDR_ERR_CUDA, std::string("sampled autotune: ") + cudaGetErrorString(e));
     if ((s = read_error_word(m->b.error, 0))) return s;
-    m->shape = best_sh;
-    {
-        std::lock_guard<std::mutex> g(g_tune_lock);
-        g_tune_cache[m->key] = best_sh;
-    }
+    m->shape = all_classes(best_sh);
+    remember(m);
     if (chosen) *chosen = best_sh;
+    return SIDR_OK;
+}
+
+sidr_status sidr_multi_autotune_classes(sidr_multi* m, int32_t reps, int32_t stride, int32_t* chosen,
+                                        float* ms) {
+    if (!m || stride < 1) return fail(SIDR_ERR_INVALID, "null batch or stride < 1");
+    if (m->gexec) return fail(SIDR_ERR_INVALID, "the batch's launch is already captured");
+    DeviceGuard device_guard;
+    SIDR_CUDA(cudaSetDevice(m->device));
+    // every stride-th rule of each class's part of the work order, in one array
+    std::vector<int32_t> sample;
+    int first[SIDR_SIZE_CLASSES] = {}, count[SIDR_SIZE_CLASSES] = {};
+    for (int c = 0; c < SIDR_SIZE_CLASSES; c++) {
+        first[c] = (int)sample.size();
+        for (int i = 0; i < m->cls_items[c]; i += stride) sample.push_back(m->order[m->cls_first[c] + i]);
+        count[c] = (int)sample.size() - first[c];
+    }
+    if (ms)
+        for (int k = 0; k < SIDR_SIZE_CLASSES * SIDR_MULTI_SHAPES; k++) ms[k] = -1.f;
+    if (sample.empty() || m->T == 0) {
+        for (int c = 0; c < SIDR_SIZE_CLASSES; c++)
+            if (chosen) chosen[c] = m->cls_items[c] ? m->shape[c] : -1;
+        return SIDR_OK;
+    }
+    int32_t* d_order = nullptr;
+    SIDR_CUDA(cudaMalloc(&d_order, sample.size() * sizeof(int32_t)));
+    cudaError_t e = cudaMemcpy(d_order, sample.data(), sample.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    sidr_status s = e ? fail(SIDR_ERR_CUDA, std::string("class autotune: ") + cudaGetErrorString(e)) : SIDR_OK;
+    ClassShapes pick = m->shape;
+    for (int c = 0; c < SIDR_SIZE_CLASSES && !s; c++) {
+        if (!count[c]) continue;
+        float best = 1e30f;
+        for (int sh = 0; sh < SIDR_MULTI_SHAPES && !s; sh++) {
+            float t = 0.f;
+            s = time_best(reps, 0, [&] { return launch_part(m, sh, d_order + first[c], count[c], 0); }, t);
+            if (s) break;
+            if (ms) ms[c * SIDR_MULTI_SHAPES + sh] = t;
+            if (t < best) {
+                best = t;
+                pick[c] = sh;
+            }
+        }
+    }
+    cudaFree(d_order);
+    if (s) return s;
+    if ((s = read_error_word(m->b.error, 0))) return s;
+    m->shape = pick;
+    remember(m);
+    for (int c = 0; c < SIDR_SIZE_CLASSES; c++)
+        if (chosen) chosen[c] = m->cls_items[c] ? m->shape[c] : -1;
     return SIDR_OK;
 }
 
@@ -1589,7 +1737,7 @@ sidr_status sidr_multi_run(sidr_multi* m, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (m->gexec) {
         SIDR_CUDA(cudaGraphLaunch(m->gexec, st));
-        if ((long long)m->P * m->T > 0) g_launches.fetch_add(1);
+        g_launches.fetch_add(class_launches(m));
         return SIDR_OK;
     }
     if ((long long)m->P * m->T == 0) return SIDR_OK;

@@ -29,6 +29,40 @@ namespace sidr {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// The lanes that simulate one (rule, scenario) pair: the whole warp
+// (LPP = 32) or a group of 16 or 8 lanes, so that a warp runs 2 or 4 pairs
+// side by side.  Small instances have few candidates per decision, and a
+// group that matches them keeps more lanes busy.  Every collective of the
+// pair's simulation (ballots, shuffles, syncs) names only its group's lanes;
+// with LPP = 32 they are the plain full-warp forms.
+template <int LPP>
+struct Group {
+    static_assert(LPP == 32 || LPP == 16 || LPP == 8, "lanes per pair: 32, 16 or 8");
+    static constexpr int kPerWarp = 32 / LPP;
+    // lane within the group
+    __device__ __forceinline__ static int lane() { return (int)(threadIdx.x & (LPP - 1)); }
+    // the group's place in its warp
+    __device__ __forceinline__ static int index() { return (int)((threadIdx.x & 31) / LPP); }
+    __device__ __forceinline__ static int first() { return (int)((threadIdx.x & 31) & ~(LPP - 1)); }
+    __device__ __forceinline__ static unsigned mask() {
+        if constexpr (LPP == 32) return kFull;
+        else return ((1u << LPP) - 1u) << first();
+    }
+    __device__ __forceinline__ static void sync() {
+        if constexpr (LPP == 32) __syncwarp();
+        else __syncwarp(mask());
+    }
+    // the group's predicate bits, bit k = group lane k
+    __device__ __forceinline__ static uint32_t ballot(bool p) {
+        if constexpr (LPP == 32) return __ballot_sync(kFull, p);
+        else return __ballot_sync(mask(), p) >> first();
+    }
+    template <class T>
+    __device__ __forceinline__ static T shfl_xor(T v, int off) {
+        return __shfl_xor_sync(mask(), v, off);
+    }
+};
+
 // Block shape of the evaluator: warps per block and the minimum resident
 // blocks per SM that bound its registers (__launch_bounds__).  The kernel is
 // latency-bound (dependent FP64 chains and L1-missing table loads), so 16
@@ -61,10 +95,10 @@ __device__ unsigned long long sidr_section_cycles[16];
 #define SIDR_SEC_ADD(idx, var)
 #endif
 
-// Shared-memory slice of one warp.
+// Shared-memory slice of one pair group (a warp when LPP = 32).
 struct WarpSmem {
     DevInst* inst;     // the rule's instance (multi-instance batches)
-    double* rows;      // [rows][32]; between rounds also ATRISK's erf queue
+    double* rows;      // [rows][LPP]; between rounds also ATRISK's erf queue
     double* cst;       // [const_cap]
     uint32_t* prog;    // [prog_cap]
     int16_t* cand;     // [kMaxN]
@@ -72,7 +106,7 @@ struct WarpSmem {
     uint32_t* feas;    // [kMaxWords] feasible-now & unvisited
     uint32_t* atr;     // [kMaxWords] ATRISK's arrive-by-close filter
     uint8_t* slots;    // [64] compact row -> terminal slot
-    int qcap;          // doubles in the ATRISK queue (carved rows * 32)
+    int qcap;          // doubles in the ATRISK queue (carved rows * LPP)
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -88,9 +122,10 @@ constexpr int kQueueRows = 16;
 
 __host__ __device__ inline int carved_rows(int rows) { return rows < kQueueRows ? kQueueRows : rows; }
 
-__host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int prog_cap) {
+// Bytes of one group's slice; a block of W warps takes W * (32 / lpp) of them.
+__host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int prog_cap, int lpp = 32) {
     size_t b = kInstBytes;
-    b += (size_t)carved_rows(rows) * 32 * sizeof(double);
+    b += (size_t)carved_rows(rows) * lpp * sizeof(double);
     b += (size_t)const_cap * sizeof(double);
     b += align_up((size_t)prog_cap * sizeof(uint32_t), 8);
     b += (size_t)kMaxN * sizeof(int16_t);
@@ -100,12 +135,12 @@ __host__ __device__ inline size_t warp_slice_bytes(int rows, int const_cap, int 
 }
 
 __device__ __forceinline__ WarpSmem carve(unsigned char* base, int rows, int const_cap,
-                                          int prog_cap) {
+                                          int prog_cap, int lpp = 32) {
     WarpSmem s;
     s.inst = reinterpret_cast<DevInst*>(base);
     base += kInstBytes;
     s.rows = reinterpret_cast<double*>(base);
-    s.cst = s.rows + (size_t)carved_rows(rows) * 32;
+    s.cst = s.rows + (size_t)carved_rows(rows) * lpp;
     s.prog = reinterpret_cast<uint32_t*>(s.cst + const_cap);
     s.cand = reinterpret_cast<int16_t*>(
         reinterpret_cast<unsigned char*>(s.prog) + align_up((size_t)prog_cap * 4, 8));
@@ -113,7 +148,7 @@ __device__ __forceinline__ WarpSmem carve(unsigned char* base, int rows, int con
     s.feas = s.unv + kMaxWords;
     s.atr = s.feas + kMaxWords;
     s.slots = reinterpret_cast<uint8_t*>(s.atr + kMaxWords);
-    s.qcap = carved_rows(rows) * 32;
+    s.qcap = carved_rows(rows) * lpp;
     return s;
 }
 
@@ -538,8 +573,9 @@ __device__ __forceinline__ double norm_cdf_ratio(double num, double den) {
 // evaluates the queue 32 entries at a time; pass 2 adds the terms in order
 // from the masks, the word's scores (one per lane, shuffled) and the queue
 // (positions from the same ballots).  A word whose arguments overflow the
-// queue is added by at_risk_word_direct.
-template <bool COUNT>
+// queue is added by at_risk_word_direct.  The "warp" above is the pair's
+// group of LPP lanes.
+template <bool COUNT, int LPP = 32>
 __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc);
 
 // The pairs of word w of the customer set in ascending order, one at a
@@ -565,9 +601,10 @@ __device__ __noinline__ double at_risk_word_direct(const AtRiskView v, int w, ui
     return eloss;
 }
 
-template <bool COUNT>
+template <bool COUNT, int LPP>
 __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
-    const int lane = threadIdx.x & 31;
+    using G = Group<LPP>;
+    const int lane = G::lane();
     const uint32_t lt = (1u << lane) - 1u;
     const double hw = 8.5 * v.sd_c, lw = -8.5 * v.sd_c;
     const bool has = v.ci >= 0;
@@ -580,7 +617,7 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
         if (word == 0) continue;
         const uint32_t own = has ? bit_in_word(v.ci, w) : 0u;
         if (COUNT && has) heavy += __popc(word & ~own);
-        __syncwarp();  // the previous word's queue reads are done
+        G::sync();  // the previous word's queue reads are done
         SIDR_SEC_MARK(t_p1)
         uint32_t addm = 0, ewm = 0, ebm = 0, pbm = 0;
         int qn = 0;
@@ -602,8 +639,8 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
             ewm |= c.ew ? m : 0u;
             ebm |= c.eb ? m : 0u;
             pbm |= c.pb1 ? m : 0u;
-            const uint32_t bw = __ballot_sync(kFull, c.ew);
-            const uint32_t bb = __ballot_sync(kFull, c.eb);
+            const uint32_t bw = G::ballot(c.ew);
+            const uint32_t bb = G::ballot(c.eb);
             const int pw = qn + __popc(bw & lt);
             qn += __popc(bw);
             const int pb = qn + __popc(bb & lt);
@@ -628,24 +665,27 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
         }
         SIDR_SEC_MARK(t_q)
         if (qn) {
-            __syncwarp();
-            for (int k = lane; k < qn; k += 32) Q[2 * k] = norm_cdf_ratio(Q[2 * k], Q[2 * k + 1]);
-            __syncwarp();
+            G::sync();
+            for (int k = lane; k < qn; k += LPP) Q[2 * k] = norm_cdf_ratio(Q[2 * k], Q[2 * k + 1]);
+            G::sync();
         }
         SIDR_SEC_ADD(12, t_q);
         SIDR_SEC_MARK(t_p2)
+        // the word's scores: one per lane, shuffled (a full warp), or loaded
         const int jl = (w << 5) + lane;
-        const double sw = jl < v.n ? v.scores[jl] : 0.0;
+        const double sw = (LPP == 32 && jl < v.n) ? v.scores[jl] : 0.0;
         const uint32_t anym = addm | ewm | ebm;
         qn = 0;
         for (uint32_t bits = word; bits;) {
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
             const uint32_t m = 1u << b;
-            const double sj = __shfl_sync(kFull, sw, b);
+            double sj;
+            if constexpr (LPP == 32) sj = __shfl_sync(kFull, sw, b);
+            else sj = v.scores[(w << 5) + b];
             const bool ew = (ewm & m) != 0, eb = (ebm & m) != 0;
-            const uint32_t bw = __ballot_sync(kFull, ew);
-            const uint32_t bb = __ballot_sync(kFull, eb);
+            const uint32_t bw = G::ballot(ew);
+            const uint32_t bb = G::ballot(eb);
             const int pw = qn + __popc(bw & lt);
             qn += __popc(bw);
             const int pb = qn + __popc(bb & lt);
@@ -662,7 +702,7 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
         }
         SIDR_SEC_ADD(13, t_p2);
     }
-    __syncwarp();
+    G::sync();
     if (COUNT) {
         wc.heavy += heavy;
         wc.ops += heavy * kOpsAtRisk;
@@ -701,10 +741,10 @@ __device__ __forceinline__ AtRiskView at_risk_view(const DevInst& I, const WarpS
 // Terminals of candidate i into the lane's value rows, then the rule program.
 // Returns the priority (NaN mapped to -1e300).  eloss: the candidate's ATRISK
 // value (at_risk), when the rule reads it.
-template <bool COUNT, bool RMOD>
+template <bool COUNT, bool RMOD, int LPP = 32>
 __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
                                   const Decision& d, int i, double eloss, WarpCounts& wc) {
-    const int lane = threadIdx.x & 31;
+    const int lane = Group<LPP>::lane();
     const int n = I.n, ld = I.ld;
     const uint32_t need = rm.need;
     const double tmax = I.tmax;
@@ -992,7 +1032,7 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         case 60: v = x_ns_family(I, S, i, fin, 4); break;
         default: v = 0.0; break;
         }
-        S.rows[k * 32 + lane] = v;
+        S.rows[k * LPP + lane] = v;
     }
 
     SIDR_SEC_ADD(6, t_rows);
@@ -1002,8 +1042,8 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
         const uint32_t wd = S.prog[q];
         const uint32_t op = wd & 7u;
         const uint32_t oa = (wd >> 3) & 1023u, ob = (wd >> 13) & 1023u, od = wd >> 23;
-        const double a = (oa & kOpConst) ? S.cst[oa & 511u] : S.rows[oa * 32 + lane];
-        const double b = (ob & kOpConst) ? S.cst[ob & 511u] : S.rows[ob * 32 + lane];
+        const double a = (oa & kOpConst) ? S.cst[oa & 511u] : S.rows[oa * LPP + lane];
+        const double b = (ob & kOpConst) ? S.cst[ob & 511u] : S.rows[ob * LPP + lane];
         double r;
         switch (op) {
         case 0: r = a + b; break;
@@ -1023,11 +1063,11 @@ __device__ double score_candidate(const DevInst& I, const WarpSmem& S, const Rul
             if constexpr (RMOD) r = libm::rmod_(a, b);
             else r = pow(a > 0.0 ? a : 0.0, 1.0 + (b < 0.0 ? 0.0 : (b > 1.0 ? 1.0 : b)));
         }
-        S.rows[od * 32 + lane] = r;
+        S.rows[od * LPP + lane] = r;
     }
     SIDR_SEC_ADD(7, t_prog);
     const uint32_t res = (uint32_t)rm.res;
-    double pri = (res & kOpConst) ? S.cst[res & 511u] : S.rows[res * 32 + lane];
+    double pri = (res & kOpConst) ? S.cst[res & 511u] : S.rows[res * LPP + lane];
     if (pri != pri) pri = -1e300;
     return pri;
 }
@@ -1041,45 +1081,56 @@ struct CaptureAt {
 // One decision: returns the chosen customer or -1 (pick_best).  CAPTURE:
 // every candidate's terminal rows (the first B.cap_k rows: the rule was
 // compiled with all active slots as rows) and the choice are recorded.
-template <bool COUNT, bool RMOD, bool CAPTURE = false>
+// LPP: lanes of the pair's group; candidates are spread LPP per round.
+template <bool COUNT, bool RMOD, bool CAPTURE = false, int LPP = 32>
 __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, Decision& d,
                       WarpCounts& wc, CaptureAt cap = CaptureAt{nullptr, -1}) {
-    const int lane = threadIdx.x & 31;
+    static_assert(LPP == 32 || !CAPTURE, "capture runs whole warps");
+    using G = Group<LPP>;
+    const int lane = G::lane();
     const int n = I.n, ld = I.ld, nw = I.nw;
     const uint32_t need = rm.need;
     const bool need_atr = (need & kNeedAtRisk) != 0;
 
     SIDR_SEC_MARK(t_prep)
     // Feasible-now bitmask (the reference's candidate filter, :75-82) and
-    // ATRISK's arrive-by-close filter, one ballot per 32 customers.
+    // ATRISK's arrive-by-close filter, one ballot per LPP customers.
     const double* Fc = I.F + (size_t)d.cur * n;
     const double* Dc = I.dist + (size_t)d.cur * ld + 1;
     for (int w = 0; w < nw; w++) {
-        const int j = (w << 5) + lane;
-        const bool u = (S.unv[w] >> lane) & 1u;
-        const bool f = u && d.ct <= Fc[j];
-        const uint32_t bf = __ballot_sync(kFull, f);
-        uint32_t ba = 0;
-        if (need_atr) {
-            const bool a = u && !(d.ct + Dc[j] > I.close_t[j]);
-            ba = __ballot_sync(kFull, a);
+        uint32_t bf = 0, ba = 0;
+#pragma unroll
+        for (int h = 0; h < 32; h += LPP) {
+            const int t = h + lane;
+            const int j = (w << 5) + t;
+            const bool u = (S.unv[w] >> t) & 1u;
+            const bool f = u && d.ct <= Fc[j];
+            bf |= G::ballot(f) << h;
+            if (need_atr) {
+                const bool a = u && !(d.ct + Dc[j] > I.close_t[j]);
+                ba |= G::ballot(a) << h;
+            }
         }
         if (lane == 0) {
             S.feas[w] = bf;
             S.atr[w] = ba;
         }
     }
-    __syncwarp();
+    G::sync();
 
     SIDR_SEC_ADD(0, t_prep);
     SIDR_SEC_MARK(t_compact)
     int ncand = 0;
     for (int w = 0; w < nw; w++) {
         const uint32_t bits = S.feas[w];
-        if ((bits >> lane) & 1u) S.cand[ncand + __popc(bits & ((1u << lane) - 1u))] = (int16_t)((w << 5) + lane);
+#pragma unroll
+        for (int h = 0; h < 32; h += LPP) {
+            const int t = h + lane;
+            if ((bits >> t) & 1u) S.cand[ncand + __popc(bits & ((1u << t) - 1u))] = (int16_t)((w << 5) + t);
+        }
         ncand += __popc(bits);
     }
-    __syncwarp();
+    G::sync();
 
     // Per-decision aggregates (:55-71).
     d.sat = I.tmax > 0.0 ? d.ct / I.tmax : 0.0;
@@ -1112,17 +1163,17 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
     SIDR_SEC_ADD(1, t_compact);
     int best = -1;
     double best_pri = -1e300;
-    for (int base = 0; base < ncand; base += 32) {
+    for (int base = 0; base < ncand; base += LPP) {
         const int k = base + lane;
         double pri = -1e300;
         int idx = 0x7fffffff;
         SIDR_SEC_MARK(t_atr)
         const double eloss =
-            need_atr ? at_risk<COUNT>(at_risk_view(I, S, d, k < ncand ? S.cand[k] : -1), wc) : 0.0;
+            need_atr ? at_risk<COUNT, LPP>(at_risk_view(I, S, d, k < ncand ? S.cand[k] : -1), wc) : 0.0;
         SIDR_SEC_ADD(10, t_atr);
         if (k < ncand) {
             idx = S.cand[k];
-            pri = score_candidate<COUNT, RMOD>(I, S, rm, d, idx, eloss, wc);
+            pri = score_candidate<COUNT, RMOD, LPP>(I, S, rm, d, idx, eloss, wc);
             if (CAPTURE && cap.slot >= 0 && k < cap.C->cand) {
                 const CaptureBuf& C = *cap.C;
                 const size_t at = (size_t)cap.slot * C.cand + k;
@@ -1132,9 +1183,9 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
         }
         SIDR_SEC_MARK(t_argmax)
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double op = __shfl_xor_sync(kFull, pri, off);
-            const int oi = __shfl_xor_sync(kFull, idx, off);
+        for (int off = LPP / 2; off > 0; off >>= 1) {
+            const double op = G::shfl_xor(pri, off);
+            const int oi = G::shfl_xor(idx, off);
             if (op > pri || (op == pri && oi < idx)) {
                 pri = op;
                 idx = oi;
@@ -1153,20 +1204,21 @@ __device__ int decide(const DevInst& I, const WarpSmem& S, const RuleMeta& rm, D
     return best;
 }
 
-// sim_one (engine/sim_core.hpp:207-238) for one pair; every lane returns the
-// same total.
-template <bool COUNT, bool RMOD, bool CAPTURE = false>
+// sim_one (engine/sim_core.hpp:207-238) for one pair; every lane of the
+// pair's group returns the same total.
+template <bool COUNT, bool RMOD, bool CAPTURE = false, int LPP = 32>
 __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& rm,
                           const double* smp, WarpCounts& wc, const CaptureBuf* capC = nullptr,
                           int scenario = 0) {
-    const int lane = threadIdx.x & 31;
+    using G = Group<LPP>;
+    const int lane = G::lane();
     const int n = I.n, ld = I.ld;
-    for (int w = lane; w < I.nw; w += 32) {
+    for (int w = lane; w < I.nw; w += LPP) {
         const int lo = w << 5;
         const int cnt = n - lo >= 32 ? 32 : n - lo;
         S.unv[w] = cnt >= 32 ? kFull : ((1u << cnt) - 1u);
     }
-    __syncwarp();
+    G::sync();
     double total = 0.0;
     int dec_no = 0;
     for (int v = 0; v < I.m; v++) {
@@ -1181,7 +1233,7 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
                 dec_no++;
                 b = decide<COUNT, RMOD, true>(I, S, rm, d, wc, cap);
             } else {
-                b = decide<COUNT, RMOD>(I, S, rm, d, wc);
+                b = decide<COUNT, RMOD, false, LPP>(I, S, rm, d, wc);
             }
             if (b < 0) break;
             SIDR_SEC_MARK(t_upd)
@@ -1191,7 +1243,7 @@ __device__ double rollout(const DevInst& I, const WarpSmem& S, const RuleMeta& r
             d.cur = b + 1;
             total += I.scores[b];
             if (lane == 0) S.unv[b >> 5] &= ~(1u << (b & 31));
-            __syncwarp();
+            G::sync();
             SIDR_SEC_ADD(9, t_upd);
         }
     }
@@ -1213,16 +1265,72 @@ __device__ __forceinline__ int rule_record_error(const RuleMeta& m, const DevBat
     return 0;
 }
 
+// One work item (a rule and a scenario) on the pair's group: the rule's
+// program, constants, slot list (and, MULTI, its instance descriptor) are
+// staged into the group's slice when the rule changes, then the rollout runs
+// and its total is stored.
+template <bool COUNT, bool MULTI, bool RMOD, bool CAPTURE, int LPP>
+__device__ __forceinline__ void run_item(const DevInst& I0, const DevBatch& B, const WarpSmem& S,
+                                         unsigned long long item, int& staged, RuleMeta& rm,
+                                         WarpCounts& wc, const CaptureBuf* capC) {
+    using G = Group<LPP>;
+    const int lane = G::lane();
+    const int r = (int)(item / (unsigned long long)B.T);
+    const int s = (int)(item % (unsigned long long)B.T);
+    const int p = B.order ? B.order[r] : r;
+    if (p != staged) {
+        // Guard of the group's shared-memory slice: a rule record the launch
+        // was not sized for is refused (error word set, score NaN) before
+        // anything of it is staged.  Host validation makes this unreachable;
+        // the host reads the word back after every launch.
+        const int code = (p < 0 || p >= B.P) ? kErrRuleIndex : rule_record_error(B.meta[p], B, MULTI, RMOD);
+        if (code) {
+            if (lane == 0) {
+                atomicCAS(B.error, 0, code);
+                if (p >= 0 && p < B.P) B.out[(size_t)p * B.T + s] = __longlong_as_double(0x7ff8000000000000LL);
+            }
+            staged = -1;
+            G::sync();
+            return;
+        }
+        rm = B.meta[p];
+        for (int q = lane; q < rm.n_ins; q += LPP) S.prog[q] = B.prog[rm.prog_off + q];
+        for (int q = lane; q < rm.n_const; q += LPP) S.cst[q] = B.consts[rm.const_off + q];
+        for (int q = lane; q < rm.K; q += LPP) S.slots[q] = B.slots[rm.slot_off + q];
+        if (MULTI) {
+            const unsigned long long* src =
+                reinterpret_cast<const unsigned long long*>(B.insts + rm.inst);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(S.inst);
+            for (int q = lane; q < (int)(sizeof(DevInst) / 8); q += LPP) dst[q] = src[q];
+        }
+        staged = p;
+        G::sync();
+    }
+    const DevInst& I = MULTI ? *S.inst : I0;
+    const double* smp =
+        MULTI ? B.sampled + B.smp_off[rm.inst] + (size_t)s * I.n
+              : B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
+    double tot;
+    if constexpr (CAPTURE) tot = rollout<COUNT, RMOD, true>(I, S, rm, smp, wc, capC, s);
+    else tot = rollout<COUNT, RMOD, false, LPP>(I, S, rm, smp, wc);
+    if (lane == 0) B.out[(size_t)p * B.T + s] = tot;
+}
+
 // The persistent work loop.  MULTI: every rule carries its instance; the
-// warp stages the instance descriptor with the rule's program.
-template <bool COUNT, bool MULTI, bool RMOD, bool CAPTURE = false>
+// group stages the instance descriptor with the rule's program.  LPP < 32:
+// the warp's first lane takes 32 / LPP consecutive items from the queue at
+// once (usually one rule on neighbouring scenarios), one per group; the groups
+// run side by side and the warp takes its next items when all are done.
+template <bool COUNT, bool MULTI, bool RMOD, bool CAPTURE = false, int LPP = 32>
 __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
                                           const CaptureBuf* capC = nullptr) {
+    static_assert(LPP == 32 || (!COUNT && !CAPTURE), "counting and capture run whole warps");
+    using G = Group<LPP>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const size_t slice = warp_slice_bytes(B.rows, B.const_cap, B.prog_cap);
-    const WarpSmem S = carve(smem_raw + (size_t)wib * slice, B.rows, B.const_cap, B.prog_cap);
+    const int gib = (threadIdx.x >> 5) * G::kPerWarp + G::index();  // group in block
+    const size_t slice = warp_slice_bytes(B.rows, B.const_cap, B.prog_cap, LPP);
+    const WarpSmem S = carve(smem_raw + (size_t)gib * slice, B.rows, B.const_cap, B.prog_cap, LPP);
 
     const unsigned long long total =
         (unsigned long long)(B.P_items > 0 ? B.P_items : B.P) * (unsigned long long)B.T;
@@ -1230,49 +1338,16 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
     RuleMeta rm;
     WarpCounts wc = {0, 0, 0, 0, 0, 0};
     for (;;) {
-        unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(B.counter, 1ull);
-        item = __shfl_sync(kFull, item, 0);
-        if (item >= total) break;
-        const int r = (int)(item / (unsigned long long)B.T);
-        const int s = (int)(item % (unsigned long long)B.T);
-        const int p = B.order ? B.order[r] : r;
-        if (p != staged) {
-            // Guard of the warp's shared-memory slice: a rule record the launch
-            // was not sized for is refused (error word set, score NaN) before
-            // anything of it is staged.  Host validation makes this unreachable;
-            // the host reads the word back after every launch.
-            const int code = (p < 0 || p >= B.P) ? kErrRuleIndex : rule_record_error(B.meta[p], B, MULTI, RMOD);
-            if (code) {
-                if (lane == 0) {
-                    atomicCAS(B.error, 0, code);
-                    if (p >= 0 && p < B.P) B.out[(size_t)p * B.T + s] = __longlong_as_double(0x7ff8000000000000LL);
-                }
-                staged = -1;
-                __syncwarp();
-                continue;
-            }
-            rm = B.meta[p];
-            for (int q = lane; q < rm.n_ins; q += 32) S.prog[q] = B.prog[rm.prog_off + q];
-            for (int q = lane; q < rm.n_const; q += 32) S.cst[q] = B.consts[rm.const_off + q];
-            for (int q = lane; q < rm.K; q += 32) S.slots[q] = B.slots[rm.slot_off + q];
-            if (MULTI) {
-                const unsigned long long* src =
-                    reinterpret_cast<const unsigned long long*>(B.insts + rm.inst);
-                unsigned long long* dst = reinterpret_cast<unsigned long long*>(S.inst);
-                for (int q = lane; q < (int)(sizeof(DevInst) / 8); q += 32) dst[q] = src[q];
-            }
-            staged = p;
-            __syncwarp();
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(B.counter, (unsigned long long)G::kPerWarp);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= total) break;
+        if constexpr (LPP == 32) {
+            run_item<COUNT, MULTI, RMOD, CAPTURE, LPP>(I0, B, S, base, staged, rm, wc, capC);
+        } else {
+            const unsigned long long item = base + (unsigned long long)G::index();
+            if (item < total) run_item<COUNT, MULTI, RMOD, CAPTURE, LPP>(I0, B, S, item, staged, rm, wc, capC);
         }
-        const DevInst& I = MULTI ? *S.inst : I0;
-        const double* smp =
-            MULTI ? B.sampled + B.smp_off[rm.inst] + (size_t)s * I.n
-                  : B.sampled + ((size_t)(p / B.group_size) * B.T + s) * (size_t)B.n;
-        double tot;
-        if constexpr (CAPTURE) tot = rollout<COUNT, RMOD, true>(I, S, rm, smp, wc, capC, s);
-        else tot = rollout<COUNT, RMOD>(I, S, rm, smp, wc);
-        if (lane == 0) B.out[(size_t)p * B.T + s] = tot;
     }
     if (COUNT) {
         // dec/cand/per-decision ops live in lane 0; the rest are per lane.
@@ -1295,12 +1370,13 @@ __device__ __forceinline__ void eval_body(const DevInst& I0, const DevBatch& B,
 // SIDR_MIN_BLOCKS (4: 128 registers) by default, or kMoreBlocks (5: 96
 // registers, more warps to hide latency, more spills), which pays on
 // populations that spend their time in ATRISK's long classification loops.
+// LPP: lanes per pair (32: a warp per pair; 16: two pairs per warp).
 constexpr int kMoreBlocks = 5;
 
-template <bool COUNT, bool RMOD, int MINB>
+template <bool COUNT, bool RMOD, int MINB, int LPP = 32>
 __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, MINB)
     eval_kernel(const DevInst I, const DevBatch B) {
-    eval_body<COUNT, false, RMOD>(I, B);
+    eval_body<COUNT, false, RMOD, false, LPP>(I, B);
 }
 
 // Decision-situation capture: one rule on B.T scenarios, every decision's
@@ -1311,10 +1387,11 @@ __global__ void __launch_bounds__(32 * SIDR_WARPS_PER_BLOCK, SIDR_MIN_BLOCKS)
 }
 
 // Multi-instance evaluator, one instantiation per block shape (warps per
-// block x minimum resident blocks); the autotuner picks among them.
-template <int WPB, int MINB, bool RMOD>
+// block x minimum resident blocks x lanes per pair); the autotuner picks
+// among them for each class of instance sizes.
+template <int WPB, int MINB, bool RMOD, int LPP = 32>
 __global__ void __launch_bounds__(32 * WPB, MINB) eval_multi_kernel(const DevBatch B) {
-    eval_body<false, true, RMOD>(DevInst{}, B);
+    eval_body<false, true, RMOD, false, LPP>(DevInst{}, B);
 }
 
 }  // namespace sidr

@@ -68,6 +68,7 @@ EXPORTS = [
     "sidr_multi_capture", "sidr_multi_run", "sidr_multi_read", "sidr_multi_destroy",
     "sidr_libm_eval", "sidr_batch_guard_check", "sidr_libm_pow", "sidr_multi_autotune_sampled",
     "sidr_batch_set_shape", "sidr_batch_autotune_sampled", "sidr_ctx_set_shape",
+    "sidr_multi_autotune_classes", "sidr_multi_set_class_shape", "sidr_multi_shapes",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -269,7 +270,8 @@ class Batch:
     def set_counting(self, on: bool) -> None:
         _check(load().sidr_batch_set_counting(self.h, int(on)))
 
-    SHAPES = ((4, 4), (4, 5))  # warps per block, resident blocks per SM
+    # warps per block, resident blocks per SM, lanes per (rule, scenario) pair
+    SHAPES = ((4, 4, 32), (4, 5, 32), (4, 4, 16), (4, 5, 16))
 
     def set_shape(self, shape: int) -> None:
         """sidr_batch_set_shape: the block shape of the following runs."""
@@ -377,7 +379,10 @@ class Multi:
     """A multi-instance batch (sidr_multi_*): several instances of uneven size,
     each with its own rules, scenarios and mask, in one persistent launch."""
 
-    SHAPES = ((4, 3), (8, 2), (2, 6))  # warps per block, min blocks per SM
+    # warps per block, min blocks per SM, lanes per (rule, scenario) pair
+    SHAPES = ((4, 3, 32), (8, 2, 32), (2, 6, 32), (4, 3, 16), (4, 3, 8))
+    # size classes of instances (customers): each class runs in a launch of its own
+    CLASSES = ((0, 32), (33, 64), (65, 128), (129, 512))
 
     def __init__(self, sds, zps, rules_per_instance, sampled_per_instance, T, masks,
                  device: int = 0):
@@ -392,6 +397,10 @@ class Multi:
             L.sidr_multi_autotune_sampled.argtypes = [vp, C.c_int32, C.c_int32,
                                                       C.POINTER(C.c_int32), C.POINTER(C.c_float)]
             L.sidr_multi_set_shape.argtypes = [vp, C.c_int32]
+            L.sidr_multi_autotune_classes.argtypes = [vp, C.c_int32, C.c_int32,
+                                                      C.POINTER(C.c_int32), C.POINTER(C.c_float)]
+            L.sidr_multi_set_class_shape.argtypes = [vp, C.c_int32, C.c_int32]
+            L.sidr_multi_shapes.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
             L.sidr_multi_capture.argtypes = [vp]
             L.sidr_multi_run.argtypes = [vp, vp]
             L.sidr_multi_read.argtypes = [vp, _dp]
@@ -439,8 +448,30 @@ class Multi:
         _check(load().sidr_multi_autotune_sampled(self.h, reps, stride, C.byref(ch), ms))
         return ch.value, [float(x) for x in ms]
 
+    def autotune_classes(self, stride: int = 16, reps: int = 1):
+        """sidr_multi_autotune_classes: a block shape per size class, each
+        timed on every stride-th rule of the class.  Returns ([shape per class,
+        -1 for classes without rules], [[ms per shape] per class, -1 where not
+        timed])."""
+        nc, ns = len(self.CLASSES), len(self.SHAPES)
+        ch = (C.c_int32 * nc)()
+        ms = (C.c_float * (nc * ns))()
+        _check(load().sidr_multi_autotune_classes(self.h, reps, stride, ch, ms))
+        return list(ch), [[float(ms[c * ns + s]) for s in range(ns)] for c in range(nc)]
+
     def set_shape(self, shape: int):
+        """The same block shape for every size class."""
         _check(load().sidr_multi_set_shape(self.h, shape))
+
+    def set_class_shape(self, cls: int, shape: int):
+        _check(load().sidr_multi_set_class_shape(self.h, cls, shape))
+
+    def shapes(self):
+        """(shape per size class, rules per size class)."""
+        nc = len(self.CLASSES)
+        sh, cnt = (C.c_int32 * nc)(), (C.c_int32 * nc)()
+        _check(load().sidr_multi_shapes(self.h, sh, cnt))
+        return list(sh), list(cnt)
 
     def capture(self):
         _check(load().sidr_multi_capture(self.h))

@@ -95,6 +95,43 @@ sidr_status sidr_gp_run_batched(sidr_ctx* ctx, const sidr_instance_desc* inst,
                                 int64_t test_seed, double* best_test, double* best_train,
                                 char* best_rules, int64_t rules_cap, sidr_gp_result* result);
 
+/* The seed-batched run one generation at a time, with checkpoint and resume
+ * (the reference's exhaust_batched, engine/gp_engine.cu:131-203, runs to the
+ * end in one call and cannot resume).  sidr_gp_run_batched is create, step
+ * through every generation, finish.
+ *   sidr_gp_batched_create    the populations of seeds first_seed ..
+ *                             first_seed + n_seeds - 1 (ctx must hold inst;
+ *                             the driver keeps a copy of what it needs)
+ *   sidr_gp_batched_step      evaluates (and breeds from) up to `generations`
+ *                             more generations, no further than cfg->generations
+ *   sidr_gp_batched_generation  generations evaluated so far
+ *   sidr_gp_batched_checkpoint  the run's whole state as text: seeds, the
+ *                             instance's hash, the mask, the generation reached,
+ *                             best train fitness so far, time and evaluation
+ *                             counters, and every seed's session as
+ *                             sidr_gp_checkpoint writes it; returns the bytes
+ *                             needed (cap 0 sizes the buffer; -1 for NULL)
+ *   sidr_gp_batched_restore   a run that continues exactly as the checkpointed
+ *                             one would; refused (SIDR_ERR_INVALID) when the
+ *                             text is malformed or was written for another
+ *                             instance; ctx must hold inst
+ *   sidr_gp_batched_finish    after the last generation: the final train block,
+ *                             each seed's best rule on the held-out block, and
+ *                             the outputs of sidr_gp_run_batched (its times and
+ *                             evaluations count the resumed parts too) */
+typedef struct sidr_gp_batched sidr_gp_batched;
+sidr_status sidr_gp_batched_create(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
+                                   const char* terminals_csv, const int64_t* term_mask, int32_t n_seeds,
+                                   int64_t first_seed, int64_t test_seed, sidr_gp_batched** out);
+sidr_status sidr_gp_batched_step(sidr_gp_batched* b, int32_t generations);
+int64_t sidr_gp_batched_generation(const sidr_gp_batched* b);
+int64_t sidr_gp_batched_checkpoint(const sidr_gp_batched* b, char* buf, int64_t cap);
+sidr_status sidr_gp_batched_restore(sidr_ctx* ctx, const sidr_instance_desc* inst, const char* checkpoint,
+                                    sidr_gp_batched** out);
+sidr_status sidr_gp_batched_finish(sidr_gp_batched* b, double* best_test, double* best_train, char* best_rules,
+                                   int64_t rules_cap, sidr_gp_result* result);
+void sidr_gp_batched_destroy(sidr_gp_batched* b);
+
 /* Many instances x many seeds (no single reference call: the reference runs
  * exhaust_batched, engine/gp_engine.cu:131-203, once per instance).  For each
  * of the K instances (zps [K][10], masks [K][61]) the seed-batched run of

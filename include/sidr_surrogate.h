@@ -85,6 +85,14 @@ void sidr_mlp_destroy(sidr_mlp* m);
 sidr_status sidr_mlp_param(sidr_mlp* m, int32_t which, int32_t write, float* values, float* grads,
                            int64_t* count);
 
+/* The model's whole training state, for checkpoints: every parameter's FP32
+ * values, Adam first and second moments (parameters in order 0..5, each as
+ * values, m, v), *count floats in all, and the Adam step count.  write = 0
+ * reads into state (and *step), write = 1 replaces them from state (and
+ * *step; the BF16 copies are refreshed).  state NULL: only *count (and
+ * *step) are set. */
+sidr_status sidr_mlp_state(sidr_mlp* m, int32_t write, float* state, int64_t* count, int64_t* step);
+
 /* y[rows] = model(x[rows][40]). */
 sidr_status sidr_mlp_predict(sidr_mlp* m, const float* x, int32_t rows, float* y);
 
@@ -156,6 +164,27 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                          uint64_t seed, int64_t test_seed, double* best_train, double* held_out,
                          double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
                          sidr_sgp_result* result);
+
+/* sidr_sgp_run with checkpoints (the reference's GP runs to the end in one
+ * call and cannot resume).  After every `every` generations (0: never) the
+ * driver's whole state -- the GP session, the decision situations, the
+ * model's weights, Adam moments and step count, the fitness history the
+ * model trains on, the counters and the per-generation outputs so far -- is
+ * written to checkpoint_path, through a temporary file renamed over it.  If
+ * checkpoint_path holds a checkpoint when the call starts, the run resumes
+ * from it and gives exactly the outputs of an uninterrupted run (times
+ * excepted); one written for another seed, test seed, instance, mask or
+ * setting is refused (SIDR_ERR_INVALID).  stop_after >= 0: the call writes a
+ * checkpoint and returns after that many generations of its own (the outputs
+ * of the generations run so far are filled, best_rule is not); *finished
+ * (may be NULL) is 1 when the run reached its last generation.  A NULL
+ * checkpoint_path is sidr_sgp_run. */
+sidr_status sidr_sgp_run_resumable(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
+                                   const sidr_sgp_config* sc, const char* terminals_csv, const int64_t* mask,
+                                   uint64_t seed, int64_t test_seed, const char* checkpoint_path, int32_t every,
+                                   int32_t stop_after, int32_t* finished, double* best_train, double* held_out,
+                                   double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
+                                   sidr_sgp_result* result);
 
 /* The large combined run (no single reference call: the reference runs
  * exhaust_batched, engine/gp_engine.cu:131-203, once per instance and seed

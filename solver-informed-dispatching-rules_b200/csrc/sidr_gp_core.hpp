@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
@@ -503,6 +504,38 @@ inline bool parse_terminals(const char* csv, std::vector<std::string>& out, std:
     }
     return true;
 }
+
+inline bool same_config(const sidr_gp_config& a, const sidr_gp_config& b) {
+    return a.population == b.population && a.generations == b.generations && a.max_depth == b.max_depth &&
+           a.min_depth == b.min_depth && a.tournament == b.tournament && a.elitism == b.elitism &&
+           a.crossover_rate == b.crossover_rate && a.mutation_rate == b.mutation_rate &&
+           a.reproduction_rate == b.reproduction_rate && a.train_samples == b.train_samples &&
+           a.test_samples == b.test_samples && a.with_rmod == b.with_rmod;
+}
+
+// FNV-1a over the instance's size, limits and arrays: a checkpoint resumes
+// only on the instance it was written for.
+inline uint64_t instance_hash(const sidr_instance_desc& d) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t bytes) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < bytes; i++) h = (h ^ c[i]) * 1099511628211ull;
+    };
+    mix(&d.n, sizeof d.n);
+    mix(&d.m, sizeof d.m);
+    mix(&d.tmax, sizeof d.tmax);
+    const size_t n = d.n > 0 ? (size_t)d.n : 0;
+    for (const double* a : {d.scores, d.durations, d.open_t, d.close_t, d.dist_to_depot})
+        if (a) mix(a, n * sizeof(double));
+    if (d.dist) mix(d.dist, (n + 1) * (n + 1) * sizeof(double));
+    return h;
+}
+
+// A GP's whole state as the text of sidr_gp_checkpoint (config, step count,
+// terminal set, leaf labels, generator state, population), and back;
+// state_parse refuses malformed text (SIDR_ERR_INVALID).  In sidr_gp.cpp.
+std::string state_text(const Gp& g, int64_t generation);
+sidr_status state_parse(const std::string& text, std::unique_ptr<Gp>& out, int64_t& generation);
 
 inline bool valid_config(const sidr_gp_config* c, std::string& err) {
     if (!c) {

@@ -3,10 +3,16 @@
 // sidr_surrogate.cu on their phenotypes, with the evaluator as the judge of
 // every fitness and plain breeding whenever the model's audit rank
 // correlation is too low.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
 #include <numeric>
 #include <set>
+#include <sstream>
+#include <type_traits>
 
 #include "../../include/sidr_surrogate.h"
 #include "sidr_gp_core.hpp"
@@ -96,6 +102,245 @@ sidr_status capture_for(sidr_ctx* ctx, const sidr_instance_desc* inst, const int
     return SIDR_OK;
 }
 
+
+// ---------------------------------------------------------------- checkpoints
+// Text of the surrogate driver's state between two generations.  Doubles and
+// floats travel as the hexadecimal digits of their bits, so NaN audit values
+// and every weight come back exactly.
+
+constexpr const char* kSgpHeader = "sidr-sgp-checkpoint 1";
+
+std::string hex64(double v) {
+    uint64_t u;
+    std::memcpy(&u, &v, 8);
+    char b[24];
+    std::snprintf(b, sizeof b, "%016llx", (unsigned long long)u);
+    return b;
+}
+std::string hex32(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    char b[16];
+    std::snprintf(b, sizeof b, "%08x", u);
+    return b;
+}
+bool unhex64(const std::string& t, double& v) {
+    if (t.size() != 16) return false;
+    char* end = nullptr;
+    const uint64_t u = std::strtoull(t.c_str(), &end, 16);
+    if (!end || *end) return false;
+    std::memcpy(&v, &u, 8);
+    return true;
+}
+bool unhex32(const std::string& t, float& v) {
+    if (t.size() != 8) return false;
+    char* end = nullptr;
+    const uint32_t u = (uint32_t)std::strtoul(t.c_str(), &end, 16);
+    if (!end || *end) return false;
+    std::memcpy(&v, &u, 4);
+    return true;
+}
+
+// A named list of values, 8 per line: "<key> <count>" then the lines.
+template <class T>
+void put_list(std::string& out, const char* key, const std::vector<T>& v) {
+    out += std::string(key) + " " + std::to_string(v.size()) + "\n";
+    for (size_t i = 0; i < v.size(); i++) {
+        if constexpr (std::is_same<T, double>::value) out += hex64(v[i]);
+        else if constexpr (std::is_same<T, float>::value) out += hex32(v[i]);
+        else out += std::to_string(v[i]);
+        out += (i % 8 == 7 || i + 1 == v.size()) ? "\n" : " ";
+    }
+}
+
+template <class T>
+bool get_list(std::istream& in, const char* key, std::vector<T>& v, size_t limit = (size_t)1 << 28) {
+    std::string line, word;
+    if (!std::getline(in, line)) return false;
+    std::istringstream ls(line);
+    long long cnt = -1;
+    if (!(ls >> word >> cnt) || word != key || cnt < 0 || (size_t)cnt > limit) return false;
+    v.clear();
+    v.reserve((size_t)cnt);
+    while ((long long)v.size() < cnt) {
+        if (!std::getline(in, line)) return false;
+        std::istringstream vs(line);
+        std::string tok;
+        while (vs >> tok) {
+            T x{};
+            if constexpr (std::is_same<T, double>::value) {
+                if (!unhex64(tok, x)) return false;
+            } else if constexpr (std::is_same<T, float>::value) {
+                if (!unhex32(tok, x)) return false;
+            } else {
+                char* end = nullptr;
+                const long long q = std::strtoll(tok.c_str(), &end, 10);
+                if (!end || *end) return false;
+                x = (T)q;
+            }
+            v.push_back(x);
+        }
+    }
+    return (long long)v.size() == cnt;
+}
+
+std::string sgp_config_text(const sidr_sgp_config& c) {
+    return "sgp " + std::to_string(c.screen) + " " + std::to_string(c.train_steps) + " " +
+           std::to_string(c.batch) + " " + hex32(c.lr) + " " + std::to_string(c.audit) + " " + hex64(c.rho_min) +
+           " " + std::to_string(c.history) + " " + std::to_string(c.n_situations) + " " +
+           std::to_string(c.capture_scenarios) + " " + std::to_string(c.max_cand) + " " +
+           std::to_string(c.model_seed) + " " + std::to_string(c.use_surrogate) + " " +
+           std::to_string(c.selection) + " " + std::to_string(c.target) + " " + hex64(c.screen_fraction) + " " +
+           std::to_string(c.distinct);
+}
+
+// Everything the driver carries from one generation to the next.
+struct SgpState {
+    int64_t next = 0;  // the generation to run next
+    double t_eval = 0.0, t_model = 0.0, elapsed = 0.0;
+    int64_t evals = 0;
+    int64_t screened = 0, fallback = 0;
+    std::vector<double> best_train, held_out, rho, gen_seconds;  // [next]
+    std::vector<double> sit_terms;
+    std::vector<int32_t> sit_nc, sit_ref;
+    std::vector<float> model;  // sidr_mlp_state; empty without a model
+    int64_t model_step = 0;
+    std::vector<std::vector<float>> hist_x;
+    std::vector<std::vector<double>> hist_t;
+    std::string gp_text;  // sidr::gp::state_text
+};
+
+std::string sgp_state_text(const SgpState& st, uint64_t seed, int64_t test_seed, const sidr_instance_desc& inst,
+                           const int64_t* mask, const sidr_sgp_config& sc) {
+    std::string t = std::string(kSgpHeader) + "\n";
+    char hb[32];
+    std::snprintf(hb, sizeof hb, "%016llx", (unsigned long long)instance_hash(inst));
+    t += "run " + std::to_string(seed) + " " + std::to_string(test_seed) + " " + std::to_string(inst.n) + " " +
+         hb + "\n";
+    t += "mask";
+    for (int k = 0; k < 61; k++) t += " " + std::to_string(mask[k]);
+    t += "\n" + sgp_config_text(sc) + "\n";
+    t += "next " + std::to_string(st.next) + "\n";
+    t += "counters " + hex64(st.t_eval) + " " + hex64(st.t_model) + " " + hex64(st.elapsed) + " " +
+         std::to_string(st.evals) + " " + std::to_string(st.screened) + " " + std::to_string(st.fallback) + "\n";
+    put_list(t, "best_train", st.best_train);
+    put_list(t, "held_out", st.held_out);
+    put_list(t, "rho", st.rho);
+    put_list(t, "gen_seconds", st.gen_seconds);
+    put_list(t, "sit_terms", st.sit_terms);
+    put_list(t, "sit_nc", st.sit_nc);
+    put_list(t, "sit_ref", st.sit_ref);
+    t += "model_step " + std::to_string(st.model_step) + "\n";
+    put_list(t, "model", st.model);
+    t += "history " + std::to_string(st.hist_x.size()) + "\n";
+    for (size_t h = 0; h < st.hist_x.size(); h++) {
+        put_list(t, "x", st.hist_x[h]);
+        put_list(t, "t", st.hist_t[h]);
+    }
+    const size_t lines = (size_t)std::count(st.gp_text.begin(), st.gp_text.end(), '\n');
+    t += "gp " + std::to_string(lines) + "\n" + st.gp_text;
+    return t;
+}
+
+sidr_status sgp_state_parse(const std::string& text, uint64_t seed, int64_t test_seed,
+                            const sidr_instance_desc& inst, const int64_t* mask, const sidr_sgp_config& sc,
+                            SgpState& st) {
+    auto bad = [](const std::string& what) { return gp_fail(SIDR_ERR_INVALID, "surrogate checkpoint: " + what); };
+    std::istringstream in(text);
+    std::string line;
+    if (!std::getline(in, line) || line != kSgpHeader) return bad("not a surrogate GP checkpoint of version 1");
+    char hb[32];
+    std::snprintf(hb, sizeof hb, "%016llx", (unsigned long long)instance_hash(inst));
+    if (!std::getline(in, line) ||
+        line != "run " + std::to_string(seed) + " " + std::to_string(test_seed) + " " + std::to_string(inst.n) +
+                    " " + hb)
+        return bad("written for another seed, test seed or instance");
+    std::string want = "mask";
+    for (int k = 0; k < 61; k++) want += " " + std::to_string(mask[k]);
+    if (!std::getline(in, line) || line != want) return bad("written for another terminal mask");
+    if (!std::getline(in, line) || line != sgp_config_text(sc)) return bad("written with other surrogate settings");
+    long long next = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "next %lld", &next) != 1 || next < 1)
+        return bad("malformed generation line");
+    st.next = next;
+    {
+        if (!std::getline(in, line)) return bad("no counters");
+        std::istringstream ls(line);
+        std::string w, a, b, c;
+        long long ev, sc_, fb;
+        if (!(ls >> w >> a >> b >> c >> ev >> sc_ >> fb) || w != "counters" || !unhex64(a, st.t_eval) ||
+            !unhex64(b, st.t_model) || !unhex64(c, st.elapsed) || ev < 0 || sc_ < 0 || fb < 0)
+            return bad("malformed counters");
+        st.evals = ev;
+        st.screened = sc_;
+        st.fallback = fb;
+    }
+    if (!get_list(in, "best_train", st.best_train) || !get_list(in, "held_out", st.held_out) ||
+        !get_list(in, "rho", st.rho) || !get_list(in, "gen_seconds", st.gen_seconds))
+        return bad("malformed per-generation outputs");
+    const size_t g = (size_t)next;
+    if (st.best_train.size() != g || st.held_out.size() != g || st.rho.size() != g || st.gen_seconds.size() != g)
+        return bad("per-generation outputs differ from the generation count");
+    if (!get_list(in, "sit_terms", st.sit_terms) || !get_list(in, "sit_nc", st.sit_nc) ||
+        !get_list(in, "sit_ref", st.sit_ref))
+        return bad("malformed decision situations");
+    long long ms = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "model_step %lld", &ms) != 1 || ms < 0)
+        return bad("malformed model step");
+    st.model_step = ms;
+    if (!get_list(in, "model", st.model)) return bad("malformed model state");
+    long long nh = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "history %lld", &nh) != 1 || nh < 0 || nh > 4096)
+        return bad("malformed history");
+    st.hist_x.assign((size_t)nh, {});
+    st.hist_t.assign((size_t)nh, {});
+    for (long long h = 0; h < nh; h++)
+        if (!get_list(in, "x", st.hist_x[h]) || !get_list(in, "t", st.hist_t[h]) ||
+            st.hist_x[h].size() != st.hist_t[h].size() * SIDR_MLP_INPUTS)
+            return bad("malformed history entry");
+    long long lines = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "gp %lld", &lines) != 1 || lines < 1)
+        return bad("malformed GP header");
+    st.gp_text.clear();
+    for (long long k = 0; k < lines; k++) {
+        if (!std::getline(in, line)) return bad("GP state truncated");
+        st.gp_text += line + "\n";
+    }
+    if (std::getline(in, line) && !line.empty()) return bad("trailing text");
+    if (sc.use_surrogate) {
+        const size_t C = (size_t)sc.max_cand, NS = (size_t)sc.n_situations;
+        if (st.sit_nc.size() != NS || st.sit_ref.size() != NS || st.sit_terms.size() != NS * C * 61)
+            return bad("decision situations of another size");
+        for (size_t j = 0; j < NS; j++)
+            if (st.sit_nc[j] < 2 || st.sit_nc[j] > (int32_t)C || st.sit_ref[j] < 0 || st.sit_ref[j] >= st.sit_nc[j])
+                return bad("decision situation out of range");
+    }
+    return SIDR_OK;
+}
+
+// Writes text to path through a temporary file renamed over it, so that an
+// interrupted write leaves the previous checkpoint in place.
+sidr_status write_atomically(const char* path, const std::string& text) {
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return gp_fail(SIDR_ERR_INVALID, "cannot write " + tmp);
+    const bool ok = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+    if (std::fclose(f) != 0 || !ok) return gp_fail(SIDR_ERR_INVALID, "cannot write " + tmp);
+    if (std::rename(tmp.c_str(), path) != 0) return gp_fail(SIDR_ERR_INVALID, std::string("cannot replace ") + path);
+    return SIDR_OK;
+}
+
+bool read_file(const char* path, std::string& out) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return false;
+    char buf[1 << 16];
+    size_t k;
+    out.clear();
+    while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) out.append(buf, k);
+    std::fclose(f);
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -126,7 +371,18 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                          uint64_t seed, int64_t test_seed, double* best_train, double* held_out,
                          double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
                          sidr_sgp_result* result) {
+    return sidr_sgp_run_resumable(ctx, inst, cfg, sc, terminals_csv, mask, seed, test_seed, nullptr, 0, -1,
+                                  nullptr, best_train, held_out, rho, gen_seconds, best_rule, rule_cap, result);
+}
+
+sidr_status sidr_sgp_run_resumable(sidr_ctx* ctx, const sidr_instance_desc* inst, const sidr_gp_config* cfg,
+                                   const sidr_sgp_config* sc, const char* terminals_csv, const int64_t* mask,
+                                   uint64_t seed, int64_t test_seed, const char* checkpoint_path, int32_t every,
+                                   int32_t stop_after, int32_t* finished, double* best_train, double* held_out,
+                                   double* rho, double* gen_seconds, char* best_rule, int64_t rule_cap,
+                                   sidr_sgp_result* result) {
     std::string err;
+    if (finished) *finished = 0;
     if (!ctx || !inst || !sc || !mask) return gp_fail(SIDR_ERR_INVALID, "null argument");
     if (!valid_config(cfg, err)) return gp_fail(SIDR_ERR_INVALID, err);
     if (sc->n_situations + 8 != SIDR_MLP_INPUTS)
@@ -141,15 +397,50 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
     if (!parse_terminals(terminals_csv, terms, err)) return gp_fail(SIDR_ERR_INVALID, err);
     const int n = inst->n, ps = cfg->population, T = cfg->train_samples, G = cfg->generations;
     const int NS = sc->n_situations, NF = SIDR_MLP_INPUTS;
-    const double t_start = now_s();
+    double t_start = now_s();
     double t_eval = 0.0, t_model = 0.0;
     int64_t evals = 0;
     int screened = 0, fallback = 0;
+    // per-generation outputs of the whole run (a resumed run starts with the checkpoint's)
+    std::vector<double> out_bt, out_ho, out_rho, out_gs;
+
+    // a checkpoint at checkpoint_path: the state after generation next - 1
+    SgpState resume;
+    bool resuming = false;
+    if (checkpoint_path) {
+        std::string text;
+        if (read_file(checkpoint_path, text)) {
+            const sidr_status st = sgp_state_parse(text, seed, test_seed, *inst, mask, *sc, resume);
+            if (st != SIDR_OK) return st;
+            if (resume.next >= G) return gp_fail(SIDR_ERR_INVALID, "surrogate checkpoint: beyond the run's end");
+            resuming = true;
+        }
+    }
 
     Gp gp(*cfg, seed);
     gp.vocab.terminals = terms;
     gp.vocab.n_funcs = cfg->with_rmod ? 7 : 6;
-    gp.init();
+    if (resuming) {
+        std::unique_ptr<Gp> saved;
+        int64_t steps = -1;
+        const sidr_status st = sidr::gp::state_parse(resume.gp_text, saved, steps);
+        if (st != SIDR_OK) return st;
+        if (!same_config(saved->cfg, *cfg) || saved->vocab.terminals != terms)
+            return gp_fail(SIDR_ERR_INVALID, "surrogate checkpoint: written for another GP configuration");
+        gp = *saved;
+        t_eval = resume.t_eval;
+        t_model = resume.t_model;
+        t_start = now_s() - resume.elapsed;
+        evals = resume.evals;
+        screened = (int)resume.screened;
+        fallback = (int)resume.fallback;
+        out_bt = resume.best_train;
+        out_ho = resume.held_out;
+        out_rho = resume.rho;
+        out_gs = resume.gen_seconds;
+    } else {
+        gp.init();
+    }
 
     auto simulate = [&](const std::vector<Rule>& rules, long long block_seed, int S,
                         std::vector<double>& fit) -> sidr_status {
@@ -196,21 +487,85 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
     };
     std::vector<std::vector<float>> hist_x;
     std::vector<std::vector<double>> hist_t;
+    int g0 = 0;
+    if (resuming) {
+        g0 = (int)resume.next;
+        sit_terms.swap(resume.sit_terms);
+        sit_nc.swap(resume.sit_nc);
+        sit_ref.swap(resume.sit_ref);
+        hist_x.swap(resume.hist_x);
+        hist_t.swap(resume.hist_t);
+        if (sc->use_surrogate) {
+            sidr_status st = sidr_mlp_create(sc->device, sc->model_seed, &model);
+            int64_t cnt = 0;
+            if (st == SIDR_OK) st = sidr_mlp_state(model, 0, nullptr, &cnt, nullptr);
+            if (st == SIDR_OK && cnt != (int64_t)resume.model.size())
+                return gp_fail(SIDR_ERR_INVALID, "surrogate checkpoint: model state of another size");
+            if (st == SIDR_OK) st = sidr_mlp_state(model, 1, resume.model.data(), &cnt, &resume.model_step);
+            if (st != SIDR_OK) return st;
+        }
+    }
+    // the state after generation g, for the next call to resume from
+    auto save = [&](int g) -> sidr_status {
+        SgpState cur;
+        cur.next = g + 1;
+        cur.t_eval = t_eval;
+        cur.t_model = t_model;
+        cur.elapsed = now_s() - t_start;
+        cur.evals = evals;
+        cur.screened = screened;
+        cur.fallback = fallback;
+        cur.best_train = out_bt;
+        cur.held_out = out_ho;
+        cur.rho = out_rho;
+        cur.gen_seconds = out_gs;
+        cur.sit_terms = sit_terms;
+        cur.sit_nc = sit_nc;
+        cur.sit_ref = sit_ref;
+        if (model) {
+            int64_t cnt = 0;
+            sidr_status st = sidr_mlp_state(model, 0, nullptr, &cnt, nullptr);
+            cur.model.resize((size_t)cnt);
+            if (st == SIDR_OK) st = sidr_mlp_state(model, 0, cur.model.data(), &cnt, &cur.model_step);
+            if (st != SIDR_OK) return st;
+        }
+        cur.hist_x = hist_x;
+        cur.hist_t = hist_t;
+        cur.gp_text = sidr::gp::state_text(gp, g + 1);
+        return write_atomically(checkpoint_path, sgp_state_text(cur, seed, test_seed, *inst, mask, *sc));
+    };
+    auto copy_out = [&]() {
+        for (size_t g = 0; g < out_bt.size(); g++) {
+            if (best_train) best_train[g] = out_bt[g];
+            if (held_out) held_out[g] = out_ho[g];
+            if (rho) rho[g] = out_rho[g];
+            if (gen_seconds) gen_seconds[g] = out_gs[g];
+        }
+        if (result) {
+            result->eval_seconds = t_eval;
+            result->model_seconds = t_model;
+            result->host_seconds = now_s() - t_start - t_eval - t_model;
+            result->evaluations = evals;
+            result->generations_screened = screened;
+            result->generations_fallback = fallback;
+        }
+    };
 
     std::vector<double> fit;
-    for (int g = 0; g < G; g++) {
+    int ran = 0;  // generations run by this call
+    for (int g = g0; g < G; g++) {
         sidr_status st = simulate(gp.pop, (long long)seed * 10000 + g, T, fit);
         if (st != SIDR_OK) return st;
         size_t bi = 0;
         for (size_t p = 1; p < fit.size(); p++)
             if (fit[p] > fit[bi]) bi = p;
-        if (best_train) best_train[g] = fit[bi];
+        out_bt.push_back(fit[bi]);
         {
             std::vector<double> ho;
             if ((st = simulate({gp.pop[bi]}, test_seed, cfg->test_samples, ho)) != SIDR_OK) return st;
-            if (held_out) held_out[g] = ho[0];
+            out_ho.push_back(ho[0]);
         }
-        if (rho) rho[g] = std::nan("");
+        out_rho.push_back(std::nan(""));
         if (sc->use_surrogate && g == 0) {
             // situations from the first generation's best rule
             Packed pk;
@@ -274,7 +629,7 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
                     aud_x.insert(aud_x.end(), cf.begin() + a * NF, cf.begin() + (a + 1) * NF);
                 }
                 const double r_s = spearman(aud_pred, aud_fit);
-                if (rho) rho[g] = r_s;
+                out_rho[g] = r_s;
                 hist_x.push_back(aud_x);
                 hist_t.push_back(aud_fit);
                 if (r_s >= sc->rho_min) {
@@ -315,7 +670,17 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
             }
             if (!screened_gen) gp.step(fit);
         }
-        if (gen_seconds) gen_seconds[g] = now_s() - t_start;
+        out_gs.push_back(now_s() - t_start);
+        ran++;
+        if (checkpoint_path && g < G - 1) {
+            const bool stop = stop_after >= 0 && ran >= stop_after;
+            if (stop || (every > 0 && (g + 1) % every == 0))
+                if ((st = save(g)) != SIDR_OK) return st;
+            if (stop) {
+                copy_out();
+                return SIDR_OK;  // *finished stays 0
+            }
+        }
     }
     // the last generation's best rule
     size_t bi = 0;
@@ -325,14 +690,8 @@ sidr_status sidr_sgp_run(sidr_ctx* ctx, const sidr_instance_desc* inst, const si
     size_t k = 0;
     prefix_at(gp.pop[bi], k, gp.vocab, text);
     if (best_rule && rule_cap > (int64_t)text.size()) std::memcpy(best_rule, text.c_str(), text.size() + 1);
-    if (result) {
-        result->eval_seconds = t_eval;
-        result->model_seconds = t_model;
-        result->host_seconds = now_s() - t_start - t_eval - t_model;
-        result->evaluations = evals;
-        result->generations_screened = screened;
-        result->generations_fallback = fallback;
-    }
+    copy_out();
+    if (finished) *finished = 1;
     return SIDR_OK;
 }
 

@@ -766,6 +766,37 @@ sidr_status sidr_mlp_param(sidr_mlp* m, int32_t which, int32_t write, float* val
     return SIDR_OK;
 }
 
+sidr_status sidr_mlp_state(sidr_mlp* m, int32_t write, float* state, int64_t* count, int64_t* step) {
+    if (!m) return fail_s(SIDR_ERR_INVALID, "null model");
+    int64_t total = 0;
+    for (int w = 0; w < 6; w++) total += 3 * param_by_index(m, w)->n;
+    if (count) *count = total;
+    if (!state) {
+        if (step) *step = m->step;
+        return SIDR_OK;
+    }
+    DeviceGuard device_guard;
+    SIDR_SCHECK(cudaSetDevice(m->device));
+    SIDR_SCHECK(cudaStreamSynchronize(m->st));
+    float* at = state;
+    for (int w = 0; w < 6; w++) {
+        Param* p = param_by_index(m, w);
+        for (float* dev : {p->p, p->m, p->v}) {
+            if (write) SIDR_SCHECK(cudaMemcpy(dev, at, p->n * 4, cudaMemcpyHostToDevice));
+            else SIDR_SCHECK(cudaMemcpy(at, dev, p->n * 4, cudaMemcpyDeviceToHost));
+            at += p->n;
+        }
+    }
+    if (write) {
+        if (step) m->step = *step;
+        refresh_bf16(m);
+        SIDR_SCHECK(cudaStreamSynchronize(m->st));
+    } else if (step) {
+        *step = m->step;
+    }
+    return SIDR_OK;
+}
+
 sidr_status sidr_mlp_predict(sidr_mlp* m, const float* x, int32_t rows, float* y) {
     if (!m || (rows > 0 && (!x || !y)) || rows < 0) return fail_s(SIDR_ERR_INVALID, "bad argument");
     if (rows == 0) return SIDR_OK;

@@ -52,6 +52,18 @@ def _lib():
                                         C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
                                         C.c_int32, C.c_int32, dp, dp, C.c_char_p, C.c_int64,
                                         C.POINTER(_Result)]
+        vp = C.c_void_p
+        L.sidr_gp_batched_create.argtypes = [vp, C.POINTER(_Inst), C.POINTER(_Cfg), C.c_char_p,
+                                             C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
+                                             C.POINTER(vp)]
+        L.sidr_gp_batched_step.argtypes = [vp, C.c_int32]
+        L.sidr_gp_batched_generation.argtypes = [vp]
+        L.sidr_gp_batched_generation.restype = C.c_int64
+        L.sidr_gp_batched_checkpoint.argtypes = [vp, C.c_char_p, C.c_int64]
+        L.sidr_gp_batched_checkpoint.restype = C.c_int64
+        L.sidr_gp_batched_restore.argtypes = [vp, C.POINTER(_Inst), C.c_char_p, C.POINTER(vp)]
+        L.sidr_gp_batched_finish.argtypes = [vp, dp, dp, C.c_char_p, C.c_int64, C.POINTER(_Result)]
+        L.sidr_gp_batched_destroy.argtypes = [vp]
         L._gp_ready = True
     return L
 
@@ -177,6 +189,73 @@ def run_batched(ctx, terminals: Sequence[str], mask, n_seeds: int, first_seed: i
                                       btr.ctypes.data_as(dp), buf, 1 << 22, C.byref(res)))
     return RunResult(bt, btr, buf.value.decode().splitlines(), res.eval_seconds,
                      res.host_seconds, res.evaluations)
+
+
+class Batched:
+    """The seed-batched run one generation at a time (sidr_gp_batched_*):
+    step, checkpoint to text, restore from it and finish with the results of
+    run_batched.  The context must hold the instance the run evolves on."""
+
+    def __init__(self, ctx, terminals: Sequence[str] = (), mask=None, n_seeds: int = 1,
+                 first_seed: int = 0, test_seed: int = 1000000, _restore: str = None, **cfg):
+        L = _lib()
+        self.ctx = ctx
+        k = _Keep()
+        inst = k.inst(ctx.sd)
+        h = C.c_void_p()
+        if _restore is not None:
+            _check(L.sidr_gp_batched_restore(ctx.h, C.byref(inst), _restore.encode(), C.byref(h)))
+            lines = _restore.splitlines()
+            self.n_seeds = int(lines[1].split()[1])
+            self.generations = int(next(x for x in lines if x.startswith("config ")).split()[2])
+        else:
+            c = config(**cfg)
+            _check(L.sidr_gp_batched_create(ctx.h, C.byref(inst), C.byref(c),
+                                            ",".join(terminals).encode(), k.i64(mask), n_seeds,
+                                            first_seed, test_seed, C.byref(h)))
+            self.n_seeds, self.generations = n_seeds, c.generations
+        self.h = h.value
+
+    @classmethod
+    def restore(cls, ctx, checkpoint: str) -> "Batched":
+        """sidr_gp_batched_restore: a run that continues as the checkpointed one."""
+        return cls(ctx, _restore=checkpoint)
+
+    def step(self, generations: int = 1) -> None:
+        _check(_lib().sidr_gp_batched_step(self.h, generations))
+
+    @property
+    def generation(self) -> int:
+        return int(_lib().sidr_gp_batched_generation(self.h))
+
+    def checkpoint(self) -> str:
+        L = _lib()
+        n = L.sidr_gp_batched_checkpoint(self.h, None, 0)
+        buf = C.create_string_buffer(int(n))
+        L.sidr_gp_batched_checkpoint(self.h, buf, n)
+        return buf.value.decode()
+
+    def finish(self) -> RunResult:
+        bt = np.zeros(self.n_seeds)
+        btr = np.zeros((self.generations, self.n_seeds))
+        buf = C.create_string_buffer(1 << 22)
+        res = _Result()
+        dp = C.POINTER(C.c_double)
+        _check(_lib().sidr_gp_batched_finish(self.h, bt.ctypes.data_as(dp), btr.ctypes.data_as(dp),
+                                             buf, 1 << 22, C.byref(res)))
+        return RunResult(bt, btr, buf.value.decode().splitlines(), res.eval_seconds,
+                         res.host_seconds, res.evaluations)
+
+    def close(self) -> None:
+        if self.h:
+            _lib().sidr_gp_batched_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run_multi(sds, zps, terminals: Sequence[str], masks, n_seeds: int, first_seed: int = 0,

@@ -157,6 +157,12 @@ def _lib2():
         L.sidr_sgp_run.argtypes = [C.c_void_p, C.POINTER(_Inst), C.POINTER(_Cfg), C.POINTER(_SgpCfg),
                                    C.c_char_p, C.POINTER(C.c_int64), C.c_uint64, C.c_int64, _dp, _dp,
                                    _dp, _dp, C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
+        L.sidr_sgp_run_resumable.argtypes = [
+            C.c_void_p, C.POINTER(_Inst), C.POINTER(_Cfg), C.POINTER(_SgpCfg), C.c_char_p,
+            C.POINTER(C.c_int64), C.c_uint64, C.c_int64, C.c_char_p, C.c_int32, C.c_int32,
+            C.POINTER(C.c_int32), _dp, _dp, _dp, _dp, C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
+        L.sidr_mlp_state.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.sidr_sgp_run_multi.argtypes = [C.POINTER(_Inst), _dp, C.c_int32, C.POINTER(_Cfg),
                                          C.POINTER(_SgpCfg), C.c_char_p, C.POINTER(C.c_int64),
                                          C.c_int32, C.c_int64, C.c_int64, C.c_int32, _dp, _dp, _dp,
@@ -209,10 +215,14 @@ def sgp_config(**kw) -> _SgpCfg:
 
 
 def sgp_run(ctx, terminals, mask, seed: int = 0, test_seed: int = 1000000,
-            gp: Optional[dict] = None, **sgp_kw) -> dict:
+            gp: Optional[dict] = None, checkpoint: Optional[str] = None, every: int = 1,
+            stop_after: int = -1, **sgp_kw) -> dict:
     """The surrogate-assisted GP (use_surrogate=0: the same driver breeding
     plainly); per-generation best train fitness, held-out score, audit rho and
-    wall clock."""
+    wall clock.  checkpoint: a file path (sidr_sgp_run_resumable) the run's
+    state is written to every `every` generations and resumed from when it
+    exists; stop_after >= 0 returns after that many generations of this call
+    ("finished" False, outputs of the generations so far filled)."""
     from . import _Keep
     from .gp import config
     L = _lib2()
@@ -224,11 +234,20 @@ def sgp_run(ctx, terminals, mask, seed: int = 0, test_seed: int = 1000000,
     bt, ho, rho, secs = np.zeros(G), np.zeros(G), np.zeros(G), np.zeros(G)
     buf = C.create_string_buffer(1 << 16)
     res = _SgpResult()
-    _check(L.sidr_sgp_run(ctx.h, C.byref(inst), C.byref(c), C.byref(s),
-                          ",".join(terminals).encode(), k.i64(mask), seed, test_seed,
-                          bt.ctypes.data_as(_dp), ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp),
-                          secs.ctypes.data_as(_dp), buf, 1 << 16, C.byref(res)))
-    return {"best_train": bt, "held_out": ho, "rho": rho, "seconds": secs,
+    fin = C.c_int32(1)
+    if checkpoint is None:
+        _check(L.sidr_sgp_run(ctx.h, C.byref(inst), C.byref(c), C.byref(s),
+                              ",".join(terminals).encode(), k.i64(mask), seed, test_seed,
+                              bt.ctypes.data_as(_dp), ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp),
+                              secs.ctypes.data_as(_dp), buf, 1 << 16, C.byref(res)))
+    else:
+        _check(L.sidr_sgp_run_resumable(ctx.h, C.byref(inst), C.byref(c), C.byref(s),
+                                        ",".join(terminals).encode(), k.i64(mask), seed, test_seed,
+                                        str(checkpoint).encode(), every, stop_after, C.byref(fin),
+                                        bt.ctypes.data_as(_dp), ho.ctypes.data_as(_dp),
+                                        rho.ctypes.data_as(_dp), secs.ctypes.data_as(_dp), buf,
+                                        1 << 16, C.byref(res)))
+    return {"finished": bool(fin.value), "best_train": bt, "held_out": ho, "rho": rho, "seconds": secs,
             "best_rule": buf.value.decode(), "eval_seconds": res.eval_seconds,
             "model_seconds": res.model_seconds, "host_seconds": res.host_seconds,
             "evaluations": res.evaluations, "screened": res.generations_screened,

@@ -82,3 +82,58 @@ def test_run_multi_equals_run_batched_per_instance():
         if k < 2:
             assert np.array_equal(bits(auto.best_test[k]), bits(one.best_test)), k
     assert multi.evaluations == 3 * 2 * 32 * 3 * (3 + 1) + 3 * 2 * 8
+
+
+def test_batched_checkpoint_resumes_exactly(tmp_path):
+    """The seed-batched run stepped, checkpointed to a file, restored in a new
+    object (after the first object is gone) and finished gives run_batched's
+    results bit for bit, from a checkpoint taken before any generation, in the
+    middle and after the last; malformed checkpoints and checkpoints of
+    another instance are refused."""
+    w = workload.plain_eval(P=2, S=1)
+    zp = sidr.zstats(w.sd)
+    terms = workload.MENU29
+    n_seeds, first_seed, gens = 2, 3, 5
+    cfg = dict(population=40, generations=gens, train_samples=3, test_samples=12)
+    ctx = sidr.Context(w.sd, zp)
+    try:
+        full = gp.run_batched(ctx, terms, w.mask, n_seeds, first_seed=first_seed, test_seed=99, **cfg)
+        for cut in (0, 2, gens):
+            b = gp.Batched(ctx, terms, w.mask, n_seeds, first_seed=first_seed, test_seed=99, **cfg)
+            b.step(cut)
+            assert b.generation == cut
+            path = tmp_path / f"run{cut}.ckpt"
+            path.write_text(b.checkpoint())
+            b.close()
+            r = gp.Batched.restore(ctx, path.read_text())
+            assert r.generation == cut
+            assert r.checkpoint() == path.read_text()
+            r.step(gens)  # stops at the last generation
+            assert r.generation == gens
+            res = r.finish()
+            r.close()
+            assert np.array_equal(bits(res.best_train), bits(full.best_train)), cut
+            assert np.array_equal(bits(res.best_test), bits(full.best_test)), cut
+            assert res.best_rules == full.best_rules, cut
+            assert res.evaluations == full.evaluations, cut
+        # refusals
+        b = gp.Batched(ctx, terms, w.mask, n_seeds, first_seed=first_seed, test_seed=99, **cfg)
+        b.step(1)
+        text = b.checkpoint()
+        with pytest.raises(sidr.SidrError):
+            b.finish()  # generations left
+        b.close()
+        for broken in (text[: len(text) // 2], text.replace("generation 1\n", "generation 2\n"),
+                       text.replace("sidr-gp-batched-checkpoint 1", "sidr-gp-batched-checkpoint 9"),
+                       text + "extra\n"):
+            with pytest.raises(sidr.SidrError):
+                gp.Batched.restore(ctx, broken)
+    finally:
+        ctx.close()
+    other = workload.gp_generation(P=1, S=1)
+    ctx2 = sidr.Context(other.sd, sidr.zstats(other.sd))
+    try:
+        with pytest.raises(sidr.SidrError):
+            gp.Batched.restore(ctx2, text)
+    finally:
+        ctx2.close()

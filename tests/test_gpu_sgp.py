@@ -268,3 +268,41 @@ def test_sgp_multi_matches_cpu_simulator(oracle):
         test = R.gen_durations(sd.durations, sd.sigma, gp["test_samples"], 1000000)
         cpu = oracle.eval_pairs(sd, zps[k], rules, test, gp["test_samples"], mw.masks[k])
         assert cpu.sum() / gp["test_samples"] == a["held_out"][-1, k, e % 2], e
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.uint64)
+
+
+def test_surrogate_checkpoint_resumes_exactly(setup, tmp_path):
+    """sidr_sgp_run_resumable: a run stopped after two generations (and
+    again after one more), each time resumed from its checkpoint file in a
+    new call, gives the uninterrupted run's outputs bit for bit -- model
+    weights, Adam moments, history window, situations and GP state all come
+    back exactly.  A checkpoint written with other settings is refused."""
+    w, ctx = setup
+    cfg = dict(population=64, generations=5, train_samples=4, test_samples=16)
+    kw = dict(screen=512, audit=32, train_steps=30, batch=128, rho_min=0.3, capture_scenarios=4)
+    full = SG.sgp_run(ctx, workload.MENU29, w.mask, seed=7, test_seed=557, gp=cfg, **kw)
+    path = tmp_path / "sgp.ckpt"
+    part = SG.sgp_run(ctx, workload.MENU29, w.mask, seed=7, test_seed=557, gp=cfg, checkpoint=path,
+                      every=1, stop_after=2, **kw)
+    assert not part["finished"] and path.exists()
+    assert np.array_equal(_bits(part["best_train"][:2]), _bits(full["best_train"][:2]))
+    part = SG.sgp_run(ctx, workload.MENU29, w.mask, seed=7, test_seed=557, gp=cfg, checkpoint=path,
+                      every=1, stop_after=1, **kw)
+    assert not part["finished"]
+    with pytest.raises(sidr.SidrError):  # another seed
+        SG.sgp_run(ctx, workload.MENU29, w.mask, seed=8, test_seed=557, gp=cfg, checkpoint=path, **kw)
+    with pytest.raises(sidr.SidrError):  # another audit size
+        SG.sgp_run(ctx, workload.MENU29, w.mask, seed=7, test_seed=557, gp=cfg, checkpoint=path,
+                   **{**kw, "audit": 16})
+    done = SG.sgp_run(ctx, workload.MENU29, w.mask, seed=7, test_seed=557, gp=cfg, checkpoint=path,
+                      every=1, **kw)
+    assert done["finished"]
+    for key in ("best_train", "held_out", "rho"):
+        assert np.array_equal(_bits(done[key]), _bits(full[key])), key
+    assert done["best_rule"] == full["best_rule"]
+    assert (done["screened"], done["fallback"], done["evaluations"]) == \
+        (full["screened"], full["fallback"], full["evaluations"])
+    assert full["screened"] + full["fallback"] == 4

@@ -212,6 +212,26 @@ sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const double* zp
                                double* best_train, double* held_out, double* rho,
                                char* best_rules, int64_t rules_cap, sidr_sgp_result* result);
 
+/* sidr_sgp_run_multi with checkpoints, as sidr_sgp_run_resumable: every
+ * `every` generations the whole state -- every population's GP session,
+ * each instance's situations, model (weights, Adam moments, step count) and
+ * fitness window, the launch shape, the counters and the per-generation
+ * outputs so far -- goes to checkpoint_path (temporary file, then rename);
+ * a call that finds a checkpoint there resumes from it and gives exactly the
+ * uninterrupted run's outputs (times excepted); one written for other
+ * instances, seeds, masks or settings is refused (SIDR_ERR_INVALID);
+ * stop_after >= 0 ends the call after that many generations with a
+ * checkpoint written (best_rules is filled only by the call that reaches
+ * the last generation); *finished (may be NULL) is 1 when the run is
+ * complete.  A NULL checkpoint_path is sidr_sgp_run_multi. */
+sidr_status sidr_sgp_run_multi_resumable(const sidr_instance_desc* insts, const double* zps, int32_t K,
+                                         const sidr_gp_config* cfg, const sidr_sgp_config* sc,
+                                         const char* terminals_csv, const int64_t* masks, int32_t n_seeds,
+                                         int64_t first_seed, int64_t test_seed, int32_t shape,
+                                         const char* checkpoint_path, int32_t every, int32_t stop_after,
+                                         int32_t* finished, double* best_train, double* held_out, double* rho,
+                                         char* best_rules, int64_t rules_cap, sidr_sgp_result* result);
+
 #ifdef __cplusplus
 }
 #endif

@@ -701,13 +701,172 @@ sidr_status sidr_sgp_run_resumable(sidr_ctx* ctx, const sidr_instance_desc* inst
 // ----------------------------------------------------------------------------
 // Many instances x many seeds (sidr_sgp_run_multi).
 
+namespace {
+
+constexpr const char* kSgpMultiHeader = "sidr-sgp-multi-checkpoint 1";
+
+// The combined driver's state between two generations.
+struct SgpMultiState {
+    int64_t next = 0;
+    double t_eval = 0.0, t_model = 0.0, elapsed = 0.0;
+    int64_t evals = 0, screened = 0, fallback = 0, chosen = -1;
+    std::vector<double> best_train, held_out, rho;  // [next][E]
+    struct Inst {
+        std::vector<double> sit_terms;
+        std::vector<int32_t> sit_nc, sit_ref;
+        std::vector<float> model;
+        int64_t model_step = 0;
+        std::vector<std::vector<float>> hist_x;
+        std::vector<std::vector<double>> hist_t;
+    };
+    std::vector<Inst> inst;       // [K]
+    std::vector<std::string> gp;  // [E] sidr::gp::state_text
+};
+
+std::string multi_run_line(int K, int S, int64_t first_seed, int64_t test_seed, const sidr_instance_desc* insts) {
+    std::string t = "run " + std::to_string(K) + " " + std::to_string(S) + " " + std::to_string(first_seed) + " " +
+                    std::to_string(test_seed);
+    for (int k = 0; k < K; k++) {
+        char hb[32];
+        std::snprintf(hb, sizeof hb, " %d:%016llx", insts[k].n, (unsigned long long)instance_hash(insts[k]));
+        t += hb;
+    }
+    return t;
+}
+
+std::string multi_mask_line(int K, const int64_t* masks) {
+    std::string t = "masks";
+    for (int64_t i = 0; i < (int64_t)K * 61; i++) t += " " + std::to_string(masks[i]);
+    return t;
+}
+
+std::string sgp_multi_text(const SgpMultiState& st, const std::string& run_line, const std::string& mask_line,
+                           const sidr_sgp_config& sc) {
+    std::string t = std::string(kSgpMultiHeader) + "\n" + run_line + "\n" + mask_line + "\n" + sgp_config_text(sc) +
+                    "\n";
+    t += "next " + std::to_string(st.next) + "\n";
+    t += "counters " + hex64(st.t_eval) + " " + hex64(st.t_model) + " " + hex64(st.elapsed) + " " +
+         std::to_string(st.evals) + " " + std::to_string(st.screened) + " " + std::to_string(st.fallback) + " " +
+         std::to_string(st.chosen) + "\n";
+    put_list(t, "best_train", st.best_train);
+    put_list(t, "held_out", st.held_out);
+    put_list(t, "rho", st.rho);
+    for (const SgpMultiState::Inst& u : st.inst) {
+        put_list(t, "sit_terms", u.sit_terms);
+        put_list(t, "sit_nc", u.sit_nc);
+        put_list(t, "sit_ref", u.sit_ref);
+        t += "model_step " + std::to_string(u.model_step) + "\n";
+        put_list(t, "model", u.model);
+        t += "history " + std::to_string(u.hist_x.size()) + "\n";
+        for (size_t h = 0; h < u.hist_x.size(); h++) {
+            put_list(t, "x", u.hist_x[h]);
+            put_list(t, "t", u.hist_t[h]);
+        }
+    }
+    for (const std::string& g : st.gp)
+        t += "gp " + std::to_string(std::count(g.begin(), g.end(), '\n')) + "\n" + g;
+    return t;
+}
+
+sidr_status sgp_multi_parse(const std::string& text, const std::string& run_line, const std::string& mask_line,
+                            const sidr_sgp_config& sc, int K, int E, SgpMultiState& st) {
+    auto bad = [](const std::string& what) {
+        return gp_fail(SIDR_ERR_INVALID, "combined-run checkpoint: " + what);
+    };
+    std::istringstream in(text);
+    std::string line;
+    if (!std::getline(in, line) || line != kSgpMultiHeader) return bad("not a combined-run checkpoint of version 1");
+    if (!std::getline(in, line) || line != run_line) return bad("written for other instances, seeds or test seed");
+    if (!std::getline(in, line) || line != mask_line) return bad("written for other terminal masks");
+    if (!std::getline(in, line) || line != sgp_config_text(sc)) return bad("written with other surrogate settings");
+    long long next = -1;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "next %lld", &next) != 1 || next < 1)
+        return bad("malformed generation line");
+    st.next = next;
+    {
+        if (!std::getline(in, line)) return bad("no counters");
+        std::istringstream ls(line);
+        std::string w, a, b, c;
+        long long ev, sc_, fb, ch;
+        if (!(ls >> w >> a >> b >> c >> ev >> sc_ >> fb >> ch) || w != "counters" || !unhex64(a, st.t_eval) ||
+            !unhex64(b, st.t_model) || !unhex64(c, st.elapsed) || ev < 0 || sc_ < 0 || fb < 0 || ch < -1 ||
+            ch >= SIDR_MULTI_SHAPES)
+            return bad("malformed counters");
+        st.evals = ev;
+        st.screened = sc_;
+        st.fallback = fb;
+        st.chosen = ch;
+    }
+    if (!get_list(in, "best_train", st.best_train) || !get_list(in, "held_out", st.held_out) ||
+        !get_list(in, "rho", st.rho))
+        return bad("malformed per-generation outputs");
+    const size_t want = (size_t)next * (size_t)E;
+    if (st.best_train.size() != want || st.held_out.size() != want || st.rho.size() != want)
+        return bad("per-generation outputs differ from generations x populations");
+    st.inst.assign((size_t)K, {});
+    for (SgpMultiState::Inst& u : st.inst) {
+        if (!get_list(in, "sit_terms", u.sit_terms) || !get_list(in, "sit_nc", u.sit_nc) ||
+            !get_list(in, "sit_ref", u.sit_ref))
+            return bad("malformed decision situations");
+        long long ms = -1;
+        if (!std::getline(in, line) || std::sscanf(line.c_str(), "model_step %lld", &ms) != 1 || ms < 0)
+            return bad("malformed model step");
+        u.model_step = ms;
+        if (!get_list(in, "model", u.model)) return bad("malformed model state");
+        long long nh = -1;
+        if (!std::getline(in, line) || std::sscanf(line.c_str(), "history %lld", &nh) != 1 || nh < 0 ||
+            nh > (1 << 20))
+            return bad("malformed history");
+        u.hist_x.assign((size_t)nh, {});
+        u.hist_t.assign((size_t)nh, {});
+        for (long long h = 0; h < nh; h++)
+            if (!get_list(in, "x", u.hist_x[h]) || !get_list(in, "t", u.hist_t[h]) ||
+                u.hist_x[h].size() != u.hist_t[h].size() * SIDR_MLP_INPUTS)
+                return bad("malformed history entry");
+        if (sc.use_surrogate) {
+            const size_t C = (size_t)sc.max_cand, NS = (size_t)sc.n_situations;
+            if (u.sit_nc.size() != NS || u.sit_ref.size() != NS || u.sit_terms.size() != NS * C * 61)
+                return bad("decision situations of another size");
+            for (size_t j = 0; j < NS; j++)
+                if (u.sit_nc[j] < 2 || u.sit_nc[j] > (int32_t)C || u.sit_ref[j] < 0 || u.sit_ref[j] >= u.sit_nc[j])
+                    return bad("decision situation out of range");
+        }
+    }
+    st.gp.assign((size_t)E, {});
+    for (std::string& g : st.gp) {
+        long long lines = -1;
+        if (!std::getline(in, line) || std::sscanf(line.c_str(), "gp %lld", &lines) != 1 || lines < 1)
+            return bad("malformed GP header");
+        for (long long k = 0; k < lines; k++) {
+            if (!std::getline(in, line)) return bad("GP state truncated");
+            g += line + "\n";
+        }
+    }
+    if (std::getline(in, line) && !line.empty()) return bad("trailing text");
+    return SIDR_OK;
+}
+
+}  // namespace
+
 extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const double* zps, int32_t K,
                                           const sidr_gp_config* cfg, const sidr_sgp_config* sc,
                                           const char* terminals_csv, const int64_t* masks, int32_t n_seeds,
                                           int64_t first_seed, int64_t test_seed, int32_t shape,
                                           double* best_train, double* held_out, double* rho,
                                           char* best_rules, int64_t rules_cap, sidr_sgp_result* result) {
+    return sidr_sgp_run_multi_resumable(insts, zps, K, cfg, sc, terminals_csv, masks, n_seeds, first_seed,
+                                        test_seed, shape, nullptr, 0, -1, nullptr, best_train, held_out, rho,
+                                        best_rules, rules_cap, result);
+}
+
+extern "C" sidr_status sidr_sgp_run_multi_resumable(
+    const sidr_instance_desc* insts, const double* zps, int32_t K, const sidr_gp_config* cfg,
+    const sidr_sgp_config* sc, const char* terminals_csv, const int64_t* masks, int32_t n_seeds, int64_t first_seed,
+    int64_t test_seed, int32_t shape, const char* checkpoint_path, int32_t every, int32_t stop_after,
+    int32_t* finished, double* best_train, double* held_out, double* rho, char* best_rules, int64_t rules_cap,
+    sidr_sgp_result* result) {
     std::string err;
+    if (finished) *finished = 0;
     if (!insts || !zps || !masks || !sc) return gp_fail(SIDR_ERR_INVALID, "null argument");
     if (K < 1 || n_seeds < 1) return gp_fail(SIDR_ERR_INVALID, "K < 1 or n_seeds < 1");
     if ((int64_t)K * n_seeds > 16383) return gp_fail(SIDR_ERR_INVALID, "K * n_seeds > 16383");
@@ -728,10 +887,26 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
     if (!parse_terminals(terminals_csv, terms, err)) return gp_fail(SIDR_ERR_INVALID, err);
     const int S = n_seeds, E = K * S, ps = cfg->population, T = cfg->train_samples, G = cfg->generations;
     const int NS = sc->n_situations, NF = SIDR_MLP_INPUTS;
-    const double t_start = now_s();
+    double t_start = now_s();
     double t_eval = 0.0, t_model = 0.0;
     int64_t evals = 0;
     int screened = 0, fallback = 0, chosen = shape;
+    // per-generation outputs [g][E] of the whole run (a resumed run starts with the checkpoint's)
+    std::vector<double> out_bt, out_ho, out_rho;
+
+    const std::string run_line = multi_run_line(K, S, first_seed, test_seed, insts);
+    const std::string mask_line = multi_mask_line(K, masks);
+    SgpMultiState resume;
+    bool resuming = false;
+    if (checkpoint_path) {
+        std::string text;
+        if (read_file(checkpoint_path, text)) {
+            const sidr_status st = sgp_multi_parse(text, run_line, mask_line, *sc, K, E, resume);
+            if (st != SIDR_OK) return st;
+            if (resume.next >= G) return gp_fail(SIDR_ERR_INVALID, "combined-run checkpoint: beyond the run's end");
+            resuming = true;
+        }
+    }
 
     // population e = k * S + s: instance k, GP seed first_seed + s
     std::vector<Gp> gps;
@@ -740,7 +915,29 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
         gps.emplace_back(*cfg, (uint64_t)(first_seed + e % S));
         gps.back().vocab.terminals = terms;
         gps.back().vocab.n_funcs = cfg->with_rmod ? 7 : 6;
-        gps.back().init();
+        if (resuming) {
+            std::unique_ptr<Gp> saved;
+            int64_t steps = -1;
+            const sidr_status st = sidr::gp::state_parse(resume.gp[e], saved, steps);
+            if (st != SIDR_OK) return st;
+            if (!same_config(saved->cfg, *cfg) || saved->vocab.terminals != terms)
+                return gp_fail(SIDR_ERR_INVALID, "combined-run checkpoint: written for another GP configuration");
+            gps.back() = *saved;
+        } else {
+            gps.back().init();
+        }
+    }
+    if (resuming) {
+        t_eval = resume.t_eval;
+        t_model = resume.t_model;
+        t_start = now_s() - resume.elapsed;
+        evals = resume.evals;
+        screened = (int)resume.screened;
+        fallback = (int)resume.fallback;
+        chosen = resume.chosen >= 0 ? (int)resume.chosen : shape;
+        out_bt = resume.best_train;
+        out_ho = resume.held_out;
+        out_rho = resume.rho;
     }
     auto seed_of = [&](int e) { return (long long)(first_seed + e % S); };
 
@@ -811,6 +1008,82 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
     for (int e = 0; e < E; e++) inst_of_e[e] = e / S;
 
     std::vector<InstanceSurrogate> sur(K);
+    if (resuming) {
+        for (int k = 0; k < K; k++) {
+            SgpMultiState::Inst& u = resume.inst[k];
+            sur[k].sit_terms.swap(u.sit_terms);
+            sur[k].sit_nc.swap(u.sit_nc);
+            sur[k].sit_ref.swap(u.sit_ref);
+            sur[k].hist_x.swap(u.hist_x);
+            sur[k].hist_t.swap(u.hist_t);
+            if (!sc->use_surrogate) continue;
+            sidr_status st = sidr_mlp_create(sc->device, sc->model_seed + (uint64_t)k, &sur[k].model);
+            int64_t cnt = 0;
+            if (st == SIDR_OK) st = sidr_mlp_state(sur[k].model, 0, nullptr, &cnt, nullptr);
+            if (st == SIDR_OK && cnt != (int64_t)u.model.size())
+                return gp_fail(SIDR_ERR_INVALID, "combined-run checkpoint: model state of another size");
+            if (st == SIDR_OK) st = sidr_mlp_state(sur[k].model, 1, u.model.data(), &cnt, &u.model_step);
+            if (st != SIDR_OK) return st;
+        }
+    }
+    // the state after generation g, for the next call to resume from
+    auto save = [&](int g) -> sidr_status {
+        SgpMultiState cur;
+        cur.next = g + 1;
+        cur.t_eval = t_eval;
+        cur.t_model = t_model;
+        cur.elapsed = now_s() - t_start;
+        cur.evals = evals;
+        cur.screened = screened;
+        cur.fallback = fallback;
+        cur.chosen = chosen;
+        cur.best_train = out_bt;
+        cur.held_out = out_ho;
+        cur.rho = out_rho;
+        cur.inst.resize((size_t)K);
+        for (int k = 0; k < K; k++) {
+            SgpMultiState::Inst& u = cur.inst[k];
+            u.sit_terms = sur[k].sit_terms;
+            u.sit_nc = sur[k].sit_nc;
+            u.sit_ref = sur[k].sit_ref;
+            u.hist_x = sur[k].hist_x;
+            u.hist_t = sur[k].hist_t;
+            if (sur[k].model) {
+                int64_t cnt = 0;
+                sidr_status st = sidr_mlp_state(sur[k].model, 0, nullptr, &cnt, nullptr);
+                u.model.resize((size_t)cnt);
+                if (st == SIDR_OK) st = sidr_mlp_state(sur[k].model, 0, u.model.data(), &cnt, &u.model_step);
+                if (st != SIDR_OK) return st;
+            }
+        }
+        for (int e = 0; e < E; e++) cur.gp.push_back(sidr::gp::state_text(gps[e], g + 1));
+        return write_atomically(checkpoint_path, sgp_multi_text(cur, run_line, mask_line, *sc));
+    };
+    auto copy_out = [&]() {
+        for (size_t i = 0; i < out_bt.size(); i++) {
+            if (best_train) best_train[i] = out_bt[i];
+            if (held_out) held_out[i] = out_ho[i];
+            if (rho) rho[i] = out_rho[i];
+        }
+        if (result) {
+            result->eval_seconds = t_eval;
+            result->model_seconds = t_model;
+            result->host_seconds = now_s() - t_start - t_eval - t_model;
+            result->evaluations = evals;
+            result->generations_screened = screened;
+            result->generations_fallback = fallback;
+        }
+    };
+    // after generation g: a checkpoint, and the end of this call when it has run stop_after generations
+    int ran = 0;
+    auto after_generation = [&](int g, bool& stop) -> sidr_status {
+        ran++;
+        stop = false;
+        if (!checkpoint_path || g >= G - 1) return SIDR_OK;
+        stop = stop_after >= 0 && ran >= stop_after;
+        if (stop || (every > 0 && (g + 1) % every == 0)) return save(g);
+        return SIDR_OK;
+    };
     // phenotypes of rules bred by population e, on its instance's situations
     auto features_of = [&](int e, const std::vector<Rule>& rules, std::vector<float>& f) -> sidr_status {
         const int k = e / S;
@@ -826,7 +1099,11 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
     };
 
     std::vector<std::vector<double>> fits;
-    for (int g = 0; g < G; g++) {
+    const int g0 = resuming ? (int)resume.next : 0;
+    for (int g = g0; g < G; g++) {
+        out_bt.resize((size_t)(g + 1) * E);
+        out_ho.resize((size_t)(g + 1) * E);
+        out_rho.resize((size_t)(g + 1) * E);
         std::vector<const std::vector<Rule>*> sets(E);
         for (int e = 0; e < E; e++) sets[e] = &gps[e].pop;
         const std::vector<std::vector<double>> blocks = train_blocks(g);
@@ -838,9 +1115,9 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
         for (int e = 0; e < E; e++) {
             for (size_t p = 1; p < fits[e].size(); p++)
                 if (fits[e][p] > fits[e][best[e]]) best[e] = p;
-            if (best_train) best_train[(size_t)g * E + e] = fits[e][best[e]];
+            out_bt[(size_t)g * E + e] = fits[e][best[e]];
             champions[e] = {gps[e].pop[best[e]]};
-            if (rho) rho[(size_t)g * E + e] = std::nan("");
+            out_rho[(size_t)g * E + e] = std::nan("");
         }
         if (g == G - 1 && best_rules) {  // the last generation's best rules as prefix text
             std::string text;
@@ -862,12 +1139,17 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
             }
             std::vector<std::vector<double>> ho;
             if ((st = simulate(bsets, inst_of_e, tb, cfg->test_samples, ho)) != SIDR_OK) return st;
-            if (held_out)
-                for (int e = 0; e < E; e++) held_out[(size_t)g * E + e] = ho[e][0];
+            for (int e = 0; e < E; e++) out_ho[(size_t)g * E + e] = ho[e][0];
         }
         if (!sc->use_surrogate) {
             if (g < G - 1)
                 for (int e = 0; e < E; e++) gps[e].step(fits[e]);
+            bool stop = false;
+            if ((st = after_generation(g, stop)) != SIDR_OK) return st;
+            if (stop) {
+                copy_out();
+                return SIDR_OK;
+            }
             continue;
         }
         if (g == 0) {
@@ -946,7 +1228,7 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
                 aud_x.insert(aud_x.end(), cf[e].begin() + a * NF, cf[e].begin() + (a + 1) * NF);
             }
             const double r_s = spearman(aud_pred, aud_fit[e]);
-            if (rho) rho[(size_t)g * E + e] = r_s;
+            out_rho[(size_t)g * E + e] = r_s;
             sur[k].hist_x.push_back(std::move(aud_x));
             sur[k].hist_t.push_back(aud_fit[e]);
             if (!(r_s >= sc->rho_min)) {
@@ -982,14 +1264,14 @@ extern "C" sidr_status sidr_sgp_run_multi(const sidr_instance_desc* insts, const
             gps[e].pop.swap(next);
             screened++;
         }
+        bool stop = false;
+        if ((st = after_generation(g, stop)) != SIDR_OK) return st;
+        if (stop) {
+            copy_out();
+            return SIDR_OK;
+        }
     }
-    if (result) {
-        result->eval_seconds = t_eval;
-        result->model_seconds = t_model;
-        result->host_seconds = now_s() - t_start - t_eval - t_model;
-        result->evaluations = evals;
-        result->generations_screened = screened;
-        result->generations_fallback = fallback;
-    }
+    copy_out();
+    if (finished) *finished = 1;
     return SIDR_OK;
 }

@@ -167,6 +167,10 @@ def _lib2():
                                          C.POINTER(_SgpCfg), C.c_char_p, C.POINTER(C.c_int64),
                                          C.c_int32, C.c_int64, C.c_int64, C.c_int32, _dp, _dp, _dp,
                                          C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
+        L.sidr_sgp_run_multi_resumable.argtypes = [
+            C.POINTER(_Inst), _dp, C.c_int32, C.POINTER(_Cfg), C.POINTER(_SgpCfg), C.c_char_p,
+            C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_char_p, C.c_int32,
+            C.c_int32, C.POINTER(C.c_int32), _dp, _dp, _dp, C.c_char_p, C.c_int64, C.POINTER(_SgpResult)]
         L._sgp_ready = True
     return L
 
@@ -256,11 +260,13 @@ def sgp_run(ctx, terminals, mask, seed: int = 0, test_seed: int = 1000000,
 
 def sgp_run_multi(sds, zps, terminals, masks, n_seeds: int, first_seed: int = 0,
                   test_seed: int = 1000000, shape: int = -1, gp: Optional[dict] = None,
+                  checkpoint: Optional[str] = None, every: int = 1, stop_after: int = -1,
                   **sgp_kw) -> dict:
     """sidr_sgp_run_multi: K instances x n_seeds surrogate-screened GP runs,
     one multi-instance launch per generation; per generation and population
     (e = k * n_seeds + s) the best train fitness, held-out score and audit
-    rho, shaped [G, K, n_seeds]."""
+    rho, shaped [G, K, n_seeds].  checkpoint / every / stop_after: as in
+    sgp_run (sidr_sgp_run_multi_resumable)."""
     from . import _Inst, _Keep
     from .gp import config
     L = _lib2()
@@ -276,12 +282,20 @@ def sgp_run_multi(sds, zps, terminals, masks, n_seeds: int, first_seed: int = 0,
     res = _SgpResult()
     cap = 1 << 24
     buf = C.create_string_buffer(cap)
-    _check(L.sidr_sgp_run_multi(insts, z.ctypes.data_as(_dp), K, C.byref(c), C.byref(s),
-                                ",".join(terminals).encode(), m.ctypes.data_as(C.POINTER(C.c_int64)),
-                                n_seeds, first_seed, test_seed, shape, bt.ctypes.data_as(_dp),
-                                ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp), buf, cap,
-                                C.byref(res)))
-    return {"best_train": bt, "held_out": ho, "rho": rho,
+    fin = C.c_int32(1)
+    if checkpoint is None:
+        _check(L.sidr_sgp_run_multi(insts, z.ctypes.data_as(_dp), K, C.byref(c), C.byref(s),
+                                    ",".join(terminals).encode(), m.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    n_seeds, first_seed, test_seed, shape, bt.ctypes.data_as(_dp),
+                                    ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp), buf, cap,
+                                    C.byref(res)))
+    else:
+        _check(L.sidr_sgp_run_multi_resumable(
+            insts, z.ctypes.data_as(_dp), K, C.byref(c), C.byref(s), ",".join(terminals).encode(),
+            m.ctypes.data_as(C.POINTER(C.c_int64)), n_seeds, first_seed, test_seed, shape,
+            str(checkpoint).encode(), every, stop_after, C.byref(fin), bt.ctypes.data_as(_dp),
+            ho.ctypes.data_as(_dp), rho.ctypes.data_as(_dp), buf, cap, C.byref(res)))
+    return {"finished": bool(fin.value), "best_train": bt, "held_out": ho, "rho": rho,
             "best_rules": buf.value.decode().splitlines(), "eval_seconds": res.eval_seconds,
             "model_seconds": res.model_seconds, "host_seconds": res.host_seconds,
             "evaluations": res.evaluations, "screened": res.generations_screened,

@@ -306,3 +306,31 @@ def test_surrogate_checkpoint_resumes_exactly(setup, tmp_path):
     assert (done["screened"], done["fallback"], done["evaluations"]) == \
         (full["screened"], full["fallback"], full["evaluations"])
     assert full["screened"] + full["fallback"] == 4
+
+
+def test_combined_run_checkpoint_resumes_exactly(tmp_path):
+    """sidr_sgp_run_multi_resumable on two instances (50 and 100 customers) x
+    two seeds: stopped after one generation and resumed from the checkpoint
+    file in a new call, the run gives the uninterrupted run's outputs bit for
+    bit (every population's GP session, each instance's model and fitness
+    window come back); a checkpoint of other seeds is refused."""
+    mw = workload.batched_uneven(K=3, rules_per_instance=1, S=1)
+    sds, masks = mw.sds[1:3], mw.masks[1:3]
+    zps = [sidr.zstats(sd) for sd in sds]
+    gp, sg = _small_cfg()
+    kw = dict(first_seed=2, test_seed=31, shape=0, gp=gp, **sg)
+    full = SG.sgp_run_multi(sds, zps, workload.MENU29, masks, 2, **kw)
+    path = tmp_path / "multi.ckpt"
+    part = SG.sgp_run_multi(sds, zps, workload.MENU29, masks, 2, checkpoint=path, every=1,
+                            stop_after=1, **kw)
+    assert not part["finished"] and path.exists()
+    with pytest.raises(sidr.SidrError):
+        SG.sgp_run_multi(sds, zps, workload.MENU29, masks, 2, checkpoint=path,
+                         **{**kw, "first_seed": 3})
+    done = SG.sgp_run_multi(sds, zps, workload.MENU29, masks, 2, checkpoint=path, every=2, **kw)
+    assert done["finished"]
+    for key in ("best_train", "held_out", "rho"):
+        assert np.array_equal(_bits(done[key]), _bits(full[key])), key
+    assert done["best_rules"] == full["best_rules"]
+    assert (done["screened"], done["fallback"], done["evaluations"]) == \
+        (full["screened"], full["fallback"], full["evaluations"])

@@ -63,6 +63,10 @@ def parse_args():
     ap.add_argument("--P", type=int, default=1024)
     ap.add_argument("--S", type=int, default=500)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="block shape of the benchmark generation (index into sidr.Batch.SHAPES); "
+                         "default: tuned on every 16th rule")
+    ap.add_argument("--evolved-shape", type=int, default=-1, help="the same for the evolved leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--evolved-steps", type=int, default=3,
@@ -101,6 +105,9 @@ def parse_args():
                     help="instead of one independent generation per GPU, run the benchmark GP with "
                          "every generation's rules sharded over the ranks (fitness all_gather, "
                          "strong scaling): W untimed generations, then K timed ones")
+    ap.add_argument("--sampling", action="store_true",
+                    help="also time scenario sampling on the GPU (sidr_gen_durations_device) against "
+                         "the host sampler on the benchmark's block and the large run's block")
     ap.add_argument("--large", action="store_true",
                     help="also run the large combined run's driver (sidr_sgp_run_multi): 10 instances "
                          "of 288 customers x 30 GP seeds x 4096 rules, surrogate screening 16384 "
@@ -135,7 +142,8 @@ def config_of(P, S, world):
                         f"RHH depth 2-8",
             "rules": P, "scenarios": S, "customers": 100, "vehicles": 3, "horizon": 1000,
             "terminals": 29, "parallelism": f"{world} independent generations (one per GPU)",
-            "l2": "flushed between timed steps (256 MiB device write outside the events)"}
+            "l2": "flushed between timed steps outside the events: a 256 MiB device write, then a "
+                  "256 MiB read that moves the written lines out of L2"}
 
 
 # --------------------------------------------------------------- clocks
@@ -322,7 +330,7 @@ def measured_hbm_gbs():
 
 
 def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, world, e2e_on=True,
-            clocks=None):
+            clocks=None, shape=-1):
     """Device time of `steps` evaluations of workload w (resident batch, L2
     flushed between steps), the end-to-end rate through sidr_evaluate with host
     buffers, and the FP64 op-model roofline of the evaluator launch."""
@@ -336,12 +344,16 @@ def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, wor
     torch.cuda.synchronize()
     counts = batch.counts()
     batch.set_counting(False)
-    # block shape timed on every 16th rule (untimed); the same shape for the
-    # device-timed steps and the end-to-end calls
-    shape, shape_ms = batch.autotune_sampled(stride=16, reps=1)
+    # block shape timed on every 16th rule (untimed) unless given; the same
+    # shape for the device-timed steps and the end-to-end calls
+    if shape >= 0:
+        batch.set_shape(shape)
+        shape_ms = None
+    else:
+        shape, shape_ms = batch.autotune_sampled(stride=16, reps=1)
     ctx.set_shape(shape)
     for _ in range(warmup):
-        flush.zero_()
+        flush()
         batch.run(sh)
     torch.cuda.synchronize()
     ref_out = batch.read()
@@ -354,7 +366,7 @@ def measure(ctx, w, steps, warmup, stream, flush, peak_ops, allmax, barrier, wor
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(steps)]
     for e0, e1 in ev:
-        flush.zero_()
+        flush()
         e0.record(stream)
         batch.run(sh)
         e1.record(stream)
@@ -439,10 +451,18 @@ def run_ours(args, rank, world, local):
     stream = torch.cuda.Stream()  # the launching stream: events are recorded on it
     torch.cuda.set_stream(stream)
     peak_ops = sidr.fp64_peak(local)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush_w = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush_r = torch.ones(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush():
+        # the write evicts the workload's lines from L2; the read then replaces the
+        # written (dirty) lines with clean ones, so their write-back falls here
+        # and not inside the next step
+        flush_w.zero_()
+        flush_r.sum()
 
     r = measure(ctx, w, args.steps, args.warmup, stream, flush, peak_ops, allmax, barrier, world,
-                e2e_on=not args.no_e2e, clocks=ClockSampler(gpu_uuid(local)))
+                e2e_on=not args.no_e2e, clocks=ClockSampler(gpu_uuid(local)), shape=args.shape)
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -456,7 +476,7 @@ def run_ours(args, rank, world, local):
         from sidr import workload as W
         we = W.evolved(49, P=args.P, S=args.S)
         re = measure(ctx, we, args.evolved_steps, 3, stream, flush, peak_ops, allmax, barrier,
-                     world, e2e_on=not args.no_e2e)
+                     world, e2e_on=not args.no_e2e, shape=args.evolved_shape)
         line["evolved"] = {"workload": f"evolved_gen49: generation 49 of the benchmark GP run "
                                        f"(seed 0), {args.P} rules x {args.S} scenarios, same "
                                        f"instance and scenarios", "value": re["value"],
@@ -482,6 +502,8 @@ def run_ours(args, rank, world, local):
         line["campaign"] = campaign_leg()
     if args.large and rank == 0:
         line["large"] = large_leg(args)
+    if args.sampling and rank == 0:
+        line["sampling"] = sampling_leg()
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -577,6 +599,42 @@ def multi_leg(args, stream):
             "chosen_shape_per_class": [list(sidr.Multi.SHAPES[x]) if x >= 0 else None for x in chosen],
             "host_prep_seconds": prep,
             "spot_check_pairs": pairs, "spot_check_mismatches": mism, "per_size_class": classes}
+
+
+def sampling_leg():
+    """Scenario sampling (gen_durations) on one host core against the GPU
+    sampler, which is bit-identical: the benchmark's block (500 scenarios x
+    100 customers) and one block of the large combined run (2000 scenarios x
+    288 customers).  Host: wall clock of sidr_gen_durations; GPU: wall clock of
+    sidr_gen_durations_device with the result in host memory (transfers and the
+    host's recomputation of unsettled pairs included) and in device memory."""
+    import numpy as np
+    import torch
+    from sidr import gp as GP
+    from sidr import workload as W
+    res = {}
+    for name, sd, S in (("benchmark_block", W.gp_generation(P=1, S=1).sd, 500),
+                        ("large_run_block", W.large_combined(K=1, seeds=1, rules_per_seed=1, S=1).sds[0], 2000)):
+        d = sd.durations
+        GP.gen_durations_device(d, 0.2, 8, 1)  # warm-up
+        t0 = time.perf_counter()
+        host = GP.gen_durations(d, 0.2, S, 1)
+        t_host = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        dev, st = GP.gen_durations_device(d, 0.2, S, 1)
+        t_dev = time.perf_counter() - t0
+        out = torch.empty((S, len(d)), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        GP.gen_durations_device(d, 0.2, S, 1, out_ptr=out.data_ptr())
+        t_dres = time.perf_counter() - t0
+        same = bool(np.array_equal(host.view(np.uint64), dev.view(np.uint64))) and \
+            bool(np.array_equal(host.view(np.uint64), out.cpu().numpy().view(np.uint64)))
+        res[name] = {"scenarios": S, "customers": len(d), "host_ms": 1e3 * t_host,
+                     "gpu_to_host_ms": 1e3 * t_dev, "gpu_resident_ms": 1e3 * t_dres,
+                     "pairs": st["pairs"], "pairs_left_to_host": st["host_pairs"],
+                     "bit_identical": same}
+    return res
 
 
 def large_leg(args):

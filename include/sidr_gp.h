@@ -155,6 +155,32 @@ sidr_status sidr_gp_run_multi(const sidr_instance_desc* insts, const double* zps
 sidr_status sidr_gen_durations(int32_t n, const double* durations, double sigma, int32_t S,
                                int64_t base_seed, double* out);
 
+/* gen_durations on the GPU (the reference samples on the host:
+ * engine/sim_host.hpp:50-58 with engine/rng.hpp:27-147), bit-identical to
+ * sidr_gen_durations.  One warp per scenario runs the MT19937 seeding and
+ * refresh in shared memory; the Box-Muller log, cos and sin are computed in
+ * double-double arithmetic, and a pair whose C-library result those values
+ * do not settle (a few percent) is recomputed on the host with the C library
+ * after the kernel.  out: [S][n] doubles in host memory (out_on_device = 0)
+ * or in the device memory of `device` (1).  stats (may be NULL): Box-Muller
+ * pairs drawn and pairs recomputed on the host.  The call allocates its
+ * device scratch and waits for its work. */
+typedef struct sidr_sample_stats {
+    int64_t pairs;
+    int64_t host_pairs;
+} sidr_sample_stats;
+sidr_status sidr_gen_durations_device(int32_t device, int32_t n, const double* durations, double sigma,
+                                      int32_t S, int64_t base_seed, double* out, int32_t out_on_device,
+                                      sidr_sample_stats* stats);
+/* Diagnostic of the sampler (no reference counterpart): the double-double
+ * log(1 - u2[i]), sin(2 pi u1[i]) and cos(2 pi u1[i]) it settles pairs with
+ * and the second C-library candidate each names (the value itself when it
+ * names one), out[9 i ..] = {log hi, lo, second, sin hi, lo, second, cos hi,
+ * lo, second}, computed by the device build (on_device = 1, on `device`) or
+ * the host build (0) of the same code; the two must agree bit for bit. */
+sidr_status sidr_sample_dd_eval(int32_t device, const double* u1, const double* u2, int32_t k,
+                                int32_t on_device, double* out);
+
 #ifdef __cplusplus
 }
 #endif

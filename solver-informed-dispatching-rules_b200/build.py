@@ -28,10 +28,11 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC
            "-Xptxas", "-v"]
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall"]
 
-CU_SOURCES = ["sidr_capi.cu", "sidr_surrogate.cu"]
+CU_SOURCES = ["sidr_capi.cu", "sidr_surrogate.cu", "sidr_sample.cu"]
 CPP_SOURCES = ["sidr_host.cpp", "sidr_gp.cpp", "sidr_campaign.cpp", "sidr_sgp.cpp"]
 HEADERS = ["sidr_internal.hpp", "sidr_kernel.cuh", "sidr_host.hpp", "sidr_libm.cuh", "sidr_exp_table.h",
-           "sidr_gp_core.hpp", "sidr_mlp.cuh", "sidr_sgp_select.hpp", "sidr_device.hpp"]
+           "sidr_gp_core.hpp", "sidr_mlp.cuh", "sidr_sgp_select.hpp", "sidr_device.hpp",
+           "sidr_sample.cuh", "sidr_sample_consts.h"]
 PUBLIC_HEADERS = ["sidr.h", "sidr_gp.h", "sidr_campaign.h", "sidr_surrogate.h"]
 
 

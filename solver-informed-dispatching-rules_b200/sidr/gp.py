@@ -26,6 +26,10 @@ class _Result(C.Structure):
                 ("evaluations", C.c_int64)]
 
 
+class _SampleStats(C.Structure):
+    _fields_ = [("pairs", C.c_int64), ("host_pairs", C.c_int64)]
+
+
 def _lib():
     L = load()
     if not getattr(L, "_gp_ready", False):
@@ -52,6 +56,10 @@ def _lib():
                                         C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
                                         C.c_int32, C.c_int32, dp, dp, C.c_char_p, C.c_int64,
                                         C.POINTER(_Result)]
+        L.sidr_gen_durations_device.argtypes = [C.c_int32, C.c_int32, dp, C.c_double, C.c_int32,
+                                                C.c_int64, C.c_void_p, C.c_int32,
+                                                C.POINTER(_SampleStats)]
+        L.sidr_sample_dd_eval.argtypes = [C.c_int32, dp, dp, C.c_int32, C.c_int32, dp]
         vp = C.c_void_p
         L.sidr_gp_batched_create.argtypes = [vp, C.POINTER(_Inst), C.POINTER(_Cfg), C.c_char_p,
                                              C.POINTER(C.c_int64), C.c_int32, C.c_int64, C.c_int64,
@@ -159,6 +167,39 @@ def gen_durations(durations, sigma: float, S: int, base_seed: int) -> np.ndarray
     dp = C.POINTER(C.c_double)
     _check(_lib().sidr_gen_durations(len(d), d.ctypes.data_as(dp), sigma, S, base_seed,
                                      out.ctypes.data_as(dp)))
+    return out
+
+
+def gen_durations_device(durations, sigma: float, S: int, base_seed: int, device: int = 0,
+                         out_ptr: int = 0):
+    """sidr_gen_durations_device: gen_durations on the GPU, bit-identical to
+    gen_durations.  Returns ([S, n] array, stats dict); with out_ptr (a device
+    pointer to S * n doubles on `device`) the durations are written there and
+    the array is None."""
+    d = np.ascontiguousarray(durations, dtype=np.float64)
+    st = _SampleStats()
+    dp = C.POINTER(C.c_double)
+    if out_ptr:
+        _check(_lib().sidr_gen_durations_device(device, len(d), d.ctypes.data_as(dp), sigma, S, base_seed,
+                                                C.c_void_p(out_ptr), 1, C.byref(st)))
+        out = None
+    else:
+        out = np.zeros((S, len(d)))
+        _check(_lib().sidr_gen_durations_device(device, len(d), d.ctypes.data_as(dp), sigma, S, base_seed,
+                                                C.c_void_p(out.ctypes.data), 0, C.byref(st)))
+    return out, {"pairs": st.pairs, "host_pairs": st.host_pairs}
+
+
+def sample_dd_eval(u1, u2, on_device: bool = True, device: int = 0) -> np.ndarray:
+    """sidr_sample_dd_eval: [k, 9] = log hi, lo, second candidate, sin hi, lo,
+    second, cos hi, lo, second of the sampler's double-double evaluation, by
+    the device or the host build."""
+    a = np.ascontiguousarray(u1, dtype=np.float64)
+    b = np.ascontiguousarray(u2, dtype=np.float64)
+    out = np.zeros((len(a), 9))
+    dp = C.POINTER(C.c_double)
+    _check(_lib().sidr_sample_dd_eval(device, a.ctypes.data_as(dp), b.ctypes.data_as(dp), len(a),
+                                      int(on_device), out.ctypes.data_as(dp)))
     return out
 
 

@@ -140,7 +140,8 @@ void sidr_gp_batched_destroy(sidr_gp_batched* b);
  * per generation (sidr_multi_*), each on its own instance and train block.
  * Per instance the results equal sidr_gp_run_batched's on that instance
  * alone.  shape: the launch's block shape (0 .. SIDR_MULTI_SHAPES-1), or -1 to
- * autotune on the first launch and keep the choice.  Each generation builds
+ * choose it on the first launch (sidr_multi_autotune_sampled on every 16th
+ * rule) and keep the choice.  Each generation builds
  * its batch anew (instance tables included, on the host).
  *   best_test[K*n_seeds]           held-out mean of each population's best rule
  *   best_train[gens*K*n_seeds]     index (gen*K + k)*n_seeds + s

@@ -596,7 +596,7 @@ sidr_status sidr_gp_run_multi(const sidr_instance_desc* insts, const double* zps
         sidr_multi* m = nullptr;
         sidr_status st = sidr_multi_create(d.data(), z.data(), Q, &r, owner.data(), flat.data(),
                                            (int64_t)flat.size(), offs.data(), Tn, mk.data(), device, &m);
-        if (st == SIDR_OK) st = chosen < 0 ? sidr_multi_autotune(m, 1, &chosen, nullptr) : sidr_multi_set_shape(m, chosen);
+        if (st == SIDR_OK) st = chosen < 0 ? sidr_multi_autotune_sampled(m, 1, 16, &chosen, nullptr) : sidr_multi_set_shape(m, chosen);
         if (st == SIDR_OK) st = sidr_multi_run(m, nullptr);
         if (st == SIDR_OK) st = sidr_multi_read(m, out.data());
         const std::string why = st == SIDR_OK ? std::string() : std::string(sidr_last_error());

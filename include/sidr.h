@@ -84,6 +84,15 @@ int sidr_version(void);
  * with the same libm as the reference. */
 sidr_status sidr_zstats(const sidr_instance_desc* inst, double zp[10]);
 
+/* Diagnostic, host only (no reference counterpart): builds the instance's
+ * tables and checks ATRISK's per-pair step functions -- the outcome of
+ * engine/sim_terms.hpp:225-257's term (+0, s_j, or erf needed) as a function
+ * of the candidate's finish time, which the kernel looks up -- against the
+ * classification itself at every switch point, its neighbours and random
+ * times.  *checked: points checked; *mismatches: must be 0. */
+sidr_status sidr_atrisk_table_check(const sidr_instance_desc* inst, int32_t seed, int64_t* checked,
+                                    int64_t* mismatches);
+
 /* FactoryContext(sd, zp) (engine/factory.cuh:129-137): copies the instance to
  * device `device` once, with the per-instance lookup tables the kernels use. */
 sidr_status sidr_ctx_create(const sidr_instance_desc* inst, const double zp[10], int device,

@@ -645,6 +645,20 @@ sidr_status sidr_zstats(const sidr_instance_desc* d, double zp[10]) {
     return SIDR_OK;
 }
 
+sidr_status sidr_atrisk_table_check(const sidr_instance_desc* d, int32_t seed, int64_t* checked,
+                                    int64_t* mismatches) {
+    if (!d || !checked || !mismatches) return fail(SIDR_ERR_INVALID, "null argument");
+    HostInstance h;
+    std::string e = build_instance(d->n, d->m, d->tmax, d->scores, d->durations, d->open_t,
+                                   d->close_t, d->dist, d->dist_to_depot, h, true);
+    if (!e.empty()) return fail(SIDR_ERR_INVALID, e);
+    long long c = 0, b = 0;
+    atrisk_table_check(h, seed, c, b);
+    *checked = c;
+    *mismatches = b;
+    return SIDR_OK;
+}
+
 sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], int device,
                             sidr_ctx** out) {
     if (!out) return fail(SIDR_ERR_INVALID, "out is null");
@@ -716,6 +730,8 @@ sidr_status sidr_ctx_create(const sidr_instance_desc* d, const double zp[10], in
         {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
         {h.DP.data(), h.DP.size() * 8, (const void**)&I.DP},
         {h.CU.data(), h.CU.size() * 8, (const void**)&I.CU},
+        {h.TK.data(), h.TK.size() * 8, (const void**)&I.TK},
+        {h.TC.data(), h.TC.size(), (const void**)&I.TC},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
         {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},
@@ -1126,6 +1142,8 @@ extern "C" sidr_status sidr_evaluate_static(const sidr_instance_desc* d, const d
         {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD, 0},
         {h.DP.data(), h.DP.size() * 8, (const void**)&I.DP, 0},
         {h.CU.data(), h.CU.size() * 8, (const void**)&I.CU, 0},
+        {h.TK.data(), h.TK.size() * 8, (const void**)&I.TK, 0},
+        {h.TC.data(), h.TC.size(), (const void**)&I.TC, 0},
         {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord, 0},
         {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF, 0},
         {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG, 0},
@@ -1452,6 +1470,8 @@ sidr_status sidr_multi_create(const sidr_instance_desc* insts, const double* zps
             {h.GD.data(), h.GD.size() * 8, (const void**)&I.GD},
             {h.DP.data(), h.DP.size() * 8, (const void**)&I.DP},
             {h.CU.data(), h.CU.size() * 8, (const void**)&I.CU},
+            {h.TK.data(), h.TK.size() * 8, (const void**)&I.TK},
+        {h.TC.data(), h.TC.size(), (const void**)&I.TC},
             {h.ord.data(), h.ord.size() * 2, (const void**)&I.ord},
             {h.sF.data(), h.sF.size() * 8, (const void**)&I.sF},
             {h.sG.data(), h.sG.size() * 8, (const void**)&I.sG},

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <thread>
 
 namespace sidr {
 
@@ -138,7 +139,128 @@ double z_atrisk(const HostInstance& h, int c) {
     return acc;
 }
 
+// ATRISK's classification of the pair (candidate c, customer j) when the
+// candidate finishes at f: the kernel's at_risk_compute, operation for
+// operation.  0: the term is +0 (both factors exactly 1); 1: the term is
+// s_j (a factor exactly 0); 2: a factor needs erf.
+int atrisk_outcome(const HostInstance& h, int c, int j, double f) {
+    const double sd_c = kSigma * h.durations[c];
+    const double hw = 8.5 * sd_c, lw = -8.5 * sd_c;
+    const double cj = h.close_t[j], oj = h.open_t[j], dj = h.durations[j], ej = h.d2d[j];
+    const double marr = f + D(h, c + 1, j + 1);
+    const double dw = cj - marr;
+    const bool sdv = sd_c > 1e-9;
+    const bool ew = sdv && !(dw >= hw) && !(dw <= lw);
+    const bool pw1 = sdv ? dw >= hw : marr <= cj;
+    const bool late = marr > oj;
+    const double mst = late ? marr : oj;
+    const double pv = late ? h.P1[(size_t)c * h.n + j] : h.P0[j];
+    const double mb = mst + dj + ej;
+    const double db = h.tmax - mb;
+    const bool pvv = pv >= 0.0;
+    const double hb = 8.5 * pv, lb = -8.5 * pv;
+    const bool eb = (ew || pw1) && pvv && !(db >= hb) && !(db <= lb);
+    const bool pb1 = pvv ? db >= hb : mb <= h.tmax;
+    if (ew || eb) return 2;
+    return (pw1 && pb1) ? 0 : 1;
+}
+
+// The outcome of a pair as a step function of f.  Every test above is a
+// monotone function of f (each operation is round-to-nearest and monotone),
+// and so are the late branch's tests taken on their own; the outcome only
+// changes where one of them does.  Those points are found by bisection; the
+// outcome between them is taken at one point of each interval.  Stored as
+// {k0, k1} and a code byte: interval i is (k_{i-1}, k_i] (k_{-1} = -inf,
+// k_2 = +inf, unused points +inf) and its outcome is bits 2i..2i+1 of the
+// byte; when more than three intervals remain after merging equal neighbours,
+// the last kept interval is given outcome 2 (the kernel then classifies the
+// pair itself).
+void atrisk_steps(const HostInstance& h, int c, int j, double* ks_out, uint8_t* code_out) {
+    const double t = D(h, c + 1, j + 1);
+    const double sd_c = kSigma * h.durations[c];
+    const double hw = 8.5 * sd_c, lw = -8.5 * sd_c;
+    const double cj = h.close_t[j], oj = h.open_t[j], dj = h.durations[j], ej = h.d2d[j];
+    const double p1 = h.P1[(size_t)c * h.n + j];
+    const bool sdv = sd_c > 1e-9;
+    std::vector<double> pts;
+    auto add_pt = [&](double k) {
+        if (k > -DBL_MAX && k < DBL_MAX) pts.push_back(k);
+    };
+    // p_win exactly 1 (a down-set), exactly 0 (an up-set)
+    add_pt(largest_true([&](double f) {
+        const double m = f + t;
+        return sdv ? (cj - m) >= hw : m <= cj;
+    }));
+    if (sdv) add_pt(largest_true([&](double f) { return !((cj - (f + t)) <= lw); }));
+    // late arrival (an up-set) and, on the late branch, p_bud exactly 1 (down) or 0 (up)
+    add_pt(largest_true([&](double f) { return !((f + t) > oj); }));
+    add_pt(largest_true([&](double f) {
+        const double mb = (f + t) + dj + ej;
+        return p1 >= 0.0 ? (h.tmax - mb) >= 8.5 * p1 : mb <= h.tmax;
+    }));
+    if (p1 >= 0.0) add_pt(largest_true([&](double f) { return !((h.tmax - ((f + t) + dj + ej)) <= -8.5 * p1); }));
+    std::sort(pts.begin(), pts.end());
+    pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
+    // outcome of each interval at one of its points (interval i ends at pts[i],
+    // the last one at +inf), then equal neighbours merged
+    std::vector<int> codes;
+    std::vector<double> ends;  // right end of each merged interval
+    for (size_t i = 0; i <= pts.size(); i++) {
+        const double end = i < pts.size() ? pts[i] : INFINITY;
+        const double rep = i < pts.size() ? pts[i] : (pts.empty() ? 0.0 : std::nextafter(pts.back(), INFINITY));
+        const int o = atrisk_outcome(h, c, j, rep);
+        if (!codes.empty() && codes.back() == o) {
+            ends.back() = end;
+        } else {
+            codes.push_back(o);
+            ends.push_back(end);
+        }
+    }
+    std::vector<double> ks(ends.begin(), ends.end() - 1);  // the last interval ends at +inf
+    if (codes.size() > 3) {
+        codes.resize(3);
+        codes[2] = 2;
+        ks.resize(2);
+    }
+    uint32_t code = 0;
+    for (size_t i = 0; i < codes.size(); i++) code |= (uint32_t)codes[i] << (2 * i);
+    for (int i = 0; i < 2; i++) ks_out[i] = i < (int)ks.size() ? ks[i] : INFINITY;
+    *code_out = (uint8_t)code;
+}
+
 }  // namespace
+
+void atrisk_table_check(const HostInstance& h, int seed, long long& checked, long long& bad) {
+    checked = bad = 0;
+    uint64_t x = 0x9e3779b97f4a7c15ull * (uint64_t)(seed + 1);
+    auto rnd = [&]() {  // splitmix64 in [0, 1)
+        x += 0x9e3779b97f4a7c15ull;
+        uint64_t z = x;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const int n = h.n;
+    for (int c = 0; c < n; c++)
+        for (int j = 0; j < n; j++) {
+            if (c == j) continue;
+            const double* ta = &h.TK[2 * ((size_t)j * n + c)];
+            std::vector<double> fs = {0.0};
+            for (int k = 0; k < 2; k++)
+                if (std::isfinite(ta[k]))
+                    for (double v : {std::nextafter(ta[k], -INFINITY), ta[k], std::nextafter(ta[k], INFINITY)})
+                        if (v >= 0.0) fs.push_back(v);
+            for (int r = 0; r < 6; r++) fs.push_back(rnd() * 2.0 * h.tmax);
+            const int codes = h.TC[(size_t)j * n + c];
+            for (double f : fs) {
+                const int iv = (f > ta[0]) + (f > ta[1]);
+                const int code = (codes >> (2 * iv)) & 3;
+                checked++;
+                if (code != 2 && code != atrisk_outcome(h, c, j, f)) bad++;
+            }
+        }
+}
 
 std::string build_instance(int n, int m, double tmax, const double* scores,
                            const double* durations, const double* open_t, const double* close_t,
@@ -229,6 +351,21 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
             h.DP[t] = D(h, c + 1, j + 1);
             h.DP[t + 1] = h.P1[(size_t)c * n + j];
         }
+    // ATRISK's step functions at pair index j*n + c, candidates split over threads
+    h.TK.assign(2 * (size_t)n * n, 0.0);
+    h.TC.assign((size_t)n * n, 0);
+    {
+        const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), (n + 7) / 8));
+        std::vector<std::thread> pool;
+        for (int w = 0; w < nt; w++)
+            pool.emplace_back([&, w] {
+                for (int c = w; c < n; c += nt)
+                    for (int j = 0; j < n; j++)
+                        if (j != c)
+                            atrisk_steps(h, c, j, &h.TK[2 * ((size_t)j * n + c)], &h.TC[(size_t)j * n + c]);
+            });
+        for (std::thread& th : pool) th.join();
+    }
     // Per-origin neighbour lists by (R desc, index asc), rows padded to a
     // multiple of 4 entries; bit 14 of an index marks a coincident location.
     // cnt_pos / cnt_gm1 = how many leading entries have a ratio > 0 / > -1.

@@ -17,6 +17,8 @@ struct HostInstance {
     std::vector<uint32_t> zlt, zle;
     std::vector<double> FR, GD, DP;                                      // neighbour-major
     std::vector<double> CU;                                              // per customer
+    std::vector<double> TK;                                              // ATRISK step functions:
+    std::vector<uint8_t> TC;                                             // switch points, codes
     int ns = 0;                                                          // sorted row stride
     std::vector<int16_t> ord;                                            // sorted lists
     std::vector<double> sF, sG;
@@ -32,6 +34,12 @@ std::string build_instance(int n, int m, double tmax, const double* scores,
                            const double* durations, const double* open_t, const double* close_t,
                            const double* dist, const double* d2d, HostInstance& out,
                            bool tables = true);
+
+// ATRISK's step-function table against the classification it stands for: at
+// f = 0, at each switch point and its two neighbours, and at random f in
+// [0, 2 tmax), every pair's table outcome other than "classify in full" must
+// equal the classification.  Counts the checks and the mismatches.
+void atrisk_table_check(const HostInstance& h, int seed, long long& checked, long long& bad);
 
 // zp_of / zstats on the host (engine/sim_host.hpp:96-105,
 // engine/sim_core.hpp:277-312).

@@ -40,6 +40,15 @@ constexpr int kOrdCoincident = 1 << 14;       // flag bit of the sorted neighbou
 //                precomputed on the host with the reference's libm; -1 when
 //                var <= 1e-18 (the reference's deterministic branch).
 //
+//   TK[2*(j*n + c)], TC[j*n + c] = ATRISK's classification of the pair
+//                (candidate c, customer j) as a step function of the
+//                candidate's finish time f: switch points {k0, k1}, interval
+//                i = (k_{i-1}, k_i] (unused points +inf) has outcome
+//                (TC >> 2i) & 3 -- 0: the term is +0, 1: it is s_j, 2: the
+//                kernel classifies the pair itself (a factor needs erf).  Every test of the
+//                classification is monotone in f, so the outcome changes only
+//                at their switch points, found by bisection on the host.
+//
 // Two further layouts of the same values serve the two access patterns:
 //   * neighbour-major pair tables FR = {F, R} and GD = {G, dist[o][j+1]} at
 //     pair index j*ld + o, and DP = {dist[c+1][j+1], P1[c*n + j]} at pair
@@ -68,6 +77,8 @@ struct DevInst {
     const uint32_t *zlt, *zle;
     const double *FR, *GD, *DP;   // interleaved pairs
     const double* CU;              // [n][6] per-customer pack
+    const double* TK;              // [n][n][2] ATRISK's step functions at j*n + c: switch points
+    const uint8_t* TC;             // [n][n] and outcome codes
     int ns;                        // sorted-list row stride
     const int16_t* ord;
     const double *sF, *sG;

@@ -61,6 +61,11 @@ struct Group {
     __device__ __forceinline__ static T shfl_xor(T v, int off) {
         return __shfl_xor_sync(mask(), v, off);
     }
+    // v of group lane src
+    template <class T>
+    __device__ __forceinline__ static T shfl(T v, int src) {
+        return __shfl_sync(mask(), v, first() + src);
+    }
 };
 
 // Block shape of the evaluator: warps per block and the minimum resident
@@ -482,7 +487,10 @@ struct WarpCounts {
 struct AtRiskView {
     const double2* CU;      // per customer {close, open}, {P0, dur}, {d2d, score}
     const double* scores;
-    const double2* DPc;     // DP + ci: {dist(ci, j), P1(ci, j)} at j * n
+    const double2* DP;      // {dist(c, j), P1(c, j)} at j * n + c
+    const double2* DPc;     // DP + ci
+    const double2* TKc;     // TK + ci: the step functions' switch points {k0, k1} at j * n
+    const uint8_t* TCc;     // TC + ci: their outcome codes at j * n
     const uint32_t* atr;
     double* Q;
     int n, nw, cap, ci;
@@ -606,9 +614,10 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
     using G = Group<LPP>;
     const int lane = G::lane();
     const uint32_t lt = (1u << lane) - 1u;
-    const double hw = 8.5 * v.sd_c, lw = -8.5 * v.sd_c;
     const bool has = v.ci >= 0;
-    double* const Q = v.Q;
+    // the value rows: terms of the pairs classified in full, then their entries
+    double* const T = v.Q;
+    int* const QE = reinterpret_cast<int*>(v.Q + v.cap);
     double eloss = 0.0;
     unsigned long long heavy = 0;
 
@@ -617,88 +626,109 @@ __device__ __noinline__ double at_risk(const AtRiskView v, WarpCounts& wc) {
         if (word == 0) continue;
         const uint32_t own = has ? bit_in_word(v.ci, w) : 0u;
         if (COUNT && has) heavy += __popc(word & ~own);
-        G::sync();  // the previous word's queue reads are done
+        G::sync();  // the previous word's reads of T are done
         SIDR_SEC_MARK(t_p1)
-        uint32_t addm = 0, ewm = 0, ebm = 0, pbm = 0;
+        // pass 1: each pair's outcome from its step function at the candidate's
+        // finish time, one pair per step with the next pair's loads issued
+        // first; the pairs whose outcome needs the full classification are
+        // queued (customer bit, lane) in (customer, lane) order
+        uint32_t addm = 0, fullm = 0;
         int qn = 0;
-        // one pair per step, the next pair's loads issued before this one's
-        // classification
+        const double f = v.fin_c;
         int bc = __ffs(word) - 1;
         uint32_t bits = word & (word - 1);
         bool lc = has && !((own >> bc) & 1u);
-        AtRiskLoad Lc = at_risk_load(v, (w << 5) + bc, lc);
+        size_t rc = (size_t)(lc ? (w << 5) + bc : 0) * v.n;
+        double2 ka = v.TKc[rc];
+        int kc = v.TCc[rc];
         for (;;) {
-            const bool more = bits != 0;  // warp-uniform
+            const bool more = bits != 0;  // group-uniform
             const int bn = more ? __ffs(bits) - 1 : bc;
             bits &= bits - 1;
             const bool ln = has && !((own >> bn) & 1u);
-            const AtRiskLoad Ln = at_risk_load(v, (w << 5) + bn, ln);
-            const AtRiskClass c = at_risk_compute(v, Lc, lc, hw, lw);
+            const size_t rn = (size_t)(ln ? (w << 5) + bn : 0) * v.n;
+            const double2 na = v.TKc[rn];
+            const int nc = v.TCc[rn];
+            const int iv = (f > ka.x) + (f > ka.y);
+            const int code = lc ? (kc >> (2 * iv)) & 3 : 0;
             const uint32_t m = 1u << bc;
-            addm |= c.add ? m : 0u;
-            ewm |= c.ew ? m : 0u;
-            ebm |= c.eb ? m : 0u;
-            pbm |= c.pb1 ? m : 0u;
-            const uint32_t bw = G::ballot(c.ew);
-            const uint32_t bb = G::ballot(c.eb);
-            const int pw = qn + __popc(bw & lt);
-            qn += __popc(bw);
-            const int pb = qn + __popc(bb & lt);
-            qn += __popc(bb);
-            if (c.ew && pw < v.cap) {
-                Q[2 * pw] = c.wnum;
-                Q[2 * pw + 1] = v.sd_c;
-            }
-            if (c.eb && pb < v.cap) {
-                Q[2 * pb] = c.bnum;
-                Q[2 * pb + 1] = c.bden;
-            }
+            addm |= code == 1 ? m : 0u;
+            const bool full = code == 2;
+            fullm |= full ? m : 0u;
+            const uint32_t bf = G::ballot(full);
+            const int pos = qn + __popc(bf & lt);
+            qn += __popc(bf);
+            if (full && pos < v.cap) QE[pos] = (bc << 8) | lane;
             if (!more) break;
             bc = bn;
             lc = ln;
-            Lc = Ln;
+            ka = na;
+            kc = nc;
         }
         SIDR_SEC_ADD(11, t_p1);
-        if (qn > v.cap) {  // warp-uniform
+        if (qn > v.cap) {  // group-uniform
             eloss = at_risk_word_direct(v, w, word, eloss);
             continue;
         }
         SIDR_SEC_MARK(t_q)
+        // the queued pairs, LPP at a time with every lane busy: the owner's
+        // finish time and deviation come by shuffle, the term (s_j, +0 or
+        // s_j (1 - p_win p_bud) with erf) goes to T in queue order
         if (qn) {
             G::sync();
-            for (int k = lane; k < qn; k += LPP) Q[2 * k] = norm_cdf_ratio(Q[2 * k], Q[2 * k + 1]);
+            for (int base = 0; base < qn; base += LPP) {
+                const int k = base + lane;
+                const bool valid = k < qn;
+                const int e = valid ? QE[k] : 0;
+                const int owner = e & 31;
+                const double fin = G::shfl(v.fin_c, owner), sd = G::shfl(v.sd_c, owner);
+                const int ci = G::shfl(v.ci, owner);
+                if (valid) {
+                    const int j = (w << 5) + (e >> 8);
+                    const double2* cu = v.CU + 3 * (size_t)j;
+                    AtRiskLoad L;
+                    L.dp = v.DP[(size_t)j * v.n + ci];
+                    L.co = cu[0];
+                    L.pd = cu[1];
+                    L.es = cu[2];
+                    AtRiskView o = v;
+                    o.fin_c = fin;
+                    o.sd_c = sd;
+                    const AtRiskClass c = at_risk_compute(o, L, true, 8.5 * sd, -8.5 * sd);
+                    const double sj = L.es.y;
+                    double term = 0.0;
+                    if (c.add) {
+                        term = sj;
+                    } else if (c.ew || c.eb) {
+                        const double fw = c.ew ? norm_cdf_ratio(c.wnum, sd) : 1.0;
+                        const double fb = c.eb ? norm_cdf_ratio(c.bnum, c.bden) : (c.pb1 ? 1.0 : 0.0);
+                        term = sj * (1.0 - fw * fb);
+                    }
+                    T[k] = term;
+                }
+            }
             G::sync();
         }
         SIDR_SEC_ADD(12, t_q);
         SIDR_SEC_MARK(t_p2)
-        // the word's scores: one per lane, shuffled (a full warp), or loaded
+        // pass 2: the terms in ascending customer order, each lane its own sum
+        // (a +0 term leaves it unchanged)
         const int jl = (w << 5) + lane;
         const double sw = (LPP == 32 && jl < v.n) ? v.scores[jl] : 0.0;
-        const uint32_t anym = addm | ewm | ebm;
         qn = 0;
-        for (uint32_t bits = word; bits;) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
+        for (uint32_t bits2 = word; bits2;) {
+            const int b = __ffs(bits2) - 1;
+            bits2 &= bits2 - 1;
             const uint32_t m = 1u << b;
             double sj;
             if constexpr (LPP == 32) sj = __shfl_sync(kFull, sw, b);
             else sj = v.scores[(w << 5) + b];
-            const bool ew = (ewm & m) != 0, eb = (ebm & m) != 0;
-            const uint32_t bw = G::ballot(ew);
-            const uint32_t bb = G::ballot(eb);
-            const int pw = qn + __popc(bw & lt);
-            qn += __popc(bw);
-            const int pb = qn + __popc(bb & lt);
-            qn += __popc(bb);
-            if (anym & m) {
-                if (addm & m) {
-                    eloss += sj;
-                } else {
-                    const double fw = ew ? Q[2 * pw] : 1.0;
-                    const double fb = eb ? Q[2 * pb] : ((pbm & m) ? 1.0 : 0.0);
-                    eloss += sj * (1.0 - fw * fb);
-                }
-            }
+            const bool full = (fullm & m) != 0;
+            const uint32_t bf = G::ballot(full);
+            const int pos = qn + __popc(bf & lt);
+            qn += __popc(bf);
+            if (addm & m) eloss += sj;
+            else if (full) eloss += T[pos];
         }
         SIDR_SEC_ADD(13, t_p2);
     }
@@ -716,7 +746,10 @@ __device__ __forceinline__ AtRiskView at_risk_view(const DevInst& I, const WarpS
     AtRiskView v;
     v.CU = reinterpret_cast<const double2*>(I.CU);
     v.scores = I.scores;
-    v.DPc = reinterpret_cast<const double2*>(I.DP);
+    v.DP = reinterpret_cast<const double2*>(I.DP);
+    v.DPc = v.DP;
+    v.TKc = reinterpret_cast<const double2*>(I.TK);
+    v.TCc = I.TC;
     v.atr = S.atr;
     v.Q = S.rows;
     v.n = I.n;
@@ -734,6 +767,8 @@ __device__ __forceinline__ AtRiskView at_risk_view(const DevInst& I, const WarpS
         v.fin_c = st_c + dur_i;
         v.sd_c = kSigma * dur_i;
         v.DPc += ci;
+        v.TKc += ci;
+        v.TCc += ci;
     }
     return v;
 }

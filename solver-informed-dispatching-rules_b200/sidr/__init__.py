@@ -69,6 +69,7 @@ EXPORTS = [
     "sidr_libm_eval", "sidr_batch_guard_check", "sidr_libm_pow", "sidr_multi_autotune_sampled",
     "sidr_batch_set_shape", "sidr_batch_autotune_sampled", "sidr_ctx_set_shape",
     "sidr_multi_autotune_classes", "sidr_multi_set_class_shape", "sidr_multi_shapes",
+    "sidr_atrisk_table_check",
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -169,6 +170,19 @@ def zstats(sd) -> np.ndarray:
     inst = k.inst(sd)
     _check(L.sidr_zstats(C.byref(inst), _d(zp)))
     return zp
+
+
+def atrisk_table_check(sd, seed: int = 0):
+    """sidr_atrisk_table_check: (points checked, mismatches) of ATRISK's
+    per-pair step functions against the classification they stand for."""
+    L = load()
+    L.sidr_atrisk_table_check.argtypes = [C.POINTER(_Inst), C.c_int32, C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_int64)]
+    k = _Keep()
+    inst = k.inst(sd)
+    a, b = C.c_int64(), C.c_int64()
+    _check(L.sidr_atrisk_table_check(C.byref(inst), seed, C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def rules_check(rules, masks, mask_group=None) -> int:

@@ -8,7 +8,7 @@
  * accumulation whose GEMMs run on hand-written sm_100a tensor-core kernels
  * (tcgen05.mma with TMEM accumulators).  The model is trained online on the
  * fitness the simulator has just produced and pre-screens GP offspring; the
- * simulator stays the judge of every reported fitness, and the GP falls back
+ * simulator decides every reported fitness, and the GP falls back
  * to plain breeding when the model's rank correlation on an audit sample is
  * too low.
  */

@@ -1,6 +1,6 @@
 // sidr_sgp.cpp -- the surrogate-assisted GP driver (include/sidr_surrogate.h):
 // the GP of sidr_gp_core.hpp whose offspring are pre-screened by the MLP of
-// sidr_surrogate.cu on their phenotypes, with the evaluator as the judge of
+// sidr_surrogate.cu on their phenotypes, with the evaluator deciding
 // every fitness and plain breeding whenever the model's audit rank
 // correlation is too low.
 #include <algorithm>

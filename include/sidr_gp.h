@@ -162,10 +162,11 @@ sidr_status sidr_gen_durations(int32_t n, const double* durations, double sigma,
  * refresh in shared memory; the Box-Muller log, cos and sin are computed in
  * double-double arithmetic, and a pair whose C-library result those values
  * do not settle (a few percent) is recomputed on the host with the C library
- * after the kernel.  out: [S][n] doubles in host memory (out_on_device = 0)
- * or in the device memory of `device` (1).  stats (may be NULL): Box-Muller
- * pairs drawn and pairs recomputed on the host.  The call allocates its
- * device scratch and waits for its work. */
+ * after the kernel (a block with more of them than an eighth of its pairs
+ * is sampled on the host as a whole).  out: [S][n] doubles in host memory
+ * (out_on_device = 0) or in the device memory of `device` (1).  stats (may
+ * be NULL): Box-Muller pairs drawn and pairs computed on the host.  The call
+ * allocates its device scratch and waits for its work. */
 typedef struct sidr_sample_stats {
     int64_t pairs;
     int64_t host_pairs;

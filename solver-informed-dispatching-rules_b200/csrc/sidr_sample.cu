@@ -217,7 +217,10 @@ extern "C" sidr_status sidr_gen_durations_device(int32_t device, int32_t n, cons
     DevArr<int32_t> d_cust, d_zeros;
     DevArr<unsigned long long> d_nflag;
     DevArr<FlagRec> d_flags;
-    const long long cap = (long long)S * npairs;
+    // records of unsettled pairs: room for an eighth of the pairs (about 5 % are
+    // unsettled); a block with more falls back to the host sampler as a whole
+    const long long all_pairs = (long long)S * npairs;
+    const long long cap = std::min(all_pairs, std::max(4096ll, all_pairs / 8));
     cudaStream_t st = nullptr;
     if (!e) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (!e) e = d_mu.alloc(npos);
@@ -246,9 +249,28 @@ extern "C" sidr_status sidr_gen_durations_device(int32_t device, int32_t n, cons
     unsigned long long nflag = 0;
     if (!e) e = cudaMemcpyAsync(&nflag, d_nflag.p, sizeof nflag, cudaMemcpyDeviceToHost, st);
     if (!e) e = cudaStreamSynchronize(st);
+    if (!e && (long long)nflag > cap) {
+        // more unsettled pairs than records: the host sampler gives the block
+        std::vector<double> host;
+        double* hout = out;
+        if (out_on_device) {
+            host.resize((size_t)S * n);
+            hout = host.data();
+        }
+        const sidr_status hs = sidr_gen_durations(n, durations, sigma, S, base_seed, hout);
+        if (hs != SIDR_OK) {
+            cudaStreamDestroy(st);
+            return hs;
+        }
+        if (out_on_device) e = cudaMemcpy(out, hout, (size_t)S * n * 8, cudaMemcpyHostToDevice);
+        cudaStreamDestroy(st);
+        if (e) return fail_s(SIDR_ERR_CUDA, std::string("sampling: ") + cudaGetErrorString(e));
+        if (stats) stats->host_pairs = all_pairs;
+        return SIDR_OK;
+    }
     std::vector<FlagRec> fl;
     if (!e && nflag) {
-        fl.resize((size_t)std::min<long long>((long long)nflag, cap));
+        fl.resize((size_t)nflag);
         e = cudaMemcpyAsync(fl.data(), d_flags.p, fl.size() * sizeof(FlagRec), cudaMemcpyDeviceToHost, st);
         if (!e) e = cudaStreamSynchronize(st);
     }
